@@ -1,0 +1,361 @@
+"""Benchmark: Biot-Savart node velocities per second (velocity_on_nodes! on a 20k-node tangle).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+One step = one velocity evaluation on all nodes of the workload: device-side point data
+(quintic splines, quadrature points), cell lists, pair kernel, local term, NUFFT long range.
+`value` is measured with the filament nodes already resident in HBM; `e2e` goes through the
+public API (velocity_on_nodes_ with host arrays): host->device copy of the nodes and
+device->host copy of the velocities inside the timed region.  Multi-GPU (torchrun): every rank
+evaluates its own independent tangle (weak scaling, no collective on the data path).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Biot–Savart node-velocities/s at 1e-5 rel err: tuned FP32 vs plain FP64 GPU"
+UNIT = "node-velocities/s"
+F_PAIR_VEL = 40.0  # flops per in-range pair (velocity), convention of the roofline model
+L2_FLUSH_BYTES = 256 << 20
+
+
+def load_package():
+    import importlib.util
+    name = "vortexpasta_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = ROOT / "vortexpasta.jl_b200"
+    spec = importlib.util.spec_from_file_location(name, pkg / "__init__.py", submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+WORKLOAD_DESC = {
+    "tangle20k": "tangle20k: 100 random perturbed rings x 200 nodes = 20,000 nodes, L=2pi, quintic splines, GL(3), "
+                 "beta=3.5, r_cut=L/8 (alpha=4.456), Ns=128 (FFT 192^3), sigma=1.5, m=4, Gamma=1, a=1e-8, "
+                 "Delta=1/4, CellLists M=2",
+    "ring64": "ring64: single ring R=L/4, 64 nodes, beta=3.5, r_cut=L/4, Ns=32 (FFT 48^3), m=4",
+    "tangle1m": "tangle1m: 5000 rings x 200 nodes = 1,000,000 nodes, beta=4, r_cut=L/16, Ns=512 (FFT 768^3), m=5",
+}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        import tempfile
+        self.path = tempfile.mktemp(suffix=".csv")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_oracle_time(fs, p, nthreads, reps):
+    """Oracle (CPU FP64 restatement) timing: returns (seconds per evaluation, velocity)."""
+    from oracle import oracle as O
+    v = None
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        v, _, _ = O.compute_on_nodes(p, fs, velocity=True, streamfunction=False, nthreads=nthreads)
+        ts.append(time.perf_counter() - t0)
+    return min(ts), v
+
+
+def host_cores():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    vp = load_package()
+    fs, p = vp.configs.WORKLOADS[args.workload]()
+    Np = sum(len(f) for f in fs)
+    cores = host_cores()
+    for _ in range(min(args.warmup, 1)):
+        cpu_oracle_time(fs, p, cores, 1)
+    times = [cpu_oracle_time(fs, p, cores, 1)[0] for _ in range(args.steps)]
+    t = statistics.mean(times)
+    value = Np / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC[args.workload], "fields": "velocity"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"one full velocity evaluation of {args.workload} per step "
+                                   "(CPU FP64 restatement of the reference path, OpenMP)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def stage_model(stage, S):
+    """Algorithmic work per launch of each stage: (bound, amount, unit)."""
+    Np, Nq, n3, nc3 = S["Np"], S["Nq"], S["n3"], S["nc3"]
+    if stage == "pairs":
+        return "fp64", S["pairs"] * F_PAIR_VEL, "flop"
+    if stage == "spread":
+        return "hbm", Nq * 6 * 8 + 3 * n3 * 8, "byte"
+    if stage == "interp":
+        return "hbm", 3 * n3 * 8 + Np * 3 * 8 + Np * 3 * 8, "byte"
+    if stage == "fourier":
+        return "hbm", 2 * 3 * nc3 * 16, "byte"
+    if stage in ("fft_forward", "fft_inverse"):
+        return "hbm", 2 * 2 * 3 * n3 * 8, "byte"
+    if stage == "local_self":
+        return "hbm", Np * (11 * 8 + 6 * S["nq"] * 6 * 8) + Np * 3 * 8, "byte"
+    if stage == "geometry":
+        return "hbm", Np * 3 * 8 + Np * (3 * 3 * 8 + 12 * 8) + Np * (11 * 8) + Nq * 6 * 8, "byte"
+    if stage == "cell_lists":
+        return "hbm", Nq * (6 * 8 * 3 + 4 * 4) + Np * 16, "byte"
+    return "hbm", 0.0, "byte"
+
+
+def read_traffic(kernel_stage):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    f = ROOT / "profiles" / "dram_traffic_tangle20k.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel_stage:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    rank, local_rank, world = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA GPU")
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    vp = load_package()
+    from vortexpasta_b200 import _lib
+    fs, p = vp.configs.WORKLOADS[args.workload](seed=42 + rank) if args.workload != "ring64" else \
+        vp.configs.ring64()
+    p = p.with_(device=local_rank)
+    Np = sum(len(f) for f in fs)
+    Nq = Np * len(p.quadrature)
+    nodes, offsets = vp.curves.concat(fs)
+
+    stream = torch.cuda.Stream(device=dev)
+    cache = vp.init_cache(p)
+    cache.set_stream(stream.cuda_stream)
+    nodes_dev = torch.from_numpy(nodes).to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+
+    def step_device():
+        cache.set_filaments(None, on_device_ptr=nodes_dev.data_ptr(), offsets=offsets)
+        cache.compute(_lib.VELOCITY)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step_device()
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident inputs ----
+    cache.stage_timing(True)
+    launches0 = cache.launch_count()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stage_ms = {}
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()  # L2 flush between timed steps (outside the events)
+                starts[k].record(stream)
+                step_device()
+                ends[k].record(stream)
+                for name, ms in cache.stage_times().items():
+                    stage_ms.setdefault(name, []).append(ms)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = cache.launch_count() - launches0
+    cache.stage_timing(False)
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    pairs_in_range, _ = cache.pair_counts()
+    v_dev = cache.get(_lib.VELOCITY)
+
+    # ---- e2e: public API with host arrays ----
+    vs = [np.zeros_like(f) for f in fs]
+    with torch.cuda.stream(stream):
+        vp.velocity_on_nodes_(vs, cache, fs)  # warm
+        e_starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        e_ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.zero_()
+            e_starts[k].record(stream)
+            vp.velocity_on_nodes_(vs, cache, fs)
+            e_ends[k].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = sum(s.elapsed_time(e) for s, e in zip(e_starts, e_ends))
+
+    tot = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms = tot.tolist()
+    ms_per_step = total_ms / args.steps
+    value = world * Np * args.steps / (total_ms * 1e-3)
+    e2e_value = world * Np * args.steps / (e2e_ms * 1e-3)
+
+    if rank == 0:
+        lr = cache.params.splitting
+        n = [_lib.load().vpbs_fft_size(N, p.backend_long.sigma) for N in lr.Ns]
+        S = {"Np": Np, "Nq": Nq, "n3": n[0] * n[1] * n[2], "nc3": (n[0] // 2 + 1) * n[1] * n[2], "pairs": pairs_in_range,
+             "nq": len(p.quadrature)}
+        avg = {k: statistics.mean(v) for k, v in stage_ms.items()}
+        dom = max(avg, key=avg.get)
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+        hbm = peaks.get("hbm_gbs")
+        hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if hbm else "fallback 6650 GB/s"
+        hbm = hbm or 6650.0
+        fp64_peak = ct_double = None
+        import ctypes as ct
+        ct_double = ct.c_double()
+        if _lib.load().vpbs_fma_throughput(local_rank, 1, ct.byref(ct_double)) == 0:
+            fp64_peak = ct_double.value
+        stages = {}
+        for name, ms in avg.items():
+            bound, amount, unit = stage_model(name, S)
+            if ms <= 0:
+                continue
+            if bound == "fp64":
+                ach = amount / (ms * 1e-3) / 1e12
+                stages[name] = {"ms": ms, "bound": "fp64", "achieved": ach, "unit": "TFLOP/s",
+                                "frac": ach / fp64_peak if fp64_peak else None}
+            else:
+                ach = amount / (ms * 1e-3) / 1e9
+                stages[name] = {"ms": ms, "bound": "hbm", "achieved": ach, "unit": "GB/s", "frac": ach / hbm}
+        d = stages[dom]
+        roof = {"kernel": dom, "bound": d["bound"], "achieved": d["achieved"],
+                "peak": fp64_peak if d["bound"] == "fp64" else hbm, "unit": d["unit"], "frac": d["frac"],
+                "traffic": read_traffic(dom),
+                "peak_source": ("measured FP64 FMA throughput (vpbs_fma_throughput)" if d["bound"] == "fp64"
+                                else hbm_src)}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_DESC[args.workload], "form": "plain FP64", "fields": "velocity",
+                       "parallelism": f"replicas x{world} (independent tangles, no collective)",
+                       "l2": "flushed between timed steps (256 MiB write, outside the timed events)"},
+            "roofline": roof,
+            "stages": stages,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(nodes.nbytes + offsets.nbytes),
+                    "d2h_bytes_per_step": int(Np * 3 * 8)},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "pairs_in_range": int(pairs_in_range),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            cores = host_cores()
+            t_cpu, v_cpu = cpu_oracle_time(fs, p, cores, args.cpu_reps)
+            line["cpu_baseline"] = {"value": Np / t_cpu, "unit": UNIT, "cores": cores, "kind": "port",
+                                    "sample": f"{args.cpu_reps} full velocity evaluations of {args.workload} "
+                                              "(CPU FP64 restatement, OpenMP), best taken"}
+            line["accuracy"] = {"rel_l2_vs_oracle": float(np.linalg.norm(v_dev - v_cpu) / np.linalg.norm(v_cpu))}
+        print(json.dumps(line), flush=True)
+    cache.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="tangle20k", choices=sorted(WORKLOAD_DESC))
+    ap.add_argument("--cpu-reps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    return run_reference(args) if args.impl == "reference" else run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

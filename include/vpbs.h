@@ -1,0 +1,184 @@
+/*
+ * vpbs.h -- C ABI of libvpbs.so, a CUDA (sm_100a) implementation of VortexPasta's
+ * Ewald-split Biot-Savart velocity / streamfunction evaluation on filament nodes.
+ *
+ * The library is a drop-in for the CellListsBackend + NonuniformFFTsBackend pair of
+ * VortexPasta.BiotSavart.  Every entry point below names the reference interface it
+ * replaces (paths relative to the VortexPasta.jl source tree).  All functions
+ * return 0 on success and a negative vpbs_status on failure; the message is then
+ * available from vpbs_last_error(handle) (or vpbs_last_error(NULL) for failures of
+ * vpbs_create).
+ *
+ * Ownership: the caller owns every host array it passes; the library owns all device
+ * memory, cuFFT plans, streams and pinned staging buffers of a handle, and retains no
+ * caller pointer after a call returns.  Calls on one handle must be serialised by the
+ * caller; distinct handles may be used concurrently from different threads (each has
+ * its own CUDA stream unless vpbs_set_stream is used).
+ */
+#ifndef VPBS_H
+#define VPBS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct vpbs_handle vpbs_handle;
+
+typedef enum {
+    VPBS_OK = 0,
+    VPBS_ERR_ARG = -1,        /* invalid argument (null pointer, bad size, bad flag) */
+    VPBS_ERR_PARAMS = -2,     /* inconsistent parameters (e.g. r_cut too large) */
+    VPBS_ERR_OOM = -3,        /* device or pinned-host allocation failed */
+    VPBS_ERR_CUDA = -4,       /* CUDA runtime or cuFFT error */
+    VPBS_ERR_STATE = -5,      /* call out of order (e.g. compute before set_points) */
+    VPBS_ERR_TIMEOUT = -6     /* a bounded device-side wait gave up */
+} vpbs_status;
+
+/* Output field selection bits for vpbs_compute and friends. */
+#define VPBS_VELOCITY 1
+#define VPBS_STREAMFUNCTION 2
+
+/* LIA modes of compute_on_nodes! (src/BiotSavart/BiotSavart.jl:395-404). */
+#define VPBS_LIA_FALSE 0
+#define VPBS_LIA_TRUE 1
+#define VPBS_LIA_ONLY 2
+
+/* Arithmetic forms. */
+#define VPBS_PRECISION_FP64 0 /* plain method: everything in double precision */
+#define VPBS_PRECISION_MIXED 1 /* FP32 bulk (pairs, spreading, FFT, interpolation); FP64
+                                  positions, separations, local term, final accumulation */
+
+/* Parameters: the union of ParamsCommon, ParamsShortRange and ParamsLongRange
+ * (src/BiotSavart/params.jl:8-30, 74-115, 141-152) plus the two backends
+ * (CellListsBackend, shortrange/backends/cell_lists.jl:64-87; NonuniformFFTsBackend,
+ * longrange/backends/nonuniformffts.jl:97-126).  GaussianSplitting is described by
+ * (alpha, rcut, Ns) already derived by the caller (splitting/gaussian.jl:133-200);
+ * alpha == 0 selects NoSplitting (open domain, naive pair sum, no long range). */
+typedef struct {
+    double Gamma;                 /* circulation */
+    double a;                     /* vortex core size */
+    double Delta;                 /* core vorticity-profile coefficient */
+    double L[3];                  /* periods (ignored when alpha == 0) */
+    double alpha;                 /* Ewald splitting parameter, 0 => NoSplitting */
+    double rcut;                  /* short-range cut-off distance */
+    int32_t Ns[3];                /* Fourier modes per direction */
+    double sigma;                 /* NUFFT oversampling factor (reference default 1.5) */
+    int32_t m;                    /* NUFFT kernel half-support (HalfSupport(m)) */
+    int32_t nquad;                /* quadrature points per segment (1..16) */
+    double quad_zeta[16];         /* quadrature nodes on [0, 1] */
+    double quad_w[16];            /* quadrature weights on [0, 1] */
+    int32_t nquad_near;           /* quadrature_near_singularity (1..16) */
+    double quad_near_zeta[16];
+    double quad_near_w[16];
+    double lia_segment_fraction;  /* in (0, 1]; <= 0 means `nothing` */
+    int32_t avoid_explicit_erf;   /* reference default 1 */
+    int32_t truncate_spherical;   /* longrange_truncate_spherical */
+    int32_t nsubdiv;              /* CellListsBackend subdivisions M (reference default 2) */
+    int32_t precision;            /* VPBS_PRECISION_* */
+    int32_t device;               /* CUDA device ordinal */
+} vpbs_params;
+
+/* Structure-of-arrays view of a vector of Vec3 (the layout of a StructVector{Vec3}). */
+typedef struct { const double* x; const double* y; const double* z; } vpbs_cvec3;
+typedef struct { double* x; double* y; double* z; } vpbs_vec3;
+
+/* BiotSavart.init_cache(params) -> BiotSavartCache  (src/BiotSavart/cache.jl:40-49;
+ * init_cache_short, shortrange/backends/cell_lists.jl:103-115; init_cache_long_ewald,
+ * longrange/backends/nonuniformffts.jl:153-171).  Validates the parameters with the
+ * reference's rules (params.jl:99-106; CellLists.jl:135-147). */
+int vpbs_create(const vpbs_params* params, vpbs_handle** out);
+
+/* Releases every resource of the handle. */
+int vpbs_destroy(vpbs_handle* h);
+
+/* Message of the last failure on `h` (or of the last failed vpbs_create when h is NULL). */
+const char* vpbs_last_error(const vpbs_handle* h);
+
+/* Run all work of `h` on the caller's CUDA stream (a cudaStream_t; NULL restores the
+ * handle's own stream).  Replaces the device selection of activate_device!
+ * (src/BiotSavart/ka_utils.jl:38-49). */
+int vpbs_set_stream(vpbs_handle* h, void* stream);
+
+/* add_point_charges!(pointdata, fs, params) on the device (src/BiotSavart/pointdata_impl.jl:41-108):
+ * from closed-filament nodes (AoS [Np][3], filament f owns nodes offsets[f]..offsets[f+1]-1)
+ * builds chordal knots, periodic quintic splines (src/Filaments/spline/quintic.jl:9-100) and
+ * the point data (folded nodes, previous-node indices, s' and s'' on nodes, sub-segment
+ * lengths, quadrature points and charges).  `offsets` is always a host array; `nodes_xyz` is a
+ * host pointer (copied through pinned staging) when `on_device` = 0, or a device pointer read
+ * in place on the handle's stream when `on_device` = 1. */
+int vpbs_set_filaments(vpbs_handle* h, int64_t nfil, const int64_t* offsets, const double* nodes_xyz,
+                       int32_t on_device);
+
+/* Plugin-contract entry: PointData computed by the caller (the reference computes it on the
+ * host in add_point_charges!).  Layout per src/BiotSavart/pointdata.jl:21-31: nodes, derivatives
+ * and charges as SoA views; node_idx_prev is 1-based as in the reference; points/charges hold
+ * nquad entries per node, point index nquad*(n-1)+q on segment [n, n+1]. Host pointers. */
+int vpbs_set_points(vpbs_handle* h, int64_t Np, vpbs_cvec3 nodes, const int32_t* node_idx_prev,
+                    vpbs_cvec3 deriv1, vpbs_cvec3 deriv2, const double* delta_minus,
+                    const double* delta_plus, vpbs_cvec3 points, vpbs_cvec3 charges);
+
+/* compute_on_nodes!(fields, cache, fs; LIA, shortrange, longrange) without the host
+ * transfers (src/BiotSavart/BiotSavart.jl:515-612): results stay in device memory.
+ * fields: VPBS_VELOCITY | VPBS_STREAMFUNCTION.  integration_cutoff <= 0 means `nothing`
+ * (local_integrals.jl:115-126).  Asynchronous on the handle's stream. */
+int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t shortrange, int32_t longrange,
+                 double integration_cutoff);
+
+/* copy_output_values_on_nodes! (src/BiotSavart/BiotSavart.jl:628-715): device -> host copy of a
+ * computed field (VPBS_VELOCITY or VPBS_STREAMFUNCTION) in node order, AoS [Np][3].
+ * accumulate = 1 adds to the existing host values (op = +), 0 overwrites.  Synchronises the
+ * handle's stream. */
+int vpbs_get(vpbs_handle* h, int32_t field, double* out_xyz, int32_t accumulate);
+
+/* Same as vpbs_get but into SoA host arrays. */
+int vpbs_get_soa(vpbs_handle* h, int32_t field, vpbs_vec3 out, int32_t accumulate);
+
+/* Device pointers of a computed field (SoA, Np doubles each), valid until the next call that
+ * changes the number of nodes or vpbs_destroy. */
+int vpbs_device_field(vpbs_handle* h, int32_t field, double** x, double** y, double** z);
+
+/* get_longrange_field_fourier (src/BiotSavart/cache.jl:72-83): the vorticity Fourier
+ * coefficients of the last long-range computation (state :vorticity, unsmoothed), as
+ * complex-interleaved doubles [3][Ns2][Ns1][Ns0/2+1] (x fastest).  `n_doubles` must equal
+ * 2*3*Ns2*Ns1*(Ns0/2+1).  Synchronises the handle's stream. */
+int vpbs_get_uhat(vpbs_handle* h, double* out, int64_t n_doubles);
+
+/* Read back the device point data (the fields of PointData, src/BiotSavart/pointdata.jl:21-31,
+ * as exposed by cache.pointdata): which = 0 nodes (folded, SoA 3*Np), 1 s' on nodes (3*Np),
+ * 2 s'' on nodes (3*Np), 3 delta_minus (Np), 4 delta_plus (Np), 5 points (SoA 3*Nq),
+ * 6 charges (SoA 3*Nq), 7 node_idx_prev (Np int32, 0-based).  `n_elems` must match.
+ * Synchronises the handle's stream. */
+int vpbs_get_pointdata(vpbs_handle* h, int32_t which, void* out, int64_t n_elems);
+
+/* Short-range counters of the last computation: in-range pairs (r^2 <= r_cut^2) and
+ * examined candidate pairs.  Synchronises the handle's stream. */
+int vpbs_pair_counts(vpbs_handle* h, int64_t* in_range, int64_t* candidates);
+
+/* Oversampled FFT grid size chosen for Ns modes at oversampling sigma (smallest even
+ * 2^a 3^b 5^c >= sigma*Ns); the reference delegates this to NonuniformFFTs.jl. */
+int32_t vpbs_fft_size(int32_t Ns, double sigma);
+
+/* Number of the library's own kernels launched on `h` since creation (cuFFT's kernels are not
+ * counted).  Measurement support; no counterpart in the reference. */
+int64_t vpbs_launch_count(const vpbs_handle* h);
+
+/* Per-stage CUDA-event timing on the handle's stream, the device-side analogue of the
+ * reference's TimerOutputs sections (src/BiotSavart/BiotSavart.jl:417-509).  Enable with
+ * vpbs_stage_timing(h, 1); vpbs_stage_times fills ms[0..VPBS_NUM_STAGES) with the time of each
+ * stage since the previous query (synchronises the stream); vpbs_stage_name(i) names stage i. */
+#define VPBS_NUM_STAGES 9
+int vpbs_stage_timing(vpbs_handle* h, int32_t enable);
+int vpbs_stage_times(vpbs_handle* h, double* ms, int32_t n);
+const char* vpbs_stage_name(int32_t i);
+
+/* Measured CUDA-core FMA throughput of `device` in TFLOP/s (fp64 = 1: double, 0: float); the
+ * denominator of the pair kernel's roofline.  Measurement support; no counterpart in the
+ * reference. */
+int vpbs_fma_throughput(int32_t device, int32_t fp64, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,108 @@
+"""CPU-side checks of the C ABI: the library loads, exports exactly what include/vpbs.h
+declares, rejects bad parameters before touching a GPU, and reports errors through
+vpbs_last_error (host-side fault injection, no GPU needed)."""
+
+import ctypes as ct
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    src = (ROOT / "include" / "vpbs.h").read_text()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(vpbs_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol(vp, built_lib):
+    from vortexpasta_b200 import _lib
+    lib = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 14
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_lib.SIGNATURES), "ctypes prototypes out of sync with include/vpbs.h"
+
+
+def test_params_struct_layout(vp):
+    from vortexpasta_b200 import _lib
+    # offsets of the C struct computed by the C compiler rules for the declared members
+    P = _lib.VpbsParams
+    assert P.L.offset == 24 and P.Ns.offset == 64 and P.sigma.offset == 80
+    assert ct.sizeof(P) % 8 == 0
+
+
+def _params(vp, **kw):
+    from vortexpasta_b200.biotsavart import _c_params
+    fs, p = vp.configs.ring64()
+    return _c_params(p), p
+
+
+def test_create_rejects_bad_parameters_without_gpu(vp):
+    from vortexpasta_b200 import _lib
+    lib = _lib.load()
+    c, _ = _params(vp)
+    bad = []
+    c1 = _lib.VpbsParams.from_buffer_copy(c)
+    c1.rcut = 3.0  # > 2/5 L with nsubdiv = 2 (CellLists.jl:114-115)
+    bad.append(c1)
+    c2 = _lib.VpbsParams.from_buffer_copy(c)
+    c2.nquad = 0
+    bad.append(c2)
+    c3 = _lib.VpbsParams.from_buffer_copy(c)
+    c3.a = -1.0
+    bad.append(c3)
+    c4 = _lib.VpbsParams.from_buffer_copy(c)
+    c4.m = 20
+    bad.append(c4)
+    c5 = _lib.VpbsParams.from_buffer_copy(c)
+    c5.sigma = 1.0
+    bad.append(c5)
+    for cp in bad:
+        h = ct.c_void_p()
+        rc = lib.vpbs_create(ct.byref(cp), ct.byref(h))
+        assert rc == -2, rc
+        assert not h.value
+        assert lib.vpbs_last_error(None)
+    assert lib.vpbs_create(ct.byref(bad[0]), ct.byref(ct.c_void_p())) == -2
+    assert b"larger than that allowed" in lib.vpbs_last_error(None)
+
+
+def test_null_arguments(vp):
+    from vortexpasta_b200 import _lib
+    lib = _lib.load()
+    assert lib.vpbs_create(None, None) == -1
+    assert lib.vpbs_destroy(None) == 0
+    assert lib.vpbs_compute(None, 1, 1, 1, 1, 0.0) == -1
+    assert lib.vpbs_launch_count(None) == 0
+
+
+def test_python_params_mirror_reference_errors(vp):
+    L = vp.configs.L
+    with pytest.raises(ValueError, match="larger than that allowed"):
+        vp.ParamsBiotSavart(Gamma=1.0, a=1e-8, splitting=vp.GaussianSplitting(Ls=L, alpha=1.0, rcut=2.6, Ns=32))
+    with pytest.raises(ValueError, match="NaiveShortRangeBackend"):
+        vp.ParamsBiotSavart(Gamma=1.0, a=1e-8, splitting=vp.GaussianSplitting(Ls=L, alpha=1.0, rcut=3.2, Ns=32),
+                            backend_short=vp.NaiveShortRangeBackend())
+    # the naive backend allows up to L/2 (naive.jl:8-16)
+    vp.ParamsBiotSavart(Gamma=1.0, a=1e-8, splitting=vp.GaussianSplitting(Ls=L, alpha=1.0, rcut=3.1, Ns=32),
+                        backend_short=vp.NaiveShortRangeBackend())
+    with pytest.raises(TypeError):
+        vp.GaussianSplitting(Ls=L, alpha=1.0)
+
+
+def test_gaussian_splitting_derivations(vp):
+    """splitting/gaussian.jl:133-200 and its docstring example (Ns = 128, beta = 3.5 => alpha = 9)."""
+    L = vp.configs.L
+    g = vp.GaussianSplitting(Ls=L, beta=3.5, Ns=128)
+    assert abs(g.alpha - 9.0) < 1e-12 and abs(g.rcut - 3.5 / 9) < 1e-12
+    assert abs(g.rtol - 2.398239748342885e-7) < 1e-18
+    g2 = vp.GaussianSplitting(Ls=L, beta=3.5, rcut=L / 4)
+    assert abs(g2.alpha - 3.5 / (L / 4)) < 1e-12
+    assert g2.Ns == (vp.kmax_to_gridsize(2 * g2.alpha * 3.5, L),) * 3
+    g3 = vp.GaussianSplitting(Ls=L, rtol=g.rtol, alpha=9.0)
+    assert abs(g3.rcut - g.rcut) < 1e-12
+    assert vp.maximum_wavenumber((128,) * 3, (L,) * 3) == pytest.approx(63.0)

@@ -1,0 +1,166 @@
+"""Parity of the CUDA library (through its C ABI) with the CPU oracle.
+
+Bar (north star): the plain FP64 GPU form matches the FP64 oracle to <= 1e-10 relative L2
+per node-velocity (and streamfunction) field.  Pair counts are integers and must match
+exactly.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10  # relative L2, FP64 form vs FP64 oracle
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def gpu_fields(vp, p, fs, **kw):
+    cache = vp.init_cache(p)
+    vs = [np.zeros_like(f) for f in fs]
+    ps = [np.zeros_like(f) for f in fs]
+    vp.compute_on_nodes_({"velocity": vs, "streamfunction": ps}, cache, fs, **kw)
+    return np.concatenate(vs), np.concatenate(ps), cache
+
+
+def test_point_data_matches_oracle(vp, oracle, built_lib):
+    fs, p = vp.configs.tangle20k()
+    fs = fs[:10] + [vp.curves.ring(5, 0.3, center=(1, 1, 1)), vp.curves.ring(7, 0.5, center=(6.2, 0.1, 3))]
+    cache = vp.init_cache(p)
+    cache.set_filaments(fs)
+    g = cache.pointdata()
+    o = oracle.point_data(p, fs)
+    for k in ("nodes", "d1", "d2", "dm", "dp", "points", "charges"):
+        assert rel(g[k], o[k]) < 1e-13, k
+    np.testing.assert_array_equal(g["idx_prev"], o["idx_prev"])
+
+
+@pytest.mark.parametrize("workload", ["ring64", "tangle20k"])
+def test_full_velocity_streamfunction(vp, oracle, built_lib, workload):
+    fs, p = vp.configs.WORKLOADS[workload]()
+    v, psi, cache = gpu_fields(vp, p, fs)
+    vo, po, st = oracle.compute_on_nodes(p, fs, streamfunction=True)
+    assert rel(v, vo) < TOL
+    assert rel(psi, po) < TOL
+    assert cache.pair_counts()[0] == st["pairs_in_range"]
+
+
+def test_golden_ring64(vp, built_lib):
+    from pathlib import Path
+    g = np.load(Path(__file__).parent / "golden" / "ring64.npz")
+    fs, p = vp.configs.ring64()
+    v, psi, _ = gpu_fields(vp, p, fs)
+    assert rel(v, g["velocity"]) < TOL and rel(psi, g["streamfunction"]) < TOL
+
+
+@pytest.mark.parametrize("LIA", [True, False, "only"])
+@pytest.mark.parametrize("short,long", [(True, True), (True, False), (False, True)])
+def test_flags(vp, oracle, built_lib, LIA, short, long):
+    fs, p = vp.configs.ring64()
+    if not short and LIA == "only":
+        pytest.skip("no contribution")
+    v, psi, _ = gpu_fields(vp, p, fs, LIA=LIA, shortrange=short, longrange=long)
+    vo, po, _ = oracle.compute_on_nodes(p, fs, streamfunction=True, LIA=LIA, shortrange=short, longrange=long)
+    assert rel(v, vo) < TOL and rel(psi, po) < TOL
+
+
+@pytest.mark.parametrize("variant", ["explicit_erf", "lia_fraction", "truncate", "m5", "gl2", "nsubdiv1"])
+def test_parameter_variants(vp, oracle, built_lib, variant):
+    fs, p = vp.configs.tangle20k()
+    fs = fs[:30]
+    kw = {
+        "explicit_erf": dict(avoid_explicit_erf=False),
+        "lia_fraction": dict(lia_segment_fraction=0.3, quadrature_near_singularity=vp.GaussLegendre(6)),
+        "truncate": dict(longrange_truncate_spherical=True),
+        "m5": dict(backend_long=vp.NonuniformFFTsBackend(1.5, 5)),
+        "gl2": dict(quadrature=vp.GaussLegendre(2)),
+        "nsubdiv1": dict(backend_short=vp.CellListsBackend(1)),
+    }[variant]
+    p = p.with_(**kw)
+    v, psi, _ = gpu_fields(vp, p, fs)
+    vo, po, _ = oracle.compute_on_nodes(p, fs, streamfunction=True)
+    assert rel(v, vo) < TOL and rel(psi, po) < TOL
+
+
+def test_vorticity_fourier_coefficients(vp, oracle, built_lib):
+    fs, p = vp.configs.tangle20k()
+    fs = fs[:20]
+    _, _, cache = gpu_fields(vp, p, fs)
+    lr = vp.get_longrange_field_fourier(cache)
+    assert lr["state"].quantity == "vorticity"
+    o = oracle.point_data(p, fs)
+    uo = oracle.vorticity_fourier(p, o["points"], o["charges"])  # [3, Ns2, Ns1, nkx]
+    ug = np.stack([c.transpose(2, 1, 0) for c in lr["field"]])
+    assert np.linalg.norm(ug - uo) / np.linalg.norm(uo) < TOL
+    kx, ky, kz = lr["wavenumbers"]
+    assert kx[-1] > 0 and len(ky) == p.splitting.Ns[1]
+
+
+def test_open_domain_ring_analytic(vp, oracle, built_lib):
+    """NoSplitting on the GPU (naive pair kernel): test/ring.jl analytic answers."""
+    R, N, Gamma, a, Delta = math.pi / 3, 32, 2.4, 1e-6, 0.25
+    f = vp.curves.ring(N, R, center=(math.pi,) * 3)
+    p = vp.ParamsBiotSavart(Gamma=Gamma, a=a, Delta=Delta, alpha=0, quadrature=vp.GaussLegendre(4),
+                            lia_segment_fraction=0.4)
+    v, psi, _ = gpu_fields(vp, p, [f])
+    vo, po, _ = oracle.compute_on_nodes(p, [f], streamfunction=True)
+    assert rel(v, vo) < TOL and rel(psi, po) < TOL
+    U = np.linalg.norm(v.mean(axis=0))
+    Uex = Gamma / (4 * math.pi * R) * (math.log(8 * R / a) - Delta)
+    assert abs(U - Uex) / Uex < 1e-4
+
+
+def test_set_points_plugin_contract(vp, oracle, built_lib):
+    """Point data computed by the caller (host add_point_charges!), as in the reference plugin API."""
+    fs, p = vp.configs.tangle20k()
+    fs = fs[:15]
+    pd = oracle.point_data(p, fs)
+    cache = vp.init_cache(p)
+    cache.set_points(pd)
+    cache.compute(3)
+    v = cache.get(1)
+    psi = cache.get(2)
+    vo, po, _ = oracle.compute_on_nodes(p, fs, streamfunction=True)
+    assert rel(v, vo) < TOL and rel(psi, po) < TOL
+
+
+def test_integration_cutoff(vp, oracle, built_lib):
+    fs, p = vp.configs.ring64()
+    v1, _, _ = gpu_fields(vp, p, fs, LIA="only")
+    v2, _, _ = gpu_fields(vp, p, fs, LIA="only", integration_cutoff=1e-3)
+    # ln(delta / r) scaling: v ~ ln(delta / r_cut)
+    assert np.all(np.abs(v2[:, 2]) < np.abs(v1[:, 2]))
+
+
+def test_ragged_sizes_and_reuse(vp, oracle, built_lib):
+    fs, p = vp.configs.tangle20k()
+    cache = vp.init_cache(p)
+    for sub in (fs[:3] + [vp.curves.ring(5, 0.4, center=(3, 3, 3))], fs[:40], fs[:2]):
+        vs = [np.zeros_like(f) for f in sub]
+        vp.velocity_on_nodes_(vs, cache, sub)
+        vo, _, _ = oracle.compute_on_nodes(p, sub)
+        assert rel(np.concatenate(vs), vo) < TOL
+
+
+def test_repeatable(vp, built_lib):
+    fs, p = vp.configs.tangle20k()
+    fs = fs[:20]
+    cache = vp.init_cache(p)
+    a = np.concatenate(vp.velocity_on_nodes(cache, fs))
+    b = np.concatenate(vp.velocity_on_nodes(cache, fs))
+    assert rel(a, b) < 1e-14
+
+
+def test_errors_surface(vp, built_lib):
+    fs, p = vp.configs.ring64()
+    cache = vp.init_cache(p)
+    with pytest.raises(vp.VpbsError, match="no point data"):
+        cache.compute(1)
+    with pytest.raises(vp.VpbsError, match="at least 5 nodes"):
+        cache.set_filaments([vp.curves.ring(4, 0.5, center=(3, 3, 3))])
+    with pytest.raises(ValueError, match="not recognised"):
+        vp.compute_on_nodes_({"vorticity": [np.zeros_like(fs[0])]}, cache, fs)

@@ -1,0 +1,20 @@
+"""CUDA (sm_100a) drop-in for VortexPasta.BiotSavart's Ewald-split velocity and
+streamfunction evaluation on vortex-filament nodes.
+
+The compute path is libvpbs.so (C ABI in include/vpbs.h); this package mirrors the
+reference's BiotSavart API on top of it.
+"""
+
+from . import configs, curves
+from ._lib import LIB_PATH, VpbsError
+from .biotsavart import (BiotSavartCache, LongRangeCacheState, compute_on_nodes_, get_longrange_field_fourier,
+                         init_cache, velocity_on_nodes, velocity_on_nodes_)
+from .params import (CellListsBackend, GaussianSplitting, GaussLegendre, NaiveShortRangeBackend, NonuniformFFTsBackend,
+                     NoSplitting, ParamsBiotSavart, kmax_to_gridsize, maximum_wavenumber)
+
+__all__ = [
+    "configs", "curves", "LIB_PATH", "VpbsError", "BiotSavartCache", "LongRangeCacheState", "compute_on_nodes_",
+    "get_longrange_field_fourier", "init_cache", "velocity_on_nodes", "velocity_on_nodes_", "CellListsBackend",
+    "GaussianSplitting", "GaussLegendre", "NaiveShortRangeBackend", "NonuniformFFTsBackend", "NoSplitting",
+    "ParamsBiotSavart", "kmax_to_gridsize", "maximum_wavenumber",
+]

@@ -1,0 +1,102 @@
+"""ctypes binding of libvpbs.so (the C ABI declared in include/vpbs.h).
+
+There is no fallback: if the shared library is missing or no CUDA device is usable, every
+call raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libvpbs.so"
+
+VELOCITY = 1
+STREAMFUNCTION = 2
+LIA_FALSE, LIA_TRUE, LIA_ONLY = 0, 1, 2
+PRECISION = {"fp64": 0, "mixed": 1}
+
+c_double_p = ct.POINTER(ct.c_double)
+c_int32_p = ct.POINTER(ct.c_int32)
+c_int64_p = ct.POINTER(ct.c_int64)
+
+
+class VpbsParams(ct.Structure):
+    _fields_ = [
+        ("Gamma", ct.c_double), ("a", ct.c_double), ("Delta", ct.c_double),
+        ("L", ct.c_double * 3), ("alpha", ct.c_double), ("rcut", ct.c_double),
+        ("Ns", ct.c_int32 * 3), ("sigma", ct.c_double), ("m", ct.c_int32),
+        ("nquad", ct.c_int32), ("quad_zeta", ct.c_double * 16), ("quad_w", ct.c_double * 16),
+        ("nquad_near", ct.c_int32), ("quad_near_zeta", ct.c_double * 16), ("quad_near_w", ct.c_double * 16),
+        ("lia_segment_fraction", ct.c_double), ("avoid_explicit_erf", ct.c_int32),
+        ("truncate_spherical", ct.c_int32), ("nsubdiv", ct.c_int32), ("precision", ct.c_int32),
+        ("device", ct.c_int32),
+    ]
+
+
+class CVec3(ct.Structure):
+    _fields_ = [("x", c_double_p), ("y", c_double_p), ("z", c_double_p)]
+
+
+# name -> (restype, argtypes); every function of include/vpbs.h
+SIGNATURES = {
+    "vpbs_create": (ct.c_int, [ct.POINTER(VpbsParams), ct.POINTER(ct.c_void_p)]),
+    "vpbs_destroy": (ct.c_int, [ct.c_void_p]),
+    "vpbs_last_error": (ct.c_char_p, [ct.c_void_p]),
+    "vpbs_set_stream": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
+    "vpbs_set_filaments": (ct.c_int, [ct.c_void_p, ct.c_int64, c_int64_p, ct.c_void_p, ct.c_int32]),
+    "vpbs_set_points": (ct.c_int, [ct.c_void_p, ct.c_int64, CVec3, c_int32_p, CVec3, CVec3, c_double_p, c_double_p,
+                                   CVec3, CVec3]),
+    "vpbs_compute": (ct.c_int, [ct.c_void_p, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_double]),
+    "vpbs_get": (ct.c_int, [ct.c_void_p, ct.c_int32, c_double_p, ct.c_int32]),
+    "vpbs_get_soa": (ct.c_int, [ct.c_void_p, ct.c_int32, CVec3, ct.c_int32]),
+    "vpbs_device_field": (ct.c_int, [ct.c_void_p, ct.c_int32, ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_void_p),
+                                     ct.POINTER(ct.c_void_p)]),
+    "vpbs_get_uhat": (ct.c_int, [ct.c_void_p, c_double_p, ct.c_int64]),
+    "vpbs_pair_counts": (ct.c_int, [ct.c_void_p, c_int64_p, c_int64_p]),
+    "vpbs_get_pointdata": (ct.c_int, [ct.c_void_p, ct.c_int32, ct.c_void_p, ct.c_int64]),
+    "vpbs_fft_size": (ct.c_int32, [ct.c_int32, ct.c_double]),
+    "vpbs_launch_count": (ct.c_int64, [ct.c_void_p]),
+    "vpbs_stage_timing": (ct.c_int, [ct.c_void_p, ct.c_int32]),
+    "vpbs_stage_times": (ct.c_int, [ct.c_void_p, c_double_p, ct.c_int32]),
+    "vpbs_stage_name": (ct.c_char_p, [ct.c_int32]),
+    "vpbs_fma_throughput": (ct.c_int, [ct.c_int32, ct.c_int32, c_double_p]),
+}
+
+NUM_STAGES = 9
+
+_lib = None
+
+
+def load(path: Path | str | None = None):
+    """Load libvpbs.so and declare its prototypes (raises if the library is missing)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"libvpbs.so not found at {p}; build it with vortexpasta.jl_b200/build.py")
+    lib = ct.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class VpbsError(RuntimeError):
+    pass
+
+
+def check(rc: int, handle=None, what: str = ""):
+    if rc != 0:
+        lib = load()
+        msg = lib.vpbs_last_error(handle)
+        raise VpbsError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+
+def dptr(a):
+    """ctypes double* of a contiguous float64 numpy array."""
+    return a.ctypes.data_as(c_double_p)

@@ -1,0 +1,263 @@
+"""Host-side mirror of VortexPasta.BiotSavart's public API on top of libvpbs.so.
+
+``init_cache``, ``velocity_on_nodes(_)``, ``compute_on_nodes_`` and
+``get_longrange_field_fourier`` keep the reference's names, argument meaning and error
+behaviour (src/BiotSavart/BiotSavart.jl:85-161, 288-612; cache.jl:40-83). A trailing
+underscore stands for Julia's ``!`` (the outputs are overwritten in place).
+
+Filaments are closed curves given as ``(N, 3)`` float64 node arrays (N >= 5, quintic
+splines with chordal knots as in the reference's defaults); fields are lists of
+``(N, 3)`` arrays, one per filament.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+
+from . import _lib
+from .curves import concat
+from .params import NoSplitting, ParamsBiotSavart
+
+
+def _c_params(p: ParamsBiotSavart) -> _lib.VpbsParams:
+    c = _lib.VpbsParams()
+    c.Gamma, c.a, c.Delta = p.Gamma, p.a, p.Delta
+    sp = p.splitting
+    if isinstance(sp, NoSplitting):
+        c.alpha = 0.0
+        c.rcut = 0.0
+        for d in range(3):
+            c.L[d] = 0.0
+            c.Ns[d] = 0
+    else:
+        c.alpha, c.rcut = sp.alpha, sp.rcut
+        for d in range(3):
+            c.L[d] = sp.Ls[d]
+            c.Ns[d] = sp.Ns[d]
+    c.sigma = p.backend_long.sigma
+    c.m = p.backend_long.m
+    z, w = p.quadrature.rule()
+    c.nquad = len(z)
+    for q in range(len(z)):
+        c.quad_zeta[q], c.quad_w[q] = z[q], w[q]
+    zn, wn = p.quadrature_near_singularity.rule()
+    c.nquad_near = len(zn)
+    for q in range(len(zn)):
+        c.quad_near_zeta[q], c.quad_near_w[q] = zn[q], wn[q]
+    c.lia_segment_fraction = p.lia_segment_fraction if p.lia_segment_fraction is not None else 0.0
+    c.avoid_explicit_erf = int(p.avoid_explicit_erf)
+    c.truncate_spherical = int(p.longrange_truncate_spherical)
+    c.nsubdiv = getattr(p.backend_short, "nsubdiv", 0)  # 0: NaiveShortRangeBackend
+    c.precision = _lib.PRECISION[p.precision]
+    c.device = p.device
+    return c
+
+
+class LongRangeCacheState:
+    """longrange/cache_common.jl:17-31."""
+
+    def __init__(self, quantity="undef", smoothing_scale=0.0):
+        self.quantity = quantity
+        self.smoothing_scale = smoothing_scale
+
+    def __repr__(self):
+        return f"LongRangeCacheState(quantity = {self.quantity}, smoothing_scale = {self.smoothing_scale})"
+
+
+class BiotSavartCache:
+    """Owns one libvpbs handle (device memory, cuFFT plans, stream, pinned staging)."""
+
+    def __init__(self, params: ParamsBiotSavart):
+        self.params = params
+        self._lib = _lib.load()
+        self._cparams = _c_params(params)
+        h = ct.c_void_p()
+        rc = self._lib.vpbs_create(ct.byref(self._cparams), ct.byref(h))
+        _lib.check(rc, None, "init_cache")
+        self._h = h
+        self.state = LongRangeCacheState()
+        self.Np = 0
+        self._out = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.vpbs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr: int | None):
+        _lib.check(self._lib.vpbs_set_stream(self._h, ct.c_void_p(stream_ptr or 0)), self._h, "set_stream")
+
+    def set_filaments(self, fs, on_device_ptr: int | None = None, offsets=None):
+        """add_point_charges! on the device. `fs`: list of (N, 3) arrays, or None with a device
+        pointer to AoS nodes plus host `offsets`."""
+        if on_device_ptr is None:
+            nodes, offsets = concat(fs)
+            rc = self._lib.vpbs_set_filaments(self._h, len(offsets) - 1, offsets.ctypes.data_as(_lib.c_int64_p),
+                                              nodes.ctypes.data_as(ct.c_void_p), 0)
+        else:
+            offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+            rc = self._lib.vpbs_set_filaments(self._h, len(offsets) - 1, offsets.ctypes.data_as(_lib.c_int64_p),
+                                              ct.c_void_p(on_device_ptr), 1)
+        _lib.check(rc, self._h, "add_point_charges!")
+        self.Np = int(offsets[-1])
+        self._offsets = np.asarray(offsets)
+
+    def compute(self, fields_mask: int, lia_mode: int = _lib.LIA_TRUE, shortrange=True, longrange=True,
+                integration_cutoff=None):
+        rc = self._lib.vpbs_compute(self._h, fields_mask, lia_mode, int(bool(shortrange)), int(bool(longrange)),
+                                    0.0 if integration_cutoff is None else float(integration_cutoff))
+        _lib.check(rc, self._h, "compute_on_nodes!")
+        if longrange and lia_mode != _lib.LIA_ONLY and self.params.is_periodic:
+            self.state = LongRangeCacheState("vorticity", 0.0)
+
+    def get(self, field_mask: int, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.Np, 3))
+        rc = self._lib.vpbs_get(self._h, field_mask, _lib.dptr(out), 0)
+        _lib.check(rc, self._h, "copy_output_values_on_nodes!")
+        return out
+
+    def device_field(self, field_mask: int):
+        x, y, z = ct.c_void_p(), ct.c_void_p(), ct.c_void_p()
+        _lib.check(self._lib.vpbs_device_field(self._h, field_mask, ct.byref(x), ct.byref(y), ct.byref(z)),
+                   self._h, "device_field")
+        return x.value, y.value, z.value
+
+    def pair_counts(self):
+        a, b = ct.c_int64(), ct.c_int64()
+        _lib.check(self._lib.vpbs_pair_counts(self._h, ct.byref(a), ct.byref(b)), self._h, "pair_counts")
+        return a.value, b.value
+
+    def launch_count(self) -> int:
+        return int(self._lib.vpbs_launch_count(self._h))
+
+    def stage_timing(self, enable: bool = True):
+        _lib.check(self._lib.vpbs_stage_timing(self._h, int(enable)), self._h, "stage_timing")
+
+    def stage_times(self) -> dict:
+        """Milliseconds per stage since the previous query (CUDA events on the handle's stream)."""
+        buf = np.zeros(_lib.NUM_STAGES)
+        _lib.check(self._lib.vpbs_stage_times(self._h, _lib.dptr(buf), _lib.NUM_STAGES), self._h, "stage_times")
+        return {self._lib.vpbs_stage_name(i).decode(): float(buf[i]) for i in range(_lib.NUM_STAGES)}
+
+    def pointdata(self) -> dict:
+        """Device point data (cache.pointdata of the reference) as AoS numpy arrays."""
+        Np = self.Np
+        Nq = Np * len(self.params.quadrature)
+        out = {}
+        for which, name, n in ((0, "nodes", Np), (1, "d1", Np), (2, "d2", Np), (5, "points", Nq), (6, "charges", Nq)):
+            buf = np.empty(3 * n)
+            _lib.check(self._lib.vpbs_get_pointdata(self._h, which, buf.ctypes.data_as(ct.c_void_p), 3 * n),
+                       self._h, "get_pointdata")
+            out[name] = buf.reshape(3, n).T.copy()
+        for which, name in ((3, "dm"), (4, "dp")):
+            buf = np.empty(Np)
+            _lib.check(self._lib.vpbs_get_pointdata(self._h, which, buf.ctypes.data_as(ct.c_void_p), Np),
+                       self._h, "get_pointdata")
+            out[name] = buf
+        idx = np.empty(Np, dtype=np.int32)
+        _lib.check(self._lib.vpbs_get_pointdata(self._h, 7, idx.ctypes.data_as(ct.c_void_p), Np), self._h,
+                   "get_pointdata")
+        out["idx_prev"] = idx
+        return out
+
+    def set_points(self, pd: dict):
+        """Plugin-contract input: PointData arrays (AoS [.,3]; idx_prev 0-based here, passed
+        1-based to the C ABI as in the reference)."""
+        def soa(a):
+            a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).T)
+            return a, _lib.CVec3(_lib.dptr(a[0]), _lib.dptr(a[1]), _lib.dptr(a[2]))
+        keep = {k: soa(pd[k]) for k in ("nodes", "d1", "d2", "points", "charges")}
+        idx1 = np.ascontiguousarray(pd["idx_prev"], dtype=np.int32) + 1
+        dm = np.ascontiguousarray(pd["dm"], dtype=np.float64)
+        dp = np.ascontiguousarray(pd["dp"], dtype=np.float64)
+        Np = len(dm)
+        rc = self._lib.vpbs_set_points(self._h, Np, keep["nodes"][1], idx1.ctypes.data_as(_lib.c_int32_p),
+                                       keep["d1"][1], keep["d2"][1], _lib.dptr(dm), _lib.dptr(dp),
+                                       keep["points"][1], keep["charges"][1])
+        _lib.check(rc, self._h, "set_points")
+        self.Np = Np
+        self._offsets = np.array([0, Np])
+
+
+def init_cache(params: ParamsBiotSavart, fs=None) -> BiotSavartCache:
+    """BiotSavart.init_cache (src/BiotSavart/cache.jl:40-49)."""
+    return BiotSavartCache(params)
+
+
+def _lia_mode(LIA) -> int:
+    if LIA is True:
+        return _lib.LIA_TRUE
+    if LIA is False:
+        return _lib.LIA_FALSE
+    if LIA == "only":
+        return _lib.LIA_ONLY
+    raise ValueError("LIA must be True, False or 'only'")
+
+
+def compute_on_nodes_(fields: dict, cache: BiotSavartCache, fs, *, LIA=True, shortrange=True, longrange=True,
+                      integration_cutoff=None, callback_vorticity=None):
+    """compute_on_nodes! (src/BiotSavart/BiotSavart.jl:395-612): overwrite `fields`
+    (keys "velocity" and/or "streamfunction", each a list of (N_f, 3) arrays)."""
+    names = set(fields)
+    if not names or not names <= {"velocity", "streamfunction"}:
+        raise ValueError(f"some of these fields were not recognised: {tuple(fields)}")
+    for us in fields.values():
+        if len(us) != len(fs):
+            raise ValueError("wrong dimensions of vector")
+        for u, f in zip(us, fs):
+            if np.shape(u) != np.shape(f):
+                raise ValueError("wrong dimensions of vector")
+    mask = (_lib.VELOCITY if "velocity" in names else 0) | (_lib.STREAMFUNCTION if "streamfunction" in names else 0)
+    cache.set_filaments(fs)
+    cache.compute(mask, _lia_mode(LIA), shortrange, longrange, integration_cutoff)
+    if callback_vorticity is not None and longrange and LIA != "only" and cache.params.is_periodic:
+        callback_vorticity(cache)
+    for name, bit in (("velocity", _lib.VELOCITY), ("streamfunction", _lib.STREAMFUNCTION)):
+        if name in names:
+            flat = cache.get(bit)
+            off = cache._offsets
+            for k, u in enumerate(fields[name]):
+                u[...] = flat[off[k]:off[k + 1]]
+    return fields
+
+
+def velocity_on_nodes_(vs, cache: BiotSavartCache, fs, **kws):
+    """velocity_on_nodes! (src/BiotSavart/BiotSavart.jl:152-161)."""
+    compute_on_nodes_({"velocity": vs}, cache, fs, **kws)
+    return vs
+
+
+def velocity_on_nodes(cache: BiotSavartCache, fs, **kws):
+    """velocity_on_nodes (src/BiotSavart/BiotSavart.jl:94-102)."""
+    vs = [np.empty_like(np.asarray(f, dtype=np.float64)) for f in fs]
+    return velocity_on_nodes_(vs, cache, fs, **kws)
+
+
+def get_longrange_field_fourier(cache: BiotSavartCache):
+    """get_longrange_field_fourier (src/BiotSavart/cache.jl:72-83): returns
+    ``{"field": (ux, uy, uz), "wavenumbers": (kx, ky, kz), "state": LongRangeCacheState}``
+    with each component a complex array of shape (Ns0/2+1, Ns1, Ns2) (x first, as in Julia)."""
+    sp = cache.params.splitting
+    Ns = sp.Ns
+    nkx = Ns[0] // 2 + 1
+    buf = np.empty(2 * 3 * nkx * Ns[1] * Ns[2])
+    _lib.check(cache._lib.vpbs_get_uhat(cache.handle, _lib.dptr(buf), buf.size), cache.handle, "get_uhat")
+    u = buf.view(np.complex128).reshape(3, Ns[2], Ns[1], nkx)
+    field = tuple(np.ascontiguousarray(u[c].transpose(2, 1, 0)) for c in range(3))
+    ks = (np.fft.rfftfreq(Ns[0], 1 / Ns[0]) * 2 * np.pi / sp.Ls[0],
+          np.fft.fftfreq(Ns[1], 1 / Ns[1]) * 2 * np.pi / sp.Ls[1],
+          np.fft.fftfreq(Ns[2], 1 / Ns[2]) * 2 * np.pi / sp.Ls[2])
+    return {"field": field, "wavenumbers": ks, "state": LongRangeCacheState(cache.state.quantity, 0.0)}

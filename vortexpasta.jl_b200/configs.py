@@ -1,0 +1,51 @@
+"""Named workloads: the vortex configurations and Biot-Savart parameters the tests and the
+benchmark run on.
+
+* ``ring64``: single ring, L = 2 pi, R = L/4 at the box centre, N = 64 nodes, quintic
+  splines, GL(3), Gamma = 1, a = 1e-8, Delta = 1/4, Gaussian splitting with beta = 3.5 and
+  r_cut = L/4 (alpha = 2.228), Ns = 32 (oversampled FFT grid 48^3), NUFFT m = 4.
+* ``tangle20k``: 100 random perturbed rings x 200 nodes (20,000 nodes), r_cut = L/8,
+  beta = 3.5 (alpha = 4.456), Ns = 128 (FFT grid 192^3), m = 4.
+* ``tangle1m``: 5000 rings x 200 nodes (1,000,000 nodes), r_cut = L/16, beta = 4
+  (alpha = 10.19), Ns = 512 (FFT grid 768^3), m = 5.
+
+The ring generator is the benchmark's RandomRings shape (benchmark/benchmarks.jl:48-66) with
+radial Fourier perturbations of modes 2..8; seeds are fixed.
+"""
+
+from __future__ import annotations
+
+import math
+
+from . import curves
+from .params import GaussianSplitting, GaussLegendre, NonuniformFFTsBackend, ParamsBiotSavart
+
+L = 2 * math.pi
+
+
+def params_for(rcut: float, beta: float, Ns: int, m: int, precision: str = "fp64", **kw) -> ParamsBiotSavart:
+    alpha = beta / rcut
+    return ParamsBiotSavart(Gamma=1.0, a=1e-8, Delta=0.25,
+                            splitting=GaussianSplitting(Ls=L, alpha=alpha, rcut=rcut, Ns=Ns),
+                            quadrature=GaussLegendre(3), backend_long=NonuniformFFTsBackend(1.5, m),
+                            precision=precision, **kw)
+
+
+def ring64(**kw):
+    fs = [curves.ring(64, L / 4, center=(L / 2, L / 2, L / 2))]
+    return fs, params_for(L / 4, 3.5, 32, 4, **kw)
+
+
+def tangle(nrings: int, nodes_per_ring: int = 200, seed: int = 42):
+    return curves.random_tangle(nrings, nodes_per_ring, L=L, seed=seed)
+
+
+def tangle20k(seed: int = 42, **kw):
+    return tangle(100, 200, seed), params_for(L / 8, 3.5, 128, 4, **kw)
+
+
+def tangle1m(seed: int = 42, **kw):
+    return tangle(5000, 200, seed), params_for(L / 16, 4.0, 512, 5, **kw)
+
+
+WORKLOADS = {"ring64": ring64, "tangle20k": tangle20k, "tangle1m": tangle1m}

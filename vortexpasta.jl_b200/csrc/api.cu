@@ -1,0 +1,542 @@
+// C ABI of libvpbs.so: handle life cycle, parameter validation, host <-> device staging and
+// the compute_on_nodes! orchestration (src/BiotSavart/BiotSavart.jl:395-612).
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "vpbs_internal.cuh"
+
+namespace {
+thread_local std::string g_create_error;
+}
+
+namespace vpbs {
+
+int set_error(vpbs_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+int check_cuda(vpbs_handle* h, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return 0;
+    return set_error(h, e == cudaErrorMemoryAllocation ? VPBS_ERR_OOM : VPBS_ERR_CUDA,
+                     std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+int ensure(vpbs_handle* h, DevBuf& b, size_t bytes, const char* what) {
+    if (bytes == 0) bytes = 8;
+    if (b.bytes >= bytes) return 0;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return set_error(h, VPBS_ERR_OOM, std::string("device allocation of ") + std::to_string(bytes) + " bytes failed (" +
+                                              what + "): " + cudaGetErrorString(e));
+    }
+    b.bytes = bytes;
+    return 0;
+}
+
+int ensure_pinned(vpbs_handle* h, void** buf, size_t* cap, size_t bytes) {
+    if (*cap >= bytes) return 0;
+    if (*buf) cudaFreeHost(*buf);
+    *buf = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaHostAlloc(buf, bytes, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        *buf = nullptr;
+        return set_error(h, VPBS_ERR_OOM, std::string("pinned host allocation failed: ") + cudaGetErrorString(e));
+    }
+    *cap = bytes;
+    return 0;
+}
+
+static void free_buf(DevBuf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+static int activate(vpbs_handle* h) { return check_cuda(h, cudaSetDevice(h->device), "cudaSetDevice"); }
+
+// Allocate point-data and output buffers for Np nodes.
+static int alloc_points(vpbs_handle* h, int64_t Np) {
+    const int64_t Nq = Np * h->K.nquad;
+    int rc;
+    if ((rc = ensure(h, h->nodes, sizeof(double) * 3 * Np, "nodes"))) return rc;
+    if ((rc = ensure(h, h->idx_prev, sizeof(int32_t) * Np, "node_idx_prev"))) return rc;
+    if ((rc = ensure(h, h->d1, sizeof(double) * 3 * Np, "derivatives"))) return rc;
+    if ((rc = ensure(h, h->d2, sizeof(double) * 3 * Np, "derivatives"))) return rc;
+    if ((rc = ensure(h, h->dm, sizeof(double) * Np, "subsegment lengths"))) return rc;
+    if ((rc = ensure(h, h->dp, sizeof(double) * Np, "subsegment lengths"))) return rc;
+    if ((rc = ensure(h, h->points, sizeof(double) * 3 * Nq, "points"))) return rc;
+    if ((rc = ensure(h, h->charges, sizeof(double) * 3 * Nq, "charges"))) return rc;
+    if ((rc = ensure(h, h->li_vel, sizeof(double) * 3 * Np, "local integrals"))) return rc;
+    if ((rc = ensure(h, h->li_psi, sizeof(double) * 3 * Np, "local integrals"))) return rc;
+    if ((rc = ensure(h, h->vel, sizeof(double) * 3 * Np, "velocity"))) return rc;
+    if ((rc = ensure(h, h->psi, sizeof(double) * 3 * Np, "streamfunction"))) return rc;
+    h->Np = Np;
+    h->Nq = Nq;
+    return 0;
+}
+
+static int process_point_charges(vpbs_handle* h) {
+    // process_point_charges! of both backends: cell lists (cell_lists.jl:117-127); the long-range
+    // rescaling to [0, 2 pi) (longrange.jl:409-471) is folded into the NUFFT kernels.
+    int rc = build_cell_lists(h);
+    if (rc) return rc;
+    h->have_points = true;
+    h->have_uhat = false;
+    return 0;
+}
+
+}  // namespace vpbs
+
+using namespace vpbs;
+
+extern "C" {
+
+const char* vpbs_last_error(const vpbs_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
+    if (!params || !out) return set_error(nullptr, VPBS_ERR_ARG, "null argument to vpbs_create");
+    *out = nullptr;
+    const vpbs_params& P = *params;
+    if (!(P.a > 0) || !std::isfinite(P.Gamma))
+        return set_error(nullptr, VPBS_ERR_PARAMS, "vortex core size `a` must be positive and `Gamma` finite");
+    if (P.nquad < 1 || P.nquad > kMaxQuad)
+        return set_error(nullptr, VPBS_ERR_PARAMS, "nquad must be in 1:16");
+    if (P.nquad_near < 0 || P.nquad_near > kMaxQuad)
+        return set_error(nullptr, VPBS_ERR_PARAMS, "nquad_near must be in 0:16");
+    if (P.lia_segment_fraction > 1.0)
+        return set_error(nullptr, VPBS_ERR_PARAMS, "lia_segment_fraction must be in (0, 1]");
+    if (P.precision != VPBS_PRECISION_FP64)
+        return set_error(nullptr, VPBS_ERR_PARAMS, "only the FP64 form (VPBS_PRECISION_FP64) is available in this build");
+    const bool open = !(P.alpha > 0);
+    KParams K{};
+    K.Gamma = P.Gamma;
+    K.a = P.a;
+    K.Delta = P.Delta;
+    K.alpha = open ? 0.0 : P.alpha;
+    K.open_domain = open ? 1 : 0;
+    K.nquad = P.nquad;
+    K.nquad_near = P.nquad_near > 0 ? P.nquad_near : P.nquad;
+    for (int q = 0; q < P.nquad; ++q) { K.qz[q] = P.quad_zeta[q]; K.qw[q] = P.quad_w[q]; }
+    for (int q = 0; q < K.nquad_near; ++q) {
+        K.qnz[q] = P.nquad_near > 0 ? P.quad_near_zeta[q] : P.quad_zeta[q];
+        K.qnw[q] = P.nquad_near > 0 ? P.quad_near_w[q] : P.quad_w[q];
+    }
+    K.lia_fraction = P.lia_segment_fraction > 0 ? P.lia_segment_fraction : 0.0;
+    K.avoid_explicit_erf = P.avoid_explicit_erf;
+    CellGrid cg{};
+    if (open) {
+        for (int d = 0; d < 3; ++d) { K.L[d] = 0.0; K.Lh[d] = 0.0; }
+        K.rcut = INFINITY;
+        K.rcut2 = INFINITY;
+        if (!P.avoid_explicit_erf)
+            return set_error(nullptr, VPBS_ERR_PARAMS, "avoid_explicit_erf = false requires Ewald splitting");
+    } else {
+        for (int d = 0; d < 3; ++d) {
+            if (!(P.L[d] > 0)) return set_error(nullptr, VPBS_ERR_PARAMS, "periods L must be positive");
+            K.L[d] = P.L[d];
+            K.Lh[d] = P.L[d] / 2;
+        }
+        if (!(P.rcut > 0)) return set_error(nullptr, VPBS_ERR_PARAMS, "cutoff distance rcut must be positive");
+        const double Lmin = std::fmin(P.L[0], std::fmin(P.L[1], P.L[2]));
+        const int M = P.nsubdiv;  // 0 selects the naive (all pairs) short-range backend
+        if (M < 0) return set_error(nullptr, VPBS_ERR_PARAMS, "nsubdiv must be >= 0");
+        // params.jl:99-106, CellLists.jl:135-147 and naive.jl:8-16
+        const double rmax = M > 0 ? (double)M / (2.0 * M + 1.0) * Lmin : 0.5 * Lmin;
+        if (P.rcut > rmax)
+            return set_error(nullptr, VPBS_ERR_PARAMS,
+                             "cutoff distance `rcut = " + std::to_string(P.rcut) + "` is larger than that allowed by the " +
+                                 (M > 0 ? "CellListsBackend{" + std::to_string(M) + "} backend (rcut <= M / (2M + 1) * L)"
+                                        : std::string("NaiveShortRangeBackend backend (rcut <= L / 2)")));
+        if (!(2 * P.rcut <= Lmin))
+            return set_error(nullptr, VPBS_ERR_PARAMS, "cutoff distance `rcut` is too large. It must be less than half the cell unit size `L` in each direction");
+        K.rcut = P.rcut;
+        K.rcut2 = P.rcut * P.rcut;
+        cg.M = M;
+        for (int d = 0; d < 3; ++d) {
+            // with M = 0 the cells only order the points (spatial locality); pairs are not culled
+            cg.nc[d] = M > 0 ? (int)std::floor(P.L[d] * M / P.rcut) : (int)std::fmax(1.0, std::floor(P.L[d] / P.rcut));
+            if (M > 0 && cg.nc[d] < 2 * M + 1)
+                return set_error(nullptr, VPBS_ERR_PARAMS, "cell lists: the cut-off distance r_cut is too large for periodic padding");
+        }
+        cg.ncell = (int64_t)cg.nc[0] * cg.nc[1] * cg.nc[2];
+        if (cg.ncell > (int64_t)1 << 30) return set_error(nullptr, VPBS_ERR_PARAMS, "too many cells (rcut too small)");
+        if (!(P.sigma > 1.0)) return set_error(nullptr, VPBS_ERR_PARAMS, "NUFFT oversampling factor sigma must be > 1");
+        if (P.m < 1 || P.m > kMaxHalfSupport) return set_error(nullptr, VPBS_ERR_PARAMS, "NUFFT half support m must be in 1:8");
+        for (int d = 0; d < 3; ++d) {
+            if (P.Ns[d] < 2) return set_error(nullptr, VPBS_ERR_PARAMS, "Ns must be >= 2 in each direction");
+            if (vpbs_fft_size(P.Ns[d], P.sigma) < 2 * P.m)
+                return set_error(nullptr, VPBS_ERR_PARAMS, "oversampled grid smaller than the NUFFT kernel support");
+        }
+    }
+    vpbs_handle* h = new (std::nothrow) vpbs_handle();
+    if (!h) return set_error(nullptr, VPBS_ERR_OOM, "host allocation failed");
+    h->P = P;
+    h->K = K;
+    h->cg = cg;
+    h->device = P.device;
+    int rc = activate(h);
+    if (!rc) rc = check_cuda(h, cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!rc) rc = check_cuda(h, cudaEventCreateWithFlags(&h->h2d_done, cudaEventDisableTiming), "cudaEventCreate");
+    h->stream = h->own_stream;
+    if (!rc && !open) rc = longrange_init(h);
+    if (rc) {
+        g_create_error = h->err;
+        vpbs_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return 0;
+}
+
+int vpbs_destroy(vpbs_handle* h) {
+    if (!h) return 0;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    longrange_free(h);
+    DevBuf* bufs[] = {&h->nodes_in, &h->offsets, &h->fil_of_node, &h->knots, &h->coefs, &h->dcoef1, &h->dcoef2,
+                      &h->spline_scratch, &h->nodes, &h->idx_prev, &h->d1, &h->d2, &h->dm, &h->dp, &h->points,
+                      &h->charges, &h->li_vel, &h->li_psi, &h->src_cell, &h->src_start, &h->src_fill, &h->src_sorted,
+                      &h->src_seg, &h->dst_cell, &h->dst_start, &h->dst_fill, &h->dst_order, &h->counters,
+                      &h->grid_r, &h->grid_c, &h->grid_c2, &h->uhat, &h->decx, &h->decy, &h->decz, &h->nodes_lr,
+                      &h->vel, &h->psi};
+    for (DevBuf* b : bufs) free_buf(*b);
+    if (h->pin_in) cudaFreeHost(h->pin_in);
+    if (h->pin_out) cudaFreeHost(h->pin_out);
+    if (h->h2d_done) cudaEventDestroy(h->h2d_done);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+    return 0;
+}
+
+int vpbs_set_stream(vpbs_handle* h, void* stream) {
+    if (!h) return VPBS_ERR_ARG;
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    return 0;
+}
+
+int vpbs_set_filaments(vpbs_handle* h, int64_t nfil, const int64_t* offsets, const double* nodes_xyz, int32_t on_device) {
+    if (!h) return VPBS_ERR_ARG;
+    if (nfil < 1 || !offsets || !nodes_xyz) return set_error(h, VPBS_ERR_ARG, "vpbs_set_filaments: bad arguments");
+    if (offsets[0] != 0) return set_error(h, VPBS_ERR_ARG, "offsets[0] must be 0");
+    for (int64_t f = 0; f < nfil; ++f)
+        if (offsets[f + 1] - offsets[f] < 5)
+            return set_error(h, VPBS_ERR_ARG, "each filament needs at least 5 nodes (quintic splines)");
+    const int64_t Np = offsets[nfil];
+    if (Np * h->K.nquad >= ((int64_t)1 << 31)) return set_error(h, VPBS_ERR_ARG, "too many quadrature points");
+    int rc;
+    if ((rc = activate(h))) return rc;
+    if ((rc = alloc_points(h, Np))) return rc;
+    if ((rc = ensure(h, h->offsets, sizeof(int64_t) * (nfil + 1), "offsets"))) return rc;
+    // stage offsets (+ nodes from the host) through pinned memory
+    const size_t bytes_off = sizeof(int64_t) * (nfil + 1);
+    const size_t bytes_nodes = on_device ? 0 : sizeof(double) * 3 * Np;
+    if ((rc = check_cuda(h, cudaEventSynchronize(h->h2d_done), "event sync"))) return rc;
+    if ((rc = ensure_pinned(h, &h->pin_in, &h->pin_in_bytes, bytes_off + bytes_nodes))) return rc;
+    std::memcpy(h->pin_in, offsets, bytes_off);
+    if ((rc = check_cuda(h, cudaMemcpyAsync(h->offsets.p, h->pin_in, bytes_off, cudaMemcpyHostToDevice, h->stream), "H2D offsets")))
+        return rc;
+    const double* d_nodes = nodes_xyz;
+    if (!on_device) {
+        if ((rc = ensure(h, h->nodes_in, bytes_nodes, "input nodes"))) return rc;
+        char* dst = (char*)h->pin_in + bytes_off;
+        std::memcpy(dst, nodes_xyz, bytes_nodes);
+        if ((rc = check_cuda(h, cudaMemcpyAsync(h->nodes_in.p, dst, bytes_nodes, cudaMemcpyHostToDevice, h->stream), "H2D nodes")))
+            return rc;
+        d_nodes = (const double*)h->nodes_in.p;
+    }
+    if ((rc = check_cuda(h, cudaEventRecord(h->h2d_done, h->stream), "event record"))) return rc;
+    h->nfil = nfil;
+    if ((rc = geometry_from_filaments(h, nfil, (const int64_t*)h->offsets.p, d_nodes))) return rc;
+    h->li_valid = h->K.lia_fraction > 0;
+    return process_point_charges(h);
+}
+
+int vpbs_set_points(vpbs_handle* h, int64_t Np, vpbs_cvec3 nodes, const int32_t* node_idx_prev, vpbs_cvec3 deriv1,
+                    vpbs_cvec3 deriv2, const double* delta_minus, const double* delta_plus, vpbs_cvec3 points,
+                    vpbs_cvec3 charges) {
+    if (!h) return VPBS_ERR_ARG;
+    if (Np < 1 || !node_idx_prev || !delta_minus || !delta_plus || !nodes.x || !nodes.y || !nodes.z || !deriv1.x ||
+        !deriv1.y || !deriv1.z || !deriv2.x || !deriv2.y || !deriv2.z || !points.x || !points.y || !points.z ||
+        !charges.x || !charges.y || !charges.z)
+        return set_error(h, VPBS_ERR_ARG, "vpbs_set_points: null pointer or empty point data");
+    if (Np * h->K.nquad >= ((int64_t)1 << 31)) return set_error(h, VPBS_ERR_ARG, "too many quadrature points");
+    int rc;
+    if ((rc = activate(h))) return rc;
+    if ((rc = alloc_points(h, Np))) return rc;
+    const int64_t Nq = h->Nq;
+    const size_t nd = sizeof(double);
+    // layout of the staging buffer: 3Np nodes | 3Np d1 | 3Np d2 | Np dm | Np dp | 3Nq points | 3Nq charges | Np idx
+    const size_t total = nd * (11 * Np + 6 * Nq) + sizeof(int32_t) * Np;
+    if ((rc = check_cuda(h, cudaEventSynchronize(h->h2d_done), "event sync"))) return rc;
+    if ((rc = ensure_pinned(h, &h->pin_in, &h->pin_in_bytes, total))) return rc;
+    double* s = (double*)h->pin_in;
+    const double* vsrc[] = {nodes.x, nodes.y, nodes.z, deriv1.x, deriv1.y, deriv1.z, deriv2.x, deriv2.y, deriv2.z,
+                            delta_minus, delta_plus};
+    for (int k = 0; k < 11; ++k) std::memcpy(s + k * Np, vsrc[k], nd * Np);
+    const double* qsrc[] = {points.x, points.y, points.z, charges.x, charges.y, charges.z};
+    for (int k = 0; k < 6; ++k) std::memcpy(s + 11 * Np + k * Nq, qsrc[k], nd * Nq);
+    int32_t* sidx = (int32_t*)(s + 11 * Np + 6 * Nq);
+    for (int64_t i = 0; i < Np; ++i) {
+        int32_t v = node_idx_prev[i] - 1;  // reference indices are 1-based
+        if (v < 0 || v >= Np) return set_error(h, VPBS_ERR_ARG, "node_idx_prev out of range");
+        sidx[i] = v;
+    }
+    struct { void* dst; const void* src; size_t n; } cp[] = {
+        {h->nodes.p, s, nd * 3 * Np},          {h->d1.p, s + 3 * Np, nd * 3 * Np},
+        {h->d2.p, s + 6 * Np, nd * 3 * Np},    {h->dm.p, s + 9 * Np, nd * Np},
+        {h->dp.p, s + 10 * Np, nd * Np},       {h->points.p, s + 11 * Np, nd * 3 * Nq},
+        {h->charges.p, s + 11 * Np + 3 * Nq, nd * 3 * Nq}, {h->idx_prev.p, sidx, sizeof(int32_t) * Np}};
+    for (auto& c : cp)
+        if ((rc = check_cuda(h, cudaMemcpyAsync(c.dst, c.src, c.n, cudaMemcpyHostToDevice, h->stream), "H2D point data")))
+            return rc;
+    if ((rc = check_cuda(h, cudaEventRecord(h->h2d_done, h->stream), "event record"))) return rc;
+    h->li_valid = false;  // add_local_integrals! stays with the caller in the point-data contract
+    return process_point_charges(h);
+}
+
+int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t shortrange, int32_t longrange,
+                 double integration_cutoff) {
+    if (!h) return VPBS_ERR_ARG;
+    if (fields < 1 || fields > 3) return set_error(h, VPBS_ERR_ARG, "fields must be VELOCITY and/or STREAMFUNCTION");
+    if (lia_mode < 0 || lia_mode > 2) return set_error(h, VPBS_ERR_ARG, "bad LIA mode");
+    if (!h->have_points) return set_error(h, VPBS_ERR_STATE, "no point data: call vpbs_set_filaments or vpbs_set_points first");
+    int rc;
+    if ((rc = activate(h))) return rc;
+    const int64_t Np = h->Np;
+    if (fields & VPBS_VELOCITY)
+        if ((rc = check_cuda(h, cudaMemsetAsync(h->vel.p, 0, sizeof(double) * 3 * Np, h->stream), "memset"))) return rc;
+    if (fields & VPBS_STREAMFUNCTION)
+        if ((rc = check_cuda(h, cudaMemsetAsync(h->psi.p, 0, sizeof(double) * 3 * Np, h->stream), "memset"))) return rc;
+    const bool with_long = longrange && lia_mode != VPBS_LIA_ONLY && !h->K.open_domain;
+    if (with_long)
+        if ((rc = longrange_compute(h, fields))) return rc;
+    if (shortrange) {
+        const bool pairs = lia_mode != VPBS_LIA_ONLY;
+        KParams saved = h->K;
+        if (!h->li_valid) h->K.lia_fraction = 0.0;
+        rc = local_and_self(h, fields, lia_mode, pairs ? 1 : 0, integration_cutoff);
+        h->K = saved;
+        if (rc) return rc;
+        if (pairs)
+            if ((rc = pair_interactions(h, fields))) return rc;
+    }
+    h->last_fields = fields;
+    return 0;
+}
+
+static int fetch_soa(vpbs_handle* h, int32_t field, const double** out) {
+    if (field != VPBS_VELOCITY && field != VPBS_STREAMFUNCTION) return set_error(h, VPBS_ERR_ARG, "bad field");
+    if (!(h->last_fields & field)) return set_error(h, VPBS_ERR_STATE, "field was not computed");
+    int rc;
+    if ((rc = activate(h))) return rc;
+    const size_t bytes = sizeof(double) * 3 * h->Np;
+    if ((rc = ensure_pinned(h, &h->pin_out, &h->pin_out_bytes, bytes))) return rc;
+    const void* src = field == VPBS_VELOCITY ? h->vel.p : h->psi.p;
+    if ((rc = check_cuda(h, cudaMemcpyAsync(h->pin_out, src, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H"))) return rc;
+    if ((rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync"))) return rc;
+    *out = (const double*)h->pin_out;
+    return 0;
+}
+
+int vpbs_get(vpbs_handle* h, int32_t field, double* out_xyz, int32_t accumulate) {
+    if (!h) return VPBS_ERR_ARG;
+    if (!out_xyz) return set_error(h, VPBS_ERR_ARG, "null output");
+    const double* s;
+    int rc = fetch_soa(h, field, &s);
+    if (rc) return rc;
+    const int64_t Np = h->Np;
+    if (accumulate) {
+        for (int64_t i = 0; i < Np; ++i)
+            for (int d = 0; d < 3; ++d) out_xyz[3 * i + d] += s[d * Np + i];
+    } else {
+        for (int64_t i = 0; i < Np; ++i)
+            for (int d = 0; d < 3; ++d) out_xyz[3 * i + d] = s[d * Np + i];
+    }
+    return 0;
+}
+
+int vpbs_get_soa(vpbs_handle* h, int32_t field, vpbs_vec3 out, int32_t accumulate) {
+    if (!h) return VPBS_ERR_ARG;
+    if (!out.x || !out.y || !out.z) return set_error(h, VPBS_ERR_ARG, "null output");
+    const double* s;
+    int rc = fetch_soa(h, field, &s);
+    if (rc) return rc;
+    const int64_t Np = h->Np;
+    double* o[3] = {out.x, out.y, out.z};
+    for (int d = 0; d < 3; ++d) {
+        if (accumulate)
+            for (int64_t i = 0; i < Np; ++i) o[d][i] += s[d * Np + i];
+        else
+            std::memcpy(o[d], s + d * Np, sizeof(double) * Np);
+    }
+    return 0;
+}
+
+int vpbs_device_field(vpbs_handle* h, int32_t field, double** x, double** y, double** z) {
+    if (!h || !x || !y || !z) return VPBS_ERR_ARG;
+    if (field != VPBS_VELOCITY && field != VPBS_STREAMFUNCTION) return set_error(h, VPBS_ERR_ARG, "bad field");
+    double* base = (double*)(field == VPBS_VELOCITY ? h->vel.p : h->psi.p);
+    if (!base) return set_error(h, VPBS_ERR_STATE, "no output allocated");
+    *x = base;
+    *y = base + h->Np;
+    *z = base + 2 * h->Np;
+    return 0;
+}
+
+int vpbs_get_uhat(vpbs_handle* h, double* out, int64_t n_doubles) {
+    if (!h || !out) return VPBS_ERR_ARG;
+    if (h->K.open_domain) return set_error(h, VPBS_ERR_STATE, "no long-range field with NoSplitting");
+    if (n_doubles != 2 * 3 * h->lr.nmodes) return set_error(h, VPBS_ERR_ARG, "wrong output size for uhat");
+    if (!h->have_uhat) return set_error(h, VPBS_ERR_STATE, "long-range field not computed yet");
+    int rc;
+    if ((rc = activate(h))) return rc;
+    if ((rc = check_cuda(h, cudaMemcpyAsync(out, h->uhat.p, sizeof(double) * n_doubles, cudaMemcpyDeviceToHost, h->stream), "D2H uhat")))
+        return rc;
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync");
+}
+
+int vpbs_pair_counts(vpbs_handle* h, int64_t* in_range, int64_t* candidates) {
+    if (!h || !in_range || !candidates) return VPBS_ERR_ARG;
+    if (!h->counters.p) return set_error(h, VPBS_ERR_STATE, "no pair computation yet");
+    unsigned long long c[2];
+    int rc;
+    if ((rc = activate(h))) return rc;
+    if ((rc = check_cuda(h, cudaMemcpyAsync(c, h->counters.p, sizeof c, cudaMemcpyDeviceToHost, h->stream), "D2H counters")))
+        return rc;
+    if ((rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync"))) return rc;
+    *in_range = (int64_t)c[0];
+    *candidates = (int64_t)c[1];
+    return 0;
+}
+
+int vpbs_get_pointdata(vpbs_handle* h, int32_t which, void* out, int64_t n_elems) {
+    if (!h || !out) return VPBS_ERR_ARG;
+    if (!h->have_points) return set_error(h, VPBS_ERR_STATE, "no point data");
+    const int64_t Np = h->Np, Nq = h->Nq;
+    const void* src = nullptr;
+    int64_t n = 0;
+    size_t esz = sizeof(double);
+    switch (which) {
+        case 0: src = h->nodes.p; n = 3 * Np; break;
+        case 1: src = h->d1.p; n = 3 * Np; break;
+        case 2: src = h->d2.p; n = 3 * Np; break;
+        case 3: src = h->dm.p; n = Np; break;
+        case 4: src = h->dp.p; n = Np; break;
+        case 5: src = h->points.p; n = 3 * Nq; break;
+        case 6: src = h->charges.p; n = 3 * Nq; break;
+        case 7: src = h->idx_prev.p; n = Np; esz = sizeof(int32_t); break;
+        default: return set_error(h, VPBS_ERR_ARG, "bad point-data selector");
+    }
+    if (n_elems != n) return set_error(h, VPBS_ERR_ARG, "wrong output size for point data");
+    int rc;
+    if ((rc = activate(h))) return rc;
+    if ((rc = check_cuda(h, cudaMemcpyAsync(out, src, esz * n, cudaMemcpyDeviceToHost, h->stream), "D2H point data")))
+        return rc;
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync");
+}
+
+int64_t vpbs_launch_count(const vpbs_handle* h) { return h ? h->launches : 0; }
+
+int vpbs_stage_timing(vpbs_handle* h, int32_t enable) {
+    if (!h) return VPBS_ERR_ARG;
+    int rc;
+    if ((rc = activate(h))) return rc;
+    if (enable && !h->tev[0][0][0]) {
+        for (int s = 0; s < ST_COUNT; ++s)
+            for (int k = 0; k < 4; ++k)
+                for (int e = 0; e < 2; ++e)
+                    if ((rc = check_cuda(h, cudaEventCreate(&h->tev[s][k][e]), "cudaEventCreate"))) return rc;
+    }
+    h->timing = enable != 0;
+    for (int s = 0; s < ST_COUNT; ++s) h->tcount[s] = 0;
+    return 0;
+}
+
+int vpbs_stage_times(vpbs_handle* h, double* ms, int32_t n) {
+    if (!h || !ms || n < ST_COUNT) return VPBS_ERR_ARG;
+    if (!h->timing) return set_error(h, VPBS_ERR_STATE, "stage timing is not enabled");
+    int rc;
+    if ((rc = activate(h))) return rc;
+    if ((rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync"))) return rc;
+    for (int s = 0; s < ST_COUNT; ++s) {
+        double acc = 0.0;
+        for (int k = 0; k < h->tcount[s] && k < 4; ++k) {
+            float t = 0.f;
+            if ((rc = check_cuda(h, cudaEventElapsedTime(&t, h->tev[s][k][0], h->tev[s][k][1]), "event time"))) return rc;
+            acc += t;
+        }
+        ms[s] = acc;
+        h->tcount[s] = 0;
+    }
+    return 0;
+}
+
+const char* vpbs_stage_name(int32_t i) {
+    static const char* names[ST_COUNT] = {"geometry", "cell_lists", "spread", "fft_forward", "fourier",
+                                          "fft_inverse", "interp", "local_self", "pairs"};
+    return (i >= 0 && i < ST_COUNT) ? names[i] : nullptr;
+}
+
+}  // extern "C"
+
+namespace {
+// Independent FMA chains (8 per thread) to measure the CUDA-core FMA throughput.
+template <typename T>
+__global__ void __launch_bounds__(256) fma_probe_kernel(T* out, int iters, T a, T b) {
+    T x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = (T)(threadIdx.x + k) * (T)1e-3;
+    for (int it = 0; it < iters; ++it)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += x[k];
+    if (s == (T)12345.678) out[threadIdx.x] = s;  // keeps the chains alive
+}
+}  // namespace
+
+extern "C" int vpbs_fma_throughput(int32_t device, int32_t fp64, double* tflops) {
+    if (!tflops) return VPBS_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return set_error(nullptr, VPBS_ERR_CUDA, "cudaSetDevice failed");
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    void* out = nullptr;
+    if (cudaMalloc(&out, 4096) != cudaSuccess) return set_error(nullptr, VPBS_ERR_OOM, "probe allocation failed");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = nsm * 8, iters = fp64 ? 4096 : 16384;
+    double best = 0.0;
+    for (int rep = 0; rep < 4; ++rep) {
+        cudaEventRecord(e0);
+        if (fp64) fma_probe_kernel<double><<<blocks, 256>>>((double*)out, iters, 0.999999, 1e-7);
+        else fma_probe_kernel<float><<<blocks, 256>>>((float*)out, iters, 0.999999f, 1e-7f);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double flops = 2.0 * 8.0 * iters * 256.0 * blocks;
+        if (rep > 0 && ms > 0) best = fmax(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaError_t err = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (err != cudaSuccess) return set_error(nullptr, VPBS_ERR_CUDA, cudaGetErrorString(err));
+    *tflops = best;
+    return 0;
+}
+
+extern "C" {
+
+}  // extern "C"

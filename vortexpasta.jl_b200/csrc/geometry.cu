@@ -1,0 +1,387 @@
+// Filament geometry on the device: chordal knots, periodic quintic spline interpolation and
+// the point data of add_point_charges! (src/BiotSavart/pointdata_impl.jl:41-108).
+//
+// One warp per filament solves the cyclic pentadiagonal B-spline collocation system
+// (src/Filaments/spline/quintic.jl:9-100 solves the same system): the band part is
+// factorised by elimination without pivoting (collocation matrices of B-splines are totally
+// positive), the seven right-hand sides (x, y, z and the four wrap-around columns) are swept
+// by seven lanes in parallel, and the corners are folded back with the Woodbury identity.
+// A second kernel evaluates the splines at the nodes and quadrature points, one thread per node.
+#include "vpbs_internal.cuh"
+
+namespace vpbs {
+namespace {
+
+struct FilView {
+    const double* t;  // knots of this filament (n values, t[0] = 0)
+    double T;         // knot period
+    int n;
+};
+
+__device__ __forceinline__ long pmodl(long j, long n) {
+    long r = j % n;
+    return r < 0 ? r + n : r;
+}
+
+__device__ __forceinline__ double knot_at(const FilView& f, long j) {
+    long n = f.n;
+    long q = (j >= 0) ? j / n : -((-j + n - 1) / n);
+    return f.t[j - q * n] + (double)q * f.T;
+}
+
+// de Boor's BSPLVB: N[s] = B_{i-K+1+s, K}(x) for x in [t_i, t_{i+1}).
+template <int K>
+__device__ __forceinline__ void bsplvb(const FilView& f, long i, double x, double (&N)[K]) {
+    double left[K], right[K];
+    N[0] = 1.0;
+#pragma unroll
+    for (int r = 1; r < K; ++r) {
+        left[r] = x - knot_at(f, i + 1 - r);
+        right[r] = knot_at(f, i + r) - x;
+        double saved = 0.0;
+#pragma unroll
+        for (int s = 0; s < r; ++s) {
+            double tmp = N[s] / (right[s + 1] + left[r - s]);
+            N[s] = saved + right[s + 1] * tmp;
+            saved = left[r - s] * tmp;
+        }
+        N[r] = saved;
+    }
+}
+
+// Spline derivative `D` (0, 1, 2) at local coordinate zeta on segment i.
+// coef: AoS [n][3] coefficients of order 6 - D for this filament.
+template <int D>
+__device__ __forceinline__ void eval_seg(const FilView& f, const double* coef, long i, double zeta, double out[3]) {
+    constexpr int K = 6 - D;
+    double ti = knot_at(f, i), ti1 = knot_at(f, i + 1);
+    double x = (1.0 - zeta) * ti + zeta * ti1;
+    double N[K];
+    bsplvb<K>(f, i, x, N);
+    out[0] = out[1] = out[2] = 0.0;
+#pragma unroll
+    for (int s = 0; s < K; ++s) {
+        long j = pmodl(i - K + 1 + s, f.n);
+        out[0] += coef[3 * j + 0] * N[s];
+        out[1] += coef[3 * j + 1] * N[s];
+        out[2] += coef[3 * j + 2] * N[s];
+    }
+}
+
+__device__ __forceinline__ double fold(double x, double L, int open) {
+    if (open) return x;
+    while (x < 0.0) x += L;
+    while (x >= L) x -= L;
+    return x;
+}
+
+__device__ __forceinline__ double deper(double r, double L, double Lh, int open) {
+    if (open) return r;
+    r = (r >= Lh) ? r - L : r;
+    r = (r < -Lh) ? r + L : r;
+    return r;
+}
+
+// Solve the 4x4 Woodbury capacitance system with partial pivoting (3 right-hand sides).
+__device__ void solve4(double H[4][4], double r[4][3]) {
+    for (int c = 0; c < 4; ++c) {
+        int piv = c;
+        for (int i = c + 1; i < 4; ++i)
+            if (fabs(H[i][c]) > fabs(H[piv][c])) piv = i;
+        if (piv != c) {
+            for (int j = 0; j < 4; ++j) { double t = H[c][j]; H[c][j] = H[piv][j]; H[piv][j] = t; }
+            for (int j = 0; j < 3; ++j) { double t = r[c][j]; r[c][j] = r[piv][j]; r[piv][j] = t; }
+        }
+        for (int i = c + 1; i < 4; ++i) {
+            double fct = H[i][c] / H[c][c];
+            for (int j = c; j < 4; ++j) H[i][j] -= fct * H[c][j];
+            for (int j = 0; j < 3; ++j) r[i][j] -= fct * r[c][j];
+        }
+    }
+    for (int c = 3; c >= 0; --c)
+        for (int j = 0; j < 3; ++j) {
+            double s = r[c][j];
+            for (int k = c + 1; k < 4; ++k) s -= H[c][k] * r[k][j];
+            r[c][j] = s / H[c][c];
+        }
+}
+
+// One warp per filament.  scratch: 12 doubles per node (5 band + 7 right-hand sides).
+__global__ void __launch_bounds__(128) spline_solve_kernel(
+    int64_t nfil, const int64_t* __restrict__ offsets, const double* __restrict__ X,
+    double* __restrict__ knots, double* __restrict__ periods, int32_t* __restrict__ fil_of_node,
+    double* __restrict__ coef, double* __restrict__ dcoef1, double* __restrict__ dcoef2,
+    double* __restrict__ scratch, int32_t* __restrict__ status) {
+    const int lane = threadIdx.x & 31;
+    const int64_t fidx = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (fidx >= nfil) return;
+    const int64_t off = offsets[fidx];
+    const int n = (int)(offsets[fidx + 1] - off);
+    if (n < 5) {
+        if (lane == 0) atomicExch(status, 1);
+        return;
+    }
+    const double* Xf = X + 3 * off;
+    double* t = knots + off;
+    double* band = scratch + 12 * off;      // [n][5]
+    double* Y = band + 5 * (int64_t)n;      // [n][7]
+    double* c = coef + 3 * off;
+    double* c1 = dcoef1 + 3 * off;
+    double* c2 = dcoef2 + 3 * off;
+
+    // 1. chordal knots: warp-wide inclusive scan of segment lengths (parametrisations.jl:43-44)
+    double carry = 0.0;
+    for (int base = 0; base < n; base += 32) {
+        int i = base + lane;
+        double len = 0.0;
+        if (i < n) {
+            int j = (i + 1 == n) ? 0 : i + 1;
+            double dx = Xf[3 * j] - Xf[3 * i], dy = Xf[3 * j + 1] - Xf[3 * i + 1], dz = Xf[3 * j + 2] - Xf[3 * i + 2];
+            len = sqrt(dx * dx + dy * dy + dz * dz);
+            fil_of_node[off + i] = (int32_t)fidx;
+        }
+        double incl = len;
+#pragma unroll
+        for (int s = 1; s < 32; s <<= 1) {
+            double v = __shfl_up_sync(0xffffffffu, incl, s);
+            if (lane >= s) incl += v;
+        }
+        if (i < n) t[i] = carry + (incl - len);  // exclusive prefix: t_i
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    const double T = carry;
+    if (lane == 0) periods[fidx] = T;
+    __syncwarp();
+    FilView f{t, T, n};
+
+    // 2. collocation rows, band part only (corners handled below)
+    for (int i = lane; i < n; i += 32) {
+        double N[6];
+        bsplvb<6>(f, i, knot_at(f, i), N);
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            int col = i + s - 2;
+            band[5 * i + s] = (col >= 0 && col < n) ? N[s] : 0.0;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Y[7 * i + d] = Xf[3 * i + d];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            int ur = (q == 0) ? 0 : (q == 1) ? 1 : (q == 2) ? n - 2 : n - 1;
+            Y[7 * i + 3 + q] = (i == ur) ? 1.0 : 0.0;
+        }
+    }
+    __syncwarp();
+
+    // 3. banded elimination without pivoting (serial, lane 0)
+    if (lane == 0) {
+        for (int i = 0; i < n; ++i) {
+            double piv = band[5 * i + 2];
+            for (int r = i + 1; r <= i + 2 && r < n; ++r) {
+                double fct = band[5 * r + (i - r + 2)] / piv;
+                band[5 * r + (i - r + 2)] = fct;
+                for (int cc = i + 1; cc <= i + 2 && cc < n; ++cc) band[5 * r + (cc - r + 2)] -= fct * band[5 * i + (cc - i + 2)];
+            }
+        }
+    }
+    __syncwarp();
+
+    // 4. forward / backward sweeps, one right-hand side per lane
+    if (lane < 7) {
+        const int q = lane;
+        for (int i = 0; i < n; ++i) {
+            double yi = Y[7 * i + q];
+            for (int r = i + 1; r <= i + 2 && r < n; ++r) Y[7 * r + q] -= band[5 * r + (i - r + 2)] * yi;
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            double yi = Y[7 * i + q];
+            for (int cc = i + 1; cc <= i + 2 && cc < n; ++cc) yi -= band[5 * i + (cc - i + 2)] * Y[7 * cc + q];
+            Y[7 * i + q] = yi / band[5 * i + 2];
+        }
+    }
+    __syncwarp();
+
+    // 5. Woodbury correction: corners W of rows 0, 1, n-2, n-1
+    __shared__ double sh_s[4][4][3];
+    double (*s4)[3] = sh_s[threadIdx.x >> 5];
+    if (lane == 0) {
+        double H[4][4], rh[4][3];
+        const int rows[4] = {0, 1, n - 2, n - 1};
+        for (int r = 0; r < 4; ++r) {
+            for (int q = 0; q < 4; ++q) H[r][q] = (r == q) ? 1.0 : 0.0;
+            for (int d = 0; d < 3; ++d) rh[r][d] = 0.0;
+            int i = rows[r];
+            double N[6];
+            bsplvb<6>(f, i, knot_at(f, i), N);
+            for (int s = 0; s < 5; ++s) {
+                int col = i + s - 2;
+                if (col >= 0 && col < n) continue;
+                int cw = (int)pmodl(col, n);
+                for (int q = 0; q < 4; ++q) H[r][q] += N[s] * Y[7 * cw + 3 + q];
+                for (int d = 0; d < 3; ++d) rh[r][d] += N[s] * Y[7 * cw + d];
+            }
+        }
+        solve4(H, rh);
+        for (int r = 0; r < 4; ++r)
+            for (int d = 0; d < 3; ++d) s4[r][d] = rh[r][d];
+    }
+    __syncwarp();
+
+    // 6. coefficients c_j = u_{j+3}, u = y - Z s
+    for (int i = lane; i < n; i += 32) {
+        int j = (int)pmodl(i - 3, n);  // u_i = c_{i-3}
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double u = Y[7 * i + d];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) u -= Y[7 * i + 3 + q] * s4[q][d];
+            c[3 * j + d] = u;
+        }
+    }
+    __syncwarp();
+    // 7. derivative coefficients (spline derivative recurrence, spline.jl:301-319)
+    for (int j = lane; j < n; j += 32) {
+        int jm = (j == 0) ? n - 1 : j - 1;
+        double den = knot_at(f, j + 5) - knot_at(f, j);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) c1[3 * j + d] = 5.0 * (c[3 * j + d] - c[3 * jm + d]) / den;
+    }
+    __syncwarp();
+    for (int j = lane; j < n; j += 32) {
+        int jm = (j == 0) ? n - 1 : j - 1;
+        double den = knot_at(f, j + 4) - knot_at(f, j);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) c2[3 * j + d] = 4.0 * (c1[3 * j + d] - c1[3 * jm + d]) / den;
+    }
+}
+
+__device__ double seg_len(const FilView& f, const double* c1, long i, int nq, const double* qz, const double* qw,
+                          double a, double b) {
+    double dt = knot_at(f, i + 1) - knot_at(f, i);
+    double acc = 0.0;
+    for (int q = 0; q < nq; ++q) {
+        double d[3];
+        eval_seg<1>(f, c1, i, a + (b - a) * qz[q], d);
+        acc += qw[q] * sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    }
+    return dt * (b - a) * acc;
+}
+
+// One thread per node: point data of pointdata_impl.jl:65-108 and, when
+// lia_segment_fraction is set, the local integrals of local_integrals.jl:253-293.
+__global__ void __launch_bounds__(128) point_data_kernel(
+    KParams K, int64_t Np, const int64_t* __restrict__ offsets, const int32_t* __restrict__ fil_of_node,
+    const double* __restrict__ X, const double* __restrict__ knots, const double* __restrict__ periods,
+    const double* __restrict__ coef, const double* __restrict__ dcoef1, const double* __restrict__ dcoef2,
+    double* __restrict__ nodes, int32_t* __restrict__ idx_prev, double* __restrict__ d1, double* __restrict__ d2,
+    double* __restrict__ dm, double* __restrict__ dp, double* __restrict__ points, double* __restrict__ charges,
+    double* __restrict__ li_vel, double* __restrict__ li_psi, int want_li) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Np) return;
+    const int fidx = fil_of_node[k];
+    const int64_t off = offsets[fidx];
+    const int n = (int)(offsets[fidx + 1] - off);
+    const int i = (int)(k - off);
+    FilView f{knots + off, periods[fidx], n};
+    const double* c = coef + 3 * off;
+    const double* c1 = dcoef1 + 3 * off;
+    const double* c2 = dcoef2 + 3 * off;
+    const int64_t Nq = Np * K.nquad;
+
+    double xf[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        xf[d] = fold(X[3 * k + d], K.L[d], K.open_domain);
+        nodes[d * Np + k] = xf[d];
+    }
+    idx_prev[k] = (int32_t)(i == 0 ? off + n - 1 : k - 1);
+    double s1[3], s2[3];
+    eval_seg<1>(f, c1, i, 0.0, s1);
+    eval_seg<2>(f, c2, i, 0.0, s2);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        d1[d * Np + k] = s1[d];
+        d2[d * Np + k] = s2[d];
+    }
+    const double g = K.lia_fraction;
+    const bool has_g = g > 0;
+    dm[k] = seg_len(f, c1, i - 1, K.nquad, K.qz, K.qw, has_g ? 1.0 - g : 0.0, 1.0);
+    dp[k] = seg_len(f, c1, i, K.nquad, K.qz, K.qw, 0.0, has_g ? g : 1.0);
+    const double dt = knot_at(f, i + 1) - knot_at(f, i);
+    for (int q = 0; q < K.nquad; ++q) {
+        const int64_t mq = k * K.nquad + q;
+        double s[3], sp[3];
+        eval_seg<0>(f, c, i, K.qz[q], s);
+        eval_seg<1>(f, c1, i, K.qz[q], sp);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            points[d * Nq + mq] = fold(s[d], K.L[d], K.open_domain);
+            charges[d * Nq + mq] = K.qw[q] * dt * sp[d];
+        }
+    }
+    if (want_li) {
+        // nonlia_integration_limits: ((0, 1-g), (g, 1))  (local_integrals.jl:103-104)
+        double v[3] = {0, 0, 0}, ps[3] = {0, 0, 0};
+        for (int side = 0; side < 2; ++side) {
+            const long seg = side == 0 ? i - 1 : i;
+            const double a = side == 0 ? 0.0 : g, b = side == 0 ? 1.0 - g : 1.0;
+            const double dts = (knot_at(f, seg + 1) - knot_at(f, seg)) * (b - a);
+            for (int q = 0; q < K.nquad_near; ++q) {
+                const double y = a + (b - a) * K.qnz[q];
+                double s[3], sp[3], r[3], qc[3];
+                eval_seg<0>(f, c, seg, y, s);
+                eval_seg<1>(f, c1, seg, y, sp);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    qc[d] = K.qnw[q] * dts * sp[d];
+                    r[d] = deper(xf[d] - fold(s[d], K.L[d], K.open_domain), K.L[d], K.Lh[d], K.open_domain);
+                }
+                const double rinv = 1.0 / sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                const double r3 = rinv * rinv * rinv;
+                v[0] += r3 * (qc[1] * r[2] - qc[2] * r[1]);
+                v[1] += r3 * (qc[2] * r[0] - qc[0] * r[2]);
+                v[2] += r3 * (qc[0] * r[1] - qc[1] * r[0]);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) ps[d] += rinv * qc[d];
+            }
+        }
+        const double pref = K.Gamma / (4.0 * kPi);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            li_vel[d * Np + k] = pref * v[d];
+            li_psi[d * Np + k] = pref * ps[d];
+        }
+    }
+}
+
+}  // namespace
+
+int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offsets, const double* d_nodes) {
+    const int64_t Np = h->Np;
+    int rc;
+    if ((rc = ensure(h, h->knots, sizeof(double) * (Np + nfil), "knots"))) return rc;
+    if ((rc = ensure(h, h->fil_of_node, sizeof(int32_t) * Np, "fil_of_node"))) return rc;
+    if ((rc = ensure(h, h->coefs, sizeof(double) * 3 * Np, "coefs"))) return rc;
+    if ((rc = ensure(h, h->dcoef1, sizeof(double) * 3 * Np, "dcoef1"))) return rc;
+    if ((rc = ensure(h, h->dcoef2, sizeof(double) * 3 * Np, "dcoef2"))) return rc;
+    if ((rc = ensure(h, h->spline_scratch, sizeof(double) * 12 * Np + 64, "spline scratch"))) return rc;
+    double* knots = (double*)h->knots.p;
+    double* periods = knots + Np;
+    int32_t* status = (int32_t*)((double*)h->spline_scratch.p + 12 * Np);
+    StageScope st(h, ST_GEOMETRY);
+    if ((rc = check_cuda(h, cudaMemsetAsync(status, 0, sizeof(int32_t), h->stream), "memset"))) return rc;
+    spline_solve_kernel<<<grid_for(nfil, 4), 128, 0, h->stream>>>(
+        nfil, d_offsets, d_nodes, knots, periods, (int32_t*)h->fil_of_node.p, (double*)h->coefs.p,
+        (double*)h->dcoef1.p, (double*)h->dcoef2.p, (double*)h->spline_scratch.p, status);
+    h->launches++;
+    const bool want_li = h->K.lia_fraction > 0;
+    point_data_kernel<<<grid_for(Np, 128), 128, 0, h->stream>>>(
+        h->K, Np, d_offsets, (const int32_t*)h->fil_of_node.p, d_nodes, knots, periods, (const double*)h->coefs.p,
+        (const double*)h->dcoef1.p, (const double*)h->dcoef2.p, (double*)h->nodes.p, (int32_t*)h->idx_prev.p,
+        (double*)h->d1.p, (double*)h->d2.p, (double*)h->dm.p, (double*)h->dp.p, (double*)h->points.p,
+        (double*)h->charges.p, (double*)h->li_vel.p, (double*)h->li_psi.p, want_li ? 1 : 0);
+    h->launches++;
+    return check_cuda(h, cudaGetLastError(), "geometry kernels");
+}
+
+}  // namespace vpbs

@@ -1,0 +1,379 @@
+// Long-range part of the Ewald split on the device (src/BiotSavart/longrange/longrange.jl,
+// longrange/backends/nonuniformffts.jl):
+//  1. type-1 NUFFT of the quadrature charges: exponential-of-semicircle (ES) kernel spreading
+//     onto the oversampled grid (Barnett, Magland & af Klinteberg, SIAM J. Sci. Comput. 2019),
+//     then a batched 3-D real-to-complex FFT (cuFFT);
+//  2. one fused Fourier-space kernel: deconvolution, Gamma/V prefactor, Hermitian-symmetry
+//     zeroing (longrange.jl:556-583), optional spherical truncation (longrange.jl:497-532),
+//     the vorticity coefficients kept for get_longrange_field_fourier, and the
+//     streamfunction (longrange.jl:102-125) / Biot-Savart (longrange.jl:128-142) operators
+//     times the Ewald Gaussian exp(-k^2/4 alpha^2) (cache_common.jl:64-76) and the type-2
+//     deconvolution, written straight into the complex-to-real FFT input;
+//  3. batched complex-to-real FFT and ES-kernel interpolation at the nodes (type 2).
+#include <cmath>
+#include <vector>
+
+#include "vpbs_internal.cuh"
+
+namespace vpbs {
+namespace {
+
+// Gauss-Legendre rule on [-1, 1] by Newton iteration on P_n (host).
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.resize(n);
+    w.resize(n);
+    for (int i = 0; i < n; ++i) {
+        double z = std::cos(kPi * (i + 0.75) / (n + 0.5));
+        double dp = 1.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = z;
+            for (int k = 2; k <= n; ++k) {
+                double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (z * p1 - p0) / (z * z - 1.0);
+            double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        double p0 = 1.0, p1 = z;
+        for (int k = 2; k <= n; ++k) {
+            double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+            p0 = p1;
+            p1 = p2;
+        }
+        dp = n * (z * p1 - p0) / (z * z - 1.0);
+        x[i] = z;
+        w[i] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+
+// Fourier transform of the ES kernel psi(u) = exp(beta (sqrt(1 - (u/m)^2) - 1)), |u| <= m,
+// at frequency xi (radians per grid spacing): m * int_{-pi/2}^{pi/2} e^{beta(cos t - 1)}
+// cos(xi m sin t) cos t dt, evaluated with a 128-point Gauss-Legendre rule (the substitution
+// u = m sin t removes the square-root endpoint behaviour, so the rule converges fast).
+double es_hat(double xi, int m, double beta) {
+    static std::vector<double> gx, gw;
+    if (gx.empty()) gauss_legendre(128, gx, gw);
+    double s = 0.0;
+    for (size_t i = 0; i < gx.size(); ++i) {
+        double th = 0.5 * kPi * gx[i];
+        s += 0.5 * kPi * gw[i] * std::exp(beta * (std::cos(th) - 1.0)) * std::cos(xi * m * std::sin(th)) * std::cos(th);
+    }
+    return m * s;
+}
+
+inline int mode_of(int i, int N) { return i < (N + 1) / 2 ? i : i - N; }
+
+__device__ __forceinline__ double es_kernel(double u, int m, double beta) {
+    double z = u / m;
+    double s = 1.0 - z * z;
+    return s > 0.0 ? exp(beta * (sqrt(s) - 1.0)) : 0.0;
+}
+
+__device__ __forceinline__ int wrapi(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+constexpr int kSpreadBatch = 32;
+
+// Type-1 spreading: each block takes kSpreadBatch points; kernel values are tabulated in shared
+// memory, then every thread adds the charges along x-lines of the (2m)^3 footprint with
+// double-precision atomics.
+__global__ void __launch_bounds__(256) spread_kernel_f64(
+    LRSizes S, int64_t Nq, const double* __restrict__ src, double sx0, double sx1, double sx2,
+    double* __restrict__ grid) {
+    __shared__ double phi[kSpreadBatch][3][2 * kMaxHalfSupport];
+    __shared__ int i0s[kSpreadBatch][3];
+    __shared__ double qs[kSpreadBatch][3];
+    const int w = 2 * S.m;
+    const int64_t pbase = (int64_t)blockIdx.x * kSpreadBatch;
+    const int np = (int)((Nq - pbase) < kSpreadBatch ? (Nq - pbase) : kSpreadBatch);
+    const double scale[3] = {sx0, sx1, sx2};
+    for (int idx = threadIdx.x; idx < np * 3; idx += blockDim.x) {
+        const int p = idx / 3, d = idx % 3;
+        const int64_t j = pbase + p;
+        const double h = 2.0 * kPi / S.n[d];
+        const double xh = (src[d * Nq + j] * scale[d]) / h;
+        const int i0 = (int)floor(xh) - S.m + 1;
+        i0s[p][d] = i0;
+        for (int s = 0; s < w; ++s) phi[p][d][s] = es_kernel(xh - (i0 + s), S.m, S.beta);
+        qs[p][d] = src[(3 + d) * Nq + j];
+    }
+    __syncthreads();
+    const int per = w * w;
+    const int64_t ng = S.ngrid;
+    for (int item = threadIdx.x; item < np * per; item += blockDim.x) {
+        const int p = item / per, l = item % per;
+        const int sy = l % w, sz = l / w;
+        const int iz = wrapi(i0s[p][2] + sz, S.n[2]);
+        const int iy = wrapi(i0s[p][1] + sy, S.n[1]);
+        const double fyz = phi[p][2][sz] * phi[p][1][sy];
+        const double q0 = qs[p][0] * fyz, q1 = qs[p][1] * fyz, q2 = qs[p][2] * fyz;
+        const int64_t row = ((int64_t)iz * S.n[1] + iy) * S.n[0];
+        for (int sx = 0; sx < w; ++sx) {
+            const int ix = wrapi(i0s[p][0] + sx, S.n[0]);
+            const double f = phi[p][0][sx];
+            atomicAdd(grid + row + ix, q0 * f);
+            atomicAdd(grid + ng + row + ix, q1 * f);
+            atomicAdd(grid + 2 * ng + row + ix, q2 * f);
+        }
+    }
+}
+
+// Fused Fourier-space kernel over the r2c grid [n2][n1][n0/2+1].
+__global__ void __launch_bounds__(256) fourier_kernel_f64(
+    LRSizes S, double pref, double k0x, double k0y, double k0z, int truncate, double kmax2, int fields,
+    const double* __restrict__ dec0, const double* __restrict__ dec1, const double* __restrict__ dec2,
+    const double* __restrict__ decE0, const double* __restrict__ decE1, const double* __restrict__ decE2,
+    double2* __restrict__ gc, double2* __restrict__ gc2, double2* __restrict__ uhat, int store_uhat) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= S.ncgrid) return;
+    const int ix = (int)(idx % S.nxc);
+    const int64_t rest = idx / S.nxc;
+    const int iy = (int)(rest % S.n[1]);
+    const int iz = (int)(rest / S.n[1]);
+    const int ky = iy < (S.n[1] + 1) / 2 ? iy : iy - S.n[1];
+    const int kz = iz < (S.n[2] + 1) / 2 ? iz : iz - S.n[2];
+    const int lo1 = -(S.Ns[1] / 2), hi1 = (S.Ns[1] - 1) / 2;
+    const int lo2 = -(S.Ns[2] / 2), hi2 = (S.Ns[2] - 1) / 2;
+    const bool in_red = ix < S.nkx && ky >= lo1 && ky <= hi1 && kz >= lo2 && kz <= hi2;
+    const int64_t cstride = S.ncgrid;
+    double2 w[3] = {{0, 0}, {0, 0}, {0, 0}};
+    bool live = false;
+    if (in_red) {
+        const bool zero = (ix == S.nkx - 1) || (S.Ns[1] % 2 == 0 && ky == lo1) || (S.Ns[2] % 2 == 0 && kz == lo2);
+        const int ry = ky < 0 ? ky + S.Ns[1] : ky;
+        const int rz = kz < 0 ? kz + S.Ns[2] : kz;
+        const double kx = k0x * ix, kyy = k0y * ky, kzz = k0z * kz;
+        const double k2 = kx * kx + kyy * kyy + kzz * kzz;
+        live = !zero && !(truncate && k2 > kmax2);
+        if (live) {
+            const double f = pref * (dec0[ix] * dec1[ry] * dec2[rz]);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const double2 F = gc[c * cstride + idx];
+                w[c] = make_double2(F.x * f, F.y * f);
+            }
+        }
+        if (store_uhat) {
+            const int64_t u = ((int64_t)rz * S.Ns[1] + ry) * S.nkx + ix;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) uhat[c * S.nmodes + u] = w[c];
+        }
+        if (live) {
+            const double k2inv = (k2 == 0.0) ? 0.0 : 1.0 / k2;
+            const double g = decE0[ix] * decE1[ry] * decE2[rz];
+            if (fields & VPBS_VELOCITY) {
+                // i k x w / k^2 ; (i w).x = -w.y, (i w).y = w.x
+                const double2 iw0 = make_double2(-w[0].y, w[0].x), iw1 = make_double2(-w[1].y, w[1].x),
+                              iw2 = make_double2(-w[2].y, w[2].x);
+                const double fk = k2inv * g;
+                gc[idx] = make_double2((kyy * iw2.x - kzz * iw1.x) * fk, (kyy * iw2.y - kzz * iw1.y) * fk);
+                gc[cstride + idx] = make_double2((kzz * iw0.x - kx * iw2.x) * fk, (kzz * iw0.y - kx * iw2.y) * fk);
+                gc[2 * cstride + idx] = make_double2((kx * iw1.x - kyy * iw0.x) * fk, (kx * iw1.y - kyy * iw0.y) * fk);
+            }
+            if (fields & VPBS_STREAMFUNCTION) {
+                const double fk = k2inv * g;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) gc2[c * cstride + idx] = make_double2(w[c].x * fk, w[c].y * fk);
+            }
+        }
+    }
+    if (!live) {
+        if (fields & VPBS_VELOCITY)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) gc[c * cstride + idx] = make_double2(0.0, 0.0);
+        if (fields & VPBS_STREAMFUNCTION)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) gc2[c * cstride + idx] = make_double2(0.0, 0.0);
+    }
+}
+
+// Type-2 interpolation: one thread per node (visited in cell order when available).
+__global__ void __launch_bounds__(128) interp_kernel_f64(
+    LRSizes S, int64_t Np, const int32_t* __restrict__ order, const double* __restrict__ nodes, double sx0,
+    double sx1, double sx2, const double* __restrict__ grid, double* __restrict__ out) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= Np) return;
+    const int64_t i = order ? order[t] : t;
+    const int w = 2 * S.m;
+    const double scale[3] = {sx0, sx1, sx2};
+    double phi[3][2 * kMaxHalfSupport];
+    int i0[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double h = 2.0 * kPi / S.n[d];
+        const double xh = (nodes[d * Np + i] * scale[d]) / h;
+        i0[d] = (int)floor(xh) - S.m + 1;
+        for (int s = 0; s < w; ++s) phi[d][s] = es_kernel(xh - (i0[d] + s), S.m, S.beta);
+    }
+    double a0 = 0, a1 = 0, a2 = 0;
+    const int64_t ng = S.ngrid;
+    for (int sz = 0; sz < w; ++sz) {
+        const int iz = wrapi(i0[2] + sz, S.n[2]);
+        for (int sy = 0; sy < w; ++sy) {
+            const int iy = wrapi(i0[1] + sy, S.n[1]);
+            const double fyz = phi[2][sz] * phi[1][sy];
+            const int64_t row = ((int64_t)iz * S.n[1] + iy) * S.n[0];
+            for (int sx = 0; sx < w; ++sx) {
+                const int ix = wrapi(i0[0] + sx, S.n[0]);
+                const double f = fyz * phi[0][sx];
+                a0 += f * grid[row + ix];
+                a1 += f * grid[ng + row + ix];
+                a2 += f * grid[2 * ng + row + ix];
+            }
+        }
+    }
+    out[i] += a0;
+    out[Np + i] += a1;
+    out[2 * Np + i] += a2;
+}
+
+int check_fft(vpbs_handle* h, cufftResult r, const char* what) {
+    if (r == CUFFT_SUCCESS) return 0;
+    return set_error(h, VPBS_ERR_CUDA, std::string("cuFFT error in ") + what + " (code " + std::to_string((int)r) + ")");
+}
+
+}  // namespace
+
+int longrange_init(vpbs_handle* h) {
+    LRSizes& S = h->lr;
+    const vpbs_params& P = h->P;
+    for (int d = 0; d < 3; ++d) {
+        S.Ns[d] = P.Ns[d];
+        S.n[d] = vpbs_fft_size(P.Ns[d], P.sigma);
+    }
+    S.nkx = P.Ns[0] / 2 + 1;
+    S.nxc = S.n[0] / 2 + 1;
+    S.ngrid = (int64_t)S.n[0] * S.n[1] * S.n[2];
+    S.ncgrid = (int64_t)S.nxc * S.n[1] * S.n[2];
+    S.nmodes = (int64_t)S.nkx * S.Ns[1] * S.Ns[2];
+    S.m = P.m;
+    S.beta = 0.97 * kPi * (1.0 - 1.0 / (2.0 * P.sigma)) * (2.0 * P.m);
+    int rc;
+    if ((rc = ensure(h, h->grid_r, sizeof(double) * 3 * S.ngrid, "real grid"))) return rc;
+    if ((rc = ensure(h, h->grid_c, sizeof(double2) * 3 * S.ncgrid, "complex grid"))) return rc;
+    if ((rc = ensure(h, h->grid_c2, sizeof(double2) * 3 * S.ncgrid, "complex grid (streamfunction)"))) return rc;
+    if ((rc = ensure(h, h->uhat, sizeof(double2) * 3 * S.nmodes, "uhat"))) return rc;
+    // separable deconvolution factors 1/psi_hat and 1/psi_hat * exp(-k^2 / 4 alpha^2)
+    std::vector<double> tab[6];
+    const double beta_g = -1.0 / (4.0 * P.alpha * P.alpha);
+    for (int d = 0; d < 3; ++d) {
+        const int len = d == 0 ? S.nkx : S.Ns[d];
+        tab[d].resize(len);
+        tab[3 + d].resize(len);
+        const double k0 = 2.0 * kPi / P.L[d];
+        for (int i = 0; i < len; ++i) {
+            const int k = d == 0 ? i : mode_of(i, S.Ns[d]);
+            const double dec = 1.0 / es_hat(2.0 * kPi * k / S.n[d], S.m, S.beta);
+            const double kk = k0 * k;
+            tab[d][i] = dec;
+            tab[3 + d][i] = dec * std::exp(beta_g * kk * kk);
+        }
+    }
+    size_t tot = 0;
+    for (int d = 0; d < 6; ++d) tot += tab[d].size();
+    if ((rc = ensure(h, h->decx, sizeof(double) * tot, "deconvolution tables"))) return rc;
+    std::vector<double> all;
+    all.reserve(tot);
+    for (int d = 0; d < 6; ++d) all.insert(all.end(), tab[d].begin(), tab[d].end());
+    if ((rc = check_cuda(h, cudaMemcpy(h->decx.p, all.data(), sizeof(double) * tot, cudaMemcpyHostToDevice), "copy tables")))
+        return rc;
+    int nrev[3] = {S.n[2], S.n[1], S.n[0]};
+    if ((rc = check_fft(h, cufftPlanMany(&h->plan_r2c, 3, nrev, nullptr, 1, (int)S.ngrid, nullptr, 1, (int)S.ncgrid,
+                                         CUFFT_D2Z, 3), "plan D2Z")))
+        return rc;
+    if ((rc = check_fft(h, cufftPlanMany(&h->plan_c2r, 3, nrev, nullptr, 1, (int)S.ncgrid, nullptr, 1, (int)S.ngrid,
+                                         CUFFT_Z2D, 3), "plan Z2D")))
+        return rc;
+    h->have_plans = true;
+    return 0;
+}
+
+void longrange_free(vpbs_handle* h) {
+    if (h->have_plans) {
+        cufftDestroy(h->plan_r2c);
+        cufftDestroy(h->plan_c2r);
+        h->have_plans = false;
+    }
+}
+
+int longrange_compute(vpbs_handle* h, int fields) {
+    const LRSizes& S = h->lr;
+    const vpbs_params& P = h->P;
+    int rc;
+    const double sx[3] = {2.0 * kPi / P.L[0], 2.0 * kPi / P.L[1], 2.0 * kPi / P.L[2]};
+    double* grid = (double*)h->grid_r.p;
+    double2* gc = (double2*)h->grid_c.p;
+    double2* gc2 = (double2*)h->grid_c2.p;
+    // sources: cell-sorted copy (SoA x,y,z,qx,qy,qz), built by build_cell_lists
+    const double* src = (const double*)h->src_sorted.p;
+    {
+        StageScope st(h, ST_SPREAD);
+        if ((rc = check_cuda(h, cudaMemsetAsync(grid, 0, sizeof(double) * 3 * S.ngrid, h->stream), "memset grid")))
+            return rc;
+        spread_kernel_f64<<<grid_for(h->Nq, kSpreadBatch), 256, 0, h->stream>>>(S, h->Nq, src, sx[0], sx[1], sx[2], grid);
+        h->launches++;
+        if ((rc = check_cuda(h, cudaGetLastError(), "spread kernel"))) return rc;
+    }
+    {
+        StageScope st(h, ST_FFT_FORWARD);
+        if ((rc = check_fft(h, cufftSetStream(h->plan_r2c, h->stream), "set stream"))) return rc;
+        if ((rc = check_fft(h, cufftExecD2Z(h->plan_r2c, grid, (cufftDoubleComplex*)gc), "exec D2Z"))) return rc;
+    }
+    double kmax = INFINITY;
+    for (int d = 0; d < 3; ++d) kmax = fmin(kmax, 2.0 * kPi * ((P.Ns[d] - 1) / 2) / P.L[d]);
+    const double pref = P.Gamma / (P.L[0] * P.L[1] * P.L[2]);
+    const double* t = (const double*)h->decx.p;
+    const double* dec0 = t;
+    const double* dec1 = dec0 + S.nkx;
+    const double* dec2 = dec1 + S.Ns[1];
+    const double* decE0 = dec2 + S.Ns[2];
+    const double* decE1 = decE0 + S.nkx;
+    const double* decE2 = decE1 + S.Ns[1];
+    {
+        StageScope st(h, ST_FOURIER);
+        fourier_kernel_f64<<<grid_for(S.ncgrid, 256), 256, 0, h->stream>>>(
+            S, pref, sx[0], sx[1], sx[2], P.truncate_spherical, kmax * kmax, fields, dec0, dec1, dec2, decE0, decE1,
+            decE2, gc, gc2, (double2*)h->uhat.p, 1);
+        h->launches++;
+        h->have_uhat = true;
+        if ((rc = check_cuda(h, cudaGetLastError(), "fourier kernel"))) return rc;
+    }
+    if ((rc = check_fft(h, cufftSetStream(h->plan_c2r, h->stream), "set stream"))) return rc;
+    const int32_t* order = (const int32_t*)h->dst_order.p;
+    for (int f = 0; f < 2; ++f) {
+        const int field = f == 0 ? VPBS_STREAMFUNCTION : VPBS_VELOCITY;
+        if (!(fields & field)) continue;
+        double2* in = field == VPBS_VELOCITY ? gc : gc2;
+        double* out = (double*)(field == VPBS_VELOCITY ? h->vel.p : h->psi.p);
+        {
+            StageScope st(h, ST_FFT_INVERSE);
+            if ((rc = check_fft(h, cufftExecZ2D(h->plan_c2r, (cufftDoubleComplex*)in, grid), "exec Z2D"))) return rc;
+        }
+        StageScope st(h, ST_INTERP);
+        interp_kernel_f64<<<grid_for(h->Np, 128), 128, 0, h->stream>>>(S, h->Np, order, (const double*)h->nodes.p,
+                                                                      sx[0], sx[1], sx[2], grid, out);
+        h->launches++;
+        if ((rc = check_cuda(h, cudaGetLastError(), "interp kernel"))) return rc;
+    }
+    return 0;
+}
+
+}  // namespace vpbs
+
+extern "C" int32_t vpbs_fft_size(int32_t Ns, double sigma) {
+    int n = (int)std::ceil(sigma * Ns - 1e-9);
+    if (n < 2) n = 2;
+    for (;; ++n) {
+        if (n % 2) continue;
+        int r = n;
+        while (r % 2 == 0) r /= 2;
+        while (r % 3 == 0) r /= 3;
+        while (r % 5 == 0) r /= 5;
+        if (r == 1) return n;
+    }
+}

@@ -1,0 +1,386 @@
+// Short-range part of the Ewald split on the device:
+//  * local (LIA) term and self-interaction removal, one thread per node
+//    (src/BiotSavart/shortrange/local_integrals.jl:4-165);
+//  * cell lists as a counting sort of the quadrature points (and of the nodes) by cell
+//    (replaces the linked lists of src/CellLists/gpu.jl:28-61 and the destination sort of
+//    gpu.jl:183-231);
+//  * the pair kernel (src/BiotSavart/shortrange/shortrange.jl:216-273 with the Gaussian
+//    weights of splitting/gaussian.jl:273-279): one warp per destination node, lanes
+//    stride over the contiguous cell-sorted source ranges of the (2M+1)^2 neighbour rows,
+//    warp-shuffle reduction at the end.
+#include "vpbs_internal.cuh"
+
+namespace vpbs {
+namespace {
+
+__device__ __forceinline__ double deper(double r, double L, double Lh, int open) {
+    if (open) return r;
+    r = (r >= Lh) ? r - L : r;
+    r = (r < -Lh) ? r + L : r;
+    return r;
+}
+
+__device__ __forceinline__ int cell_coord(double x, double L, int nc) {
+    int c = (int)((x / L) * nc);
+    return c < 0 ? 0 : (c >= nc ? nc - 1 : c);
+}
+
+__device__ __forceinline__ int64_t cell_of(const CellGrid& cg, const KParams& K, double x, double y, double z) {
+    int cx = cell_coord(x, K.L[0], cg.nc[0]);
+    int cy = cell_coord(y, K.L[1], cg.nc[1]);
+    int cz = cell_coord(z, K.L[2], cg.nc[2]);
+    return ((int64_t)cz * cg.nc[1] + cy) * cg.nc[0] + cx;
+}
+
+// Cell of every element and its rank within the cell (atomic counter).
+__global__ void cell_count_kernel(KParams K, CellGrid cg, int64_t n, const double* __restrict__ xyz,
+                                  int32_t* __restrict__ cell, int32_t* __restrict__ rank,
+                                  int32_t* __restrict__ counts) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    int64_t c = cell_of(cg, K, xyz[j], xyz[n + j], xyz[2 * n + j]);
+    cell[j] = (int32_t)c;
+    rank[j] = atomicAdd(&counts[c], 1);
+}
+
+// Exclusive scan of counts[0..n) into start[0..n] with one CTA of 1024 threads.
+__global__ void __launch_bounds__(1024) scan_kernel(const int32_t* __restrict__ counts, int32_t* __restrict__ start,
+                                                    int64_t n) {
+    __shared__ int32_t part[1024];
+    const int tid = threadIdx.x;
+    const int64_t chunk = (n + 1023) / 1024;
+    const int64_t lo = tid * chunk;
+    const int64_t hi = lo + chunk < n ? lo + chunk : n;
+    int32_t s = 0;
+    for (int64_t i = lo; i < hi; ++i) s += counts[i];
+    part[tid] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        int32_t v = tid >= off ? part[tid - off] : 0;
+        __syncthreads();
+        part[tid] += v;
+        __syncthreads();
+    }
+    int32_t acc = part[tid] - s;  // exclusive prefix of this chunk
+    for (int64_t i = lo; i < hi; ++i) {
+        start[i] = acc;
+        acc += counts[i];
+    }
+    if (tid == 1023) start[n] = part[1023];
+}
+
+// Scatter the sources into cell order (SoA: x, y, z, qx, qy, qz) and record their segment.
+__global__ void scatter_sources_kernel(int64_t Nq, int nquad, const double* __restrict__ points,
+                                       const double* __restrict__ charges, const int32_t* __restrict__ cell,
+                                       const int32_t* __restrict__ rank, const int32_t* __restrict__ start,
+                                       double* __restrict__ sorted, int32_t* __restrict__ seg) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= Nq) return;
+    int64_t pos = (int64_t)start[cell[j]] + rank[j];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        sorted[d * Nq + pos] = points[d * Nq + j];
+        sorted[(3 + d) * Nq + pos] = charges[d * Nq + j];
+    }
+    seg[pos] = (int32_t)(j / nquad);
+}
+
+__global__ void scatter_nodes_kernel(int64_t Np, const int32_t* __restrict__ cell, const int32_t* __restrict__ rank,
+                                     const int32_t* __restrict__ start, int32_t* __restrict__ order) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Np) return;
+    order[(int64_t)start[cell[i]] + rank[i]] = (int32_t)i;
+}
+
+struct PairAcc {
+    double v[3];
+    double p[3];
+    unsigned long long inr, cand;
+};
+
+template <bool VEL, bool PSI>
+__device__ __forceinline__ void pair_range(const KParams& K, const double x[3], int64_t i, int32_t iprev, bool skip_local,
+                                           const double* __restrict__ src, int64_t Ns, const int32_t* __restrict__ seg,
+                                           int64_t b, int64_t e, int lane, PairAcc& acc) {
+    const double two_over_sqrt_pi = 1.1283791670955126;  // 2/sqrt(pi)
+    for (int64_t j = b + lane; j < e; j += 32) {
+        if (skip_local) {
+            int32_t sj = seg[j];
+            if (sj == i || sj == iprev) continue;
+        }
+        double r0 = deper(x[0] - src[j], K.L[0], K.Lh[0], K.open_domain);
+        double r1 = deper(x[1] - src[Ns + j], K.L[1], K.Lh[1], K.open_domain);
+        double r2 = deper(x[2] - src[2 * Ns + j], K.L[2], K.Lh[2], K.open_domain);
+        double rr2 = r0 * r0 + r1 * r1 + r2 * r2;
+        acc.cand++;
+        if (!(rr2 <= K.rcut2)) continue;
+        acc.inr++;
+        double q0 = src[3 * Ns + j], q1 = src[4 * Ns + j], q2 = src[5 * Ns + j];
+        double r = sqrt(rr2);
+        double rinv = 1.0 / r;
+        double ar = K.alpha * r;
+        double wa = erfc(ar);
+        if (VEL) {
+            double wb = two_over_sqrt_pi * ar * exp(-(ar * ar));
+            double f = (wa + wb) * rinv * rinv * rinv;
+            acc.v[0] += f * (q1 * r2 - q2 * r1);
+            acc.v[1] += f * (q2 * r0 - q0 * r2);
+            acc.v[2] += f * (q0 * r1 - q1 * r0);
+        }
+        if (PSI) {
+            double f = wa * rinv;
+            acc.p[0] += f * q0;
+            acc.p[1] += f * q1;
+            acc.p[2] += f * q2;
+        }
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One warp per destination node (visited in cell order when cell lists are used).
+template <bool VEL, bool PSI>
+__global__ void __launch_bounds__(256) pair_kernel_f64(
+    KParams K, CellGrid cg, int64_t Np, int64_t Ns, const int32_t* __restrict__ dst_order,
+    const double* __restrict__ nodes, const int32_t* __restrict__ idx_prev, const double* __restrict__ src,
+    const int32_t* __restrict__ src_start, const int32_t* __restrict__ seg, int use_cells, int skip_local,
+    double* __restrict__ vel, double* __restrict__ psi, unsigned long long* __restrict__ counters) {
+    const int lane = threadIdx.x & 31;
+    const int64_t w = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (w >= Np) return;
+    const int64_t i = use_cells ? dst_order[w] : w;
+    const double x[3] = {nodes[i], nodes[Np + i], nodes[2 * Np + i]};
+    const int32_t iprev = idx_prev[i];
+    PairAcc acc = {{0, 0, 0}, {0, 0, 0}, 0ull, 0ull};
+    if (!use_cells) {
+        pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, 0, Ns, lane, acc);
+    } else {
+        const int M = cg.M;
+        const int nc0 = cg.nc[0], nc1 = cg.nc[1], nc2 = cg.nc[2];
+        const int cx = cell_coord(x[0], K.L[0], nc0);
+        const int cy = cell_coord(x[1], K.L[1], nc1);
+        const int cz = cell_coord(x[2], K.L[2], nc2);
+        for (int dz = -M; dz <= M; ++dz) {
+            int zz = cz + dz;
+            zz = zz < 0 ? zz + nc2 : (zz >= nc2 ? zz - nc2 : zz);
+            for (int dy = -M; dy <= M; ++dy) {
+                int yy = cy + dy;
+                yy = yy < 0 ? yy + nc1 : (yy >= nc1 ? yy - nc1 : yy);
+                const int64_t base = ((int64_t)zz * nc1 + yy) * nc0;
+                const int lo = cx - M, hi = cx + M;
+                if (lo >= 0 && hi < nc0) {
+                    pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo],
+                                         src_start[base + hi + 1], lane, acc);
+                } else if (lo < 0) {
+                    pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo + nc0],
+                                         src_start[base + nc0], lane, acc);
+                    pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base],
+                                         src_start[base + hi + 1], lane, acc);
+                } else {
+                    pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo],
+                                         src_start[base + nc0], lane, acc);
+                    pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base],
+                                         src_start[base + hi - nc0 + 1], lane, acc);
+                }
+            }
+        }
+    }
+    const double pref = K.Gamma / (4.0 * kPi);
+    double v0 = 0, v1 = 0, v2 = 0, p0 = 0, p1 = 0, p2 = 0;
+    if (VEL) { v0 = warp_sum(acc.v[0]); v1 = warp_sum(acc.v[1]); v2 = warp_sum(acc.v[2]); }
+    if (PSI) { p0 = warp_sum(acc.p[0]); p1 = warp_sum(acc.p[1]); p2 = warp_sum(acc.p[2]); }
+    unsigned long long inr = warp_sum_u(acc.inr), cand = warp_sum_u(acc.cand);
+    if (lane == 0) {
+        if (VEL) { vel[i] += pref * v0; vel[Np + i] += pref * v1; vel[2 * Np + i] += pref * v2; }
+        if (PSI) { psi[i] += pref * p0; psi[Np + i] += pref * p1; psi[2 * Np + i] += pref * p2; }
+        atomicAdd(&counters[0], inr);
+        atomicAdd(&counters[1], cand);
+    }
+}
+
+// Local term (overwrites nothing: adds into the zeroed outputs), self-interaction removal
+// and, when lia_segment_fraction is set, the local integrals over the excluded sub-segments.
+__global__ void __launch_bounds__(128) local_self_kernel(
+    KParams K, int64_t Np, int fields, int do_local, int do_self, int do_li, double rv, double rpsi,
+    const double* __restrict__ nodes, const int32_t* __restrict__ idx_prev, const double* __restrict__ d1,
+    const double* __restrict__ d2, const double* __restrict__ dm, const double* __restrict__ dp,
+    const double* __restrict__ points, const double* __restrict__ charges, const double* __restrict__ li_vel,
+    const double* __restrict__ li_psi, double* __restrict__ vel, double* __restrict__ psi) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Np) return;
+    const bool want_v = fields & VPBS_VELOCITY, want_p = fields & VPBS_STREAMFUNCTION;
+    const double pref = K.Gamma / (4.0 * kPi);
+    double v[3] = {0, 0, 0}, p[3] = {0, 0, 0};
+    if (do_local) {
+        const double delta = sqrt(dm[i] * dp[i]);
+        const double s1[3] = {d1[i], d1[Np + i], d1[2 * Np + i]};
+        const double s2[3] = {d2[i], d2[Np + i], d2[2 * Np + i]};
+        const double mu_inv = 1.0 / sqrt(s1[0] * s1[0] + s1[1] * s1[1] + s1[2] * s1[2]);
+        if (want_v) {
+            const double f = log(delta / rv) * (mu_inv * mu_inv * mu_inv);
+            v[0] = pref * (f * (s1[1] * s2[2] - s1[2] * s2[1]));
+            v[1] = pref * (f * (s1[2] * s2[0] - s1[0] * s2[2]));
+            v[2] = pref * (f * (s1[0] * s2[1] - s1[1] * s2[0]));
+        }
+        if (want_p) {
+            const double f = 2.0 * log(delta / rpsi) * mu_inv;
+            for (int d = 0; d < 3; ++d) p[d] = pref * (f * s1[d]);
+        }
+    }
+    if (do_self) {
+        const int64_t Nq = Np * K.nquad;
+        const double x[3] = {nodes[i], nodes[Np + i], nodes[2 * Np + i]};
+        const int64_t ip = idx_prev[i];
+        const bool explicit_erf = !K.avoid_explicit_erf && K.alpha > 0;
+        double sv[3] = {0, 0, 0}, sp[3] = {0, 0, 0};
+        for (int side = 0; side < 2; ++side) {
+            const int64_t base = (side == 0 ? ip : i) * K.nquad;
+            for (int q = 0; q < K.nquad; ++q) {
+                const int64_t j = base + q;
+                double r[3];
+                for (int d = 0; d < 3; ++d) r[d] = deper(x[d] - points[d * Nq + j], K.L[d], K.Lh[d], K.open_domain);
+                const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                const double rinv = 1.0 / rr;
+                const double qc[3] = {charges[j], charges[Nq + j], charges[2 * Nq + j]};
+                double fa = 1.0, fb = 0.0;
+                if (explicit_erf) {
+                    const double ar = K.alpha * rr;
+                    fa = erf(ar);
+                    fb = 1.1283791670955126 * ar * exp(-(ar * ar));
+                }
+                if (want_v) {
+                    const double f = (fa - fb) * rinv * rinv * rinv;
+                    sv[0] += f * (qc[1] * r[2] - qc[2] * r[1]);
+                    sv[1] += f * (qc[2] * r[0] - qc[0] * r[2]);
+                    sv[2] += f * (qc[0] * r[1] - qc[1] * r[0]);
+                }
+                if (want_p) {
+                    const double f = fa * rinv;
+                    for (int d = 0; d < 3; ++d) sp[d] += f * qc[d];
+                }
+            }
+        }
+        for (int d = 0; d < 3; ++d) {
+            v[d] -= pref * sv[d];
+            p[d] -= pref * sp[d];
+        }
+    }
+    if (do_li) {
+        for (int d = 0; d < 3; ++d) {
+            v[d] += li_vel[d * Np + i];
+            p[d] += li_psi[d * Np + i];
+        }
+    }
+    if (want_v)
+        for (int d = 0; d < 3; ++d) vel[d * Np + i] += v[d];
+    if (want_p)
+        for (int d = 0; d < 3; ++d) psi[d * Np + i] += p[d];
+}
+
+}  // namespace
+
+int build_cell_lists(vpbs_handle* h) {
+    if (h->K.open_domain) return 0;
+    const int64_t Np = h->Np, Nq = h->Nq, ncell = h->cg.ncell;
+    int rc;
+    if ((rc = ensure(h, h->src_cell, sizeof(int32_t) * 2 * Nq, "src_cell"))) return rc;
+    if ((rc = ensure(h, h->src_start, sizeof(int32_t) * (ncell + 1), "src_start"))) return rc;
+    if ((rc = ensure(h, h->src_fill, sizeof(int32_t) * ncell, "src_counts"))) return rc;
+    if ((rc = ensure(h, h->src_sorted, sizeof(double) * 6 * Nq, "src_sorted"))) return rc;
+    if ((rc = ensure(h, h->src_seg, sizeof(int32_t) * Nq, "src_seg"))) return rc;
+    if ((rc = ensure(h, h->dst_cell, sizeof(int32_t) * 2 * Np, "dst_cell"))) return rc;
+    if ((rc = ensure(h, h->dst_start, sizeof(int32_t) * (ncell + 1), "dst_start"))) return rc;
+    if ((rc = ensure(h, h->dst_fill, sizeof(int32_t) * ncell, "dst_counts"))) return rc;
+    if ((rc = ensure(h, h->dst_order, sizeof(int32_t) * Np, "dst_order"))) return rc;
+    int32_t* scell = (int32_t*)h->src_cell.p;
+    int32_t* srank = scell + Nq;
+    int32_t* dcell = (int32_t*)h->dst_cell.p;
+    int32_t* drank = dcell + Np;
+    StageScope st(h, ST_CELL_LISTS);
+    if ((rc = check_cuda(h, cudaMemsetAsync(h->src_fill.p, 0, sizeof(int32_t) * ncell, h->stream), "memset"))) return rc;
+    if ((rc = check_cuda(h, cudaMemsetAsync(h->dst_fill.p, 0, sizeof(int32_t) * ncell, h->stream), "memset"))) return rc;
+    cell_count_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(h->K, h->cg, Nq, (const double*)h->points.p, scell, srank,
+                                                                (int32_t*)h->src_fill.p);
+    cell_count_kernel<<<grid_for(Np, 256), 256, 0, h->stream>>>(h->K, h->cg, Np, (const double*)h->nodes.p, dcell, drank,
+                                                                (int32_t*)h->dst_fill.p);
+    scan_kernel<<<1, 1024, 0, h->stream>>>((const int32_t*)h->src_fill.p, (int32_t*)h->src_start.p, ncell);
+    scan_kernel<<<1, 1024, 0, h->stream>>>((const int32_t*)h->dst_fill.p, (int32_t*)h->dst_start.p, ncell);
+    scatter_sources_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(
+        Nq, h->K.nquad, (const double*)h->points.p, (const double*)h->charges.p, scell, srank,
+        (const int32_t*)h->src_start.p, (double*)h->src_sorted.p, (int32_t*)h->src_seg.p);
+    scatter_nodes_kernel<<<grid_for(Np, 256), 256, 0, h->stream>>>(Np, dcell, drank, (const int32_t*)h->dst_start.p,
+                                                                   (int32_t*)h->dst_order.p);
+    h->launches += 6;
+    return check_cuda(h, cudaGetLastError(), "cell list kernels");
+}
+
+int pair_interactions(vpbs_handle* h, int fields) {
+    const int64_t Np = h->Np, Nq = h->Nq;
+    const bool open = h->K.open_domain;
+    int rc;
+    if ((rc = ensure(h, h->counters, sizeof(unsigned long long) * 2, "counters"))) return rc;
+    if ((rc = check_cuda(h, cudaMemsetAsync(h->counters.p, 0, sizeof(unsigned long long) * 2, h->stream), "memset")))
+        return rc;
+    if (open) {
+        // naive pair loop over the unsorted point data; the segment of point j is j / nquad
+        if ((rc = ensure(h, h->src_sorted, sizeof(double) * 6 * Nq, "src"))) return rc;
+        if ((rc = ensure(h, h->src_seg, sizeof(int32_t) * Nq, "src_seg"))) return rc;
+        for (int d = 0; d < 3; ++d) {
+            cudaMemcpyAsync((double*)h->src_sorted.p + d * Nq, (double*)h->points.p + d * Nq, sizeof(double) * Nq,
+                            cudaMemcpyDeviceToDevice, h->stream);
+            cudaMemcpyAsync((double*)h->src_sorted.p + (3 + d) * Nq, (double*)h->charges.p + d * Nq,
+                            sizeof(double) * Nq, cudaMemcpyDeviceToDevice, h->stream);
+        }
+    }
+    const int skip_local = (!h->K.avoid_explicit_erf && h->K.alpha > 0) ? 1 : 0;
+    if (skip_local && open) return set_error(h, VPBS_ERR_PARAMS, "avoid_explicit_erf=false requires Ewald splitting");
+    StageScope st(h, ST_PAIRS);
+    const unsigned grid = grid_for(Np, 8);
+    const bool v = fields & VPBS_VELOCITY, p = fields & VPBS_STREAMFUNCTION;
+    auto launch = [&](auto kern) {
+        kern<<<grid, 256, 0, h->stream>>>(h->K, h->cg, Np, Nq, (const int32_t*)h->dst_order.p, (const double*)h->nodes.p,
+                                          (const int32_t*)h->idx_prev.p, (const double*)h->src_sorted.p,
+                                          (const int32_t*)h->src_start.p, (const int32_t*)h->src_seg.p, (open || h->cg.M == 0) ? 0 : 1,
+                                          skip_local, (double*)h->vel.p, (double*)h->psi.p,
+                                          (unsigned long long*)h->counters.p);
+    };
+    if (v && p) launch(pair_kernel_f64<true, true>);
+    else if (v) launch(pair_kernel_f64<true, false>);
+    else launch(pair_kernel_f64<false, true>);
+    h->launches++;
+    return check_cuda(h, cudaGetLastError(), "pair kernel");
+}
+
+int local_and_self(vpbs_handle* h, int fields, int lia_mode, int with_pairs_self, double integration_cutoff) {
+    const KParams& K = h->K;
+    double rpsi, rv;
+    if (integration_cutoff > 0) {
+        rpsi = rv = integration_cutoff;
+    } else {
+        rpsi = exp(K.Delta - 1.0) * K.a / 2.0;
+        rv = rpsi * exp(1.0);
+    }
+    const int do_local = (lia_mode == VPBS_LIA_TRUE || lia_mode == VPBS_LIA_ONLY) ? 1 : 0;
+    const int do_self = with_pairs_self ? 1 : 0;
+    const int do_li = (with_pairs_self && K.lia_fraction > 0) ? 1 : 0;
+    StageScope st(h, ST_LOCAL_SELF);
+    local_self_kernel<<<grid_for(h->Np, 128), 128, 0, h->stream>>>(
+        K, h->Np, fields, do_local, do_self, do_li, rv, rpsi, (const double*)h->nodes.p, (const int32_t*)h->idx_prev.p,
+        (const double*)h->d1.p, (const double*)h->d2.p, (const double*)h->dm.p, (const double*)h->dp.p,
+        (const double*)h->points.p, (const double*)h->charges.p, (const double*)h->li_vel.p,
+        (const double*)h->li_psi.p, (double*)h->vel.p, (double*)h->psi.p);
+    h->launches++;
+    return check_cuda(h, cudaGetLastError(), "local term kernel");
+}
+
+}  // namespace vpbs

@@ -1,0 +1,150 @@
+// Internal declarations shared by the libvpbs.so translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdint>
+#include <string>
+
+#include "vpbs.h"
+
+namespace vpbs {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kMaxQuad = 16;
+constexpr int kMaxHalfSupport = 8;
+
+// Parameters in the form the kernels use (passed by value to kernels).
+struct KParams {
+    double Gamma, a, Delta;
+    double L[3], Lh[3];
+    double alpha, rcut, rcut2;
+    int nquad, nquad_near;
+    double qz[kMaxQuad], qw[kMaxQuad];
+    double qnz[kMaxQuad], qnw[kMaxQuad];
+    double lia_fraction;  // <= 0: nothing
+    int avoid_explicit_erf;
+    int open_domain;      // NoSplitting
+};
+
+// Cell-list geometry.
+struct CellGrid {
+    int nc[3];
+    int M;
+    int64_t ncell;
+};
+
+// Long-range sizes.
+struct LRSizes {
+    int Ns[3];
+    int nkx;         // Ns0/2 + 1
+    int n[3];        // oversampled FFT grid
+    int nxc;         // n0/2 + 1
+    int64_t ngrid;   // n0*n1*n2 (real)
+    int64_t ncgrid;  // nxc*n1*n2 (complex)
+    int64_t nmodes;  // nkx*Ns1*Ns2
+    int m;
+    double beta;     // ES kernel shape
+};
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace vpbs
+
+struct vpbs_handle {
+    vpbs_params P;
+    vpbs::KParams K;
+    std::string err;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int64_t launches = 0;
+
+    // sizes
+    int64_t Np = 0, Nq = 0, nfil = 0;
+    bool have_points = false;
+
+    // geometry inputs / scratch
+    vpbs::DevBuf nodes_in, offsets, fil_of_node, knots, coefs, dcoef1, dcoef2, spline_scratch;
+
+    // point data (SoA; 3 consecutive blocks of Np or Nq doubles for vectors)
+    vpbs::DevBuf nodes, idx_prev, d1, d2, dm, dp, points, charges;
+    vpbs::DevBuf li_vel, li_psi;  // lia_segment_fraction local integrals (per node)
+
+    // cell lists
+    vpbs::CellGrid cg{};
+    vpbs::DevBuf src_cell, src_start, src_fill, src_sorted, src_seg, dst_cell, dst_start, dst_fill, dst_order;
+    vpbs::DevBuf counters;  // [0] in-range pairs, [1] candidates (unsigned long long)
+
+    // long range
+    vpbs::LRSizes lr{};
+    vpbs::DevBuf grid_r, grid_c, grid_c2, uhat, decx, decy, decz, nodes_lr;
+    cufftHandle plan_r2c = 0, plan_c2r = 0, plan_c2r_6 = 0;
+    bool have_plans = false;
+    bool have_uhat = false;
+
+    // outputs (SoA, 3*Np each)
+    vpbs::DevBuf vel, psi;
+    int32_t last_fields = 0;
+
+    // pinned host staging: separate regions for inputs and outputs; h2d_done guards reuse
+    void* pin_in = nullptr;
+    size_t pin_in_bytes = 0;
+    void* pin_out = nullptr;
+    size_t pin_out_bytes = 0;
+    cudaEvent_t h2d_done = nullptr;
+    bool li_valid = false;  // lia_segment_fraction integrals available (filament input only)
+
+    // optional per-stage CUDA-event timing (vpbs_stage_timing)
+    bool timing = false;
+    cudaEvent_t tev[16][4][2] = {};  // [stage][occurrence][start/stop]
+    int tcount[16] = {};
+};
+
+namespace vpbs {
+
+int set_error(vpbs_handle* h, int code, const std::string& msg);
+int check_cuda(vpbs_handle* h, cudaError_t e, const char* what);
+int ensure(vpbs_handle* h, DevBuf& b, size_t bytes, const char* what);
+int ensure_pinned(vpbs_handle* h, void** buf, size_t* cap, size_t bytes);
+
+inline unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
+
+// geometry.cu
+int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offsets, const double* d_nodes);
+
+// shortrange.cu
+int build_cell_lists(vpbs_handle* h);
+int local_and_self(vpbs_handle* h, int fields, int lia_mode, int with_pairs_self, double integration_cutoff);
+int pair_interactions(vpbs_handle* h, int fields);
+int add_local_integrals(vpbs_handle* h, int fields);
+
+// longrange.cu
+int longrange_init(vpbs_handle* h);
+void longrange_free(vpbs_handle* h);
+int longrange_compute(vpbs_handle* h, int fields);  // adds into h->vel / h->psi
+
+// stage timing
+enum Stage {
+    ST_GEOMETRY = 0, ST_CELL_LISTS, ST_SPREAD, ST_FFT_FORWARD, ST_FOURIER, ST_FFT_INVERSE, ST_INTERP,
+    ST_LOCAL_SELF, ST_PAIRS, ST_COUNT
+};
+inline void stage_mark(vpbs_handle* h, int s, int stop) {
+    if (!h->timing) return;
+    int k = stop ? h->tcount[s] - 1 : h->tcount[s];
+    if (k < 0 || k >= 4) return;
+    cudaEventRecord(h->tev[s][k][stop], h->stream);
+    if (!stop) h->tcount[s]++;
+}
+struct StageScope {
+    vpbs_handle* h;
+    int s;
+    StageScope(vpbs_handle* hh, int ss) : h(hh), s(ss) { stage_mark(h, s, 0); }
+    ~StageScope() { stage_mark(h, s, 1); }
+};
+
+}  // namespace vpbs
