@@ -720,14 +720,17 @@ static void fft3(cplx* a, const int n[3], int sign) {
 
 static double es_beta(const vpo_params* p) { return 0.97 * VPO_PI * (1.0 - 1.0 / (2.0 * p->sigma)) * (2.0 * p->m); }
 
+/* ES kernel shifted down by its edge value e^{-beta}, so that it vanishes continuously at
+ * |u| = m: the 2m-point window of a point lying on a grid node then does not depend on the
+ * last bit of its coordinate (the unshifted kernel jumps by e^{-beta} there). */
 static inline double es_kernel(double u, int m, double beta) {
     double z = u / m;
     double s = 1.0 - z * z;
-    return s > 0 ? exp(beta * (sqrt(s) - 1.0)) : 0.0;
+    return s > 0 ? exp(beta * (sqrt(s) - 1.0)) - exp(-beta) : 0.0;
 }
 
-/* Fourier transform of the ES kernel in grid units: int_{-m}^{m} psi(u) cos(xi u) du,
- * via z = sin(theta) and a 128-point Gauss-Legendre rule on [-pi/2, pi/2]. */
+/* Fourier transform of the (shifted) ES kernel in grid units: int_{-m}^{m} psi(u) cos(xi u) du,
+ * via u = m sin(theta) and a 128-point Gauss-Legendre rule on [-pi/2, pi/2]. */
 static double es_hat(double xi, int m, double beta) {
     static __thread double gz[128], gw[128];
     static __thread int init = 0;
@@ -740,7 +743,7 @@ static double es_hat(double xi, int m, double beta) {
     double s = 0.0;
     for (int i = 0; i < 128; ++i) {
         double th = gz[i];
-        s += gw[i] * exp(beta * (cos(th) - 1.0)) * cos(xi * m * sin(th)) * cos(th);
+        s += gw[i] * (exp(beta * (cos(th) - 1.0)) - exp(-beta)) * cos(xi * m * sin(th)) * cos(th);
     }
     return m * s;
 }

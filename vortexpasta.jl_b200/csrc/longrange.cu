@@ -49,8 +49,8 @@ void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
     }
 }
 
-// Fourier transform of the ES kernel psi(u) = exp(beta (sqrt(1 - (u/m)^2) - 1)), |u| <= m,
-// at frequency xi (radians per grid spacing): m * int_{-pi/2}^{pi/2} e^{beta(cos t - 1)}
+// Fourier transform of the shifted ES kernel psi(u) = exp(beta (sqrt(1 - (u/m)^2) - 1)) - e^{-beta}, |u| <= m,
+// at frequency xi (radians per grid spacing): m * int_{-pi/2}^{pi/2} (e^{beta(cos t - 1)} - e^{-beta})
 // cos(xi m sin t) cos t dt, evaluated with a 128-point Gauss-Legendre rule (the substitution
 // u = m sin t removes the square-root endpoint behaviour, so the rule converges fast).
 double es_hat(double xi, int m, double beta) {
@@ -59,17 +59,21 @@ double es_hat(double xi, int m, double beta) {
     double s = 0.0;
     for (size_t i = 0; i < gx.size(); ++i) {
         double th = 0.5 * kPi * gx[i];
-        s += 0.5 * kPi * gw[i] * std::exp(beta * (std::cos(th) - 1.0)) * std::cos(xi * m * std::sin(th)) * std::cos(th);
+        s += 0.5 * kPi * gw[i] * (std::exp(beta * (std::cos(th) - 1.0)) - std::exp(-beta)) * std::cos(xi * m * std::sin(th)) *
+             std::cos(th);
     }
     return m * s;
 }
 
 inline int mode_of(int i, int N) { return i < (N + 1) / 2 ? i : i - N; }
 
-__device__ __forceinline__ double es_kernel(double u, int m, double beta) {
+// ES kernel shifted down by its edge value e^{-beta} (passed as `edge`) so that it vanishes
+// continuously at |u| = m: which 2m-point window a point on a grid node gets then no longer
+// depends on the last bit of its coordinate.
+__device__ __forceinline__ double es_kernel(double u, int m, double beta, double edge) {
     double z = u / m;
     double s = 1.0 - z * z;
-    return s > 0.0 ? exp(beta * (sqrt(s) - 1.0)) : 0.0;
+    return s > 0.0 ? exp(beta * (sqrt(s) - 1.0)) - edge : 0.0;
 }
 
 __device__ __forceinline__ int wrapi(int i, int n) {
@@ -99,7 +103,7 @@ __global__ void __launch_bounds__(256) spread_kernel_f64(
         const double xh = (src[d * Nq + j] * scale[d]) / h;
         const int i0 = (int)floor(xh) - S.m + 1;
         i0s[p][d] = i0;
-        for (int s = 0; s < w; ++s) phi[p][d][s] = es_kernel(xh - (i0 + s), S.m, S.beta);
+        for (int s = 0; s < w; ++s) phi[p][d][s] = es_kernel(xh - (i0 + s), S.m, S.beta, S.edge);
         qs[p][d] = src[(3 + d) * Nq + j];
     }
     __syncthreads();
@@ -208,7 +212,7 @@ __global__ void __launch_bounds__(128) interp_kernel_f64(
         const double h = 2.0 * kPi / S.n[d];
         const double xh = (nodes[d * Np + i] * scale[d]) / h;
         i0[d] = (int)floor(xh) - S.m + 1;
-        for (int s = 0; s < w; ++s) phi[d][s] = es_kernel(xh - (i0[d] + s), S.m, S.beta);
+        for (int s = 0; s < w; ++s) phi[d][s] = es_kernel(xh - (i0[d] + s), S.m, S.beta, S.edge);
     }
     double a0 = 0, a1 = 0, a2 = 0;
     const int64_t ng = S.ngrid;
@@ -253,6 +257,7 @@ int longrange_init(vpbs_handle* h) {
     S.nmodes = (int64_t)S.nkx * S.Ns[1] * S.Ns[2];
     S.m = P.m;
     S.beta = 0.97 * kPi * (1.0 - 1.0 / (2.0 * P.sigma)) * (2.0 * P.m);
+    S.edge = std::exp(-S.beta);
     int rc;
     if ((rc = ensure(h, h->grid_r, sizeof(double) * 3 * S.ngrid, "real grid"))) return rc;
     if ((rc = ensure(h, h->grid_c, sizeof(double2) * 3 * S.ncgrid, "complex grid"))) return rc;

@@ -46,6 +46,7 @@ struct LRSizes {
     int64_t nmodes;  // nkx*Ns1*Ns2
     int m;
     double beta;     // ES kernel shape
+    double edge;     // e^{-beta}, subtracted so the kernel vanishes at |u| = m
 };
 
 struct DevBuf {
