@@ -173,6 +173,30 @@ int vpbs_stage_timing(vpbs_handle* h, int32_t enable);
 int vpbs_stage_times(vpbs_handle* h, double* ms, int32_t n);
 const char* vpbs_stage_name(int32_t i);
 
+/* Allocation-free variant of the point-data computation of vpbs_set_filaments, with no
+ * counterpart in the reference.  It is for callers that cannot allocate device memory: code
+ * running where cudaMalloc is forbidden or unsafe (under an external memory pool that owns all
+ * device memory, inside another runtime's stream-ordered region, or in a binding that can only
+ * hand over buffers it already owns).  It calls no cudaMalloc, cudaFree or allocating library
+ * routine: the spline solve's intermediates (knots, B-spline coefficients, banded factors) live
+ * in one file-scope device array of about 6 MB that every GPU loading the library holds until
+ * the process exits.
+ *
+ * Inputs: params (quadrature rule, periods, lia_segment_fraction, device), `nfil` filaments with
+ * host `offsets[nfil+1]`, device AoS nodes `nodes_xyz` [Np][3]; `stream` (cudaStream_t, may be
+ * NULL).  Outputs (device pointers, same layouts as vpbs_get_pointdata): nodes, s', s'' (SoA
+ * 3*Np), node_idx_prev (Np, 0-based), delta_minus, delta_plus (Np), points, charges (SoA 3*Nq).
+ * Limits: at most VPBS_NOALLOC_MAX_NODES nodes and VPBS_NOALLOC_MAX_FILAMENTS filaments; larger
+ * inputs are rejected with VPBS_ERR_ARG.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (other streams, other threads)
+ * race and must be serialised by the caller.  Errors: vpbs_last_error(NULL). Asynchronous. */
+#define VPBS_NOALLOC_MAX_NODES 32768
+#define VPBS_NOALLOC_MAX_FILAMENTS 4096
+int vpbs_point_data_noalloc(const vpbs_params* params, int64_t nfil, const int64_t* offsets, const double* nodes_xyz,
+                            void* stream, double* nodes, int32_t* node_idx_prev, double* deriv1, double* deriv2,
+                            double* delta_minus, double* delta_plus, double* points, double* charges);
+
 /* Measured CUDA-core FMA throughput of `device` in TFLOP/s (fp64 = 1: double, 0: float); the
  * denominator of the pair kernel's roofline.  Measurement support; no counterpart in the
  * reference. */

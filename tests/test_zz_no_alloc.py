@@ -1,0 +1,82 @@
+"""The allocation-free point-data entry point (vpbs_point_data_noalloc).
+
+It exists for callers that cannot allocate device memory (an external pool owns the GPU's
+memory, cudaMalloc is not allowed where they run, or their binding can only pass buffers it
+already holds).  The caller owns every input and output buffer; the library keeps its
+intermediates in a fixed file-scope device array.  This file is collected last on purpose.
+"""
+
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def _call_noalloc(vp, p, fs, torch):
+    from vortexpasta_b200 import _lib
+    from vortexpasta_b200.biotsavart import _c_params
+    lib = _lib.load()
+    nodes, offsets = vp.curves.concat(fs)
+    Np = int(offsets[-1])
+    Nq = Np * len(p.quadrature)
+    dev = torch.device("cuda", 0)
+    x = torch.from_numpy(nodes).to(dev)
+    out = {
+        "nodes": torch.empty(3 * Np, dtype=torch.float64, device=dev),
+        "idx_prev": torch.empty(Np, dtype=torch.int32, device=dev),
+        "d1": torch.empty(3 * Np, dtype=torch.float64, device=dev),
+        "d2": torch.empty(3 * Np, dtype=torch.float64, device=dev),
+        "dm": torch.empty(Np, dtype=torch.float64, device=dev),
+        "dp": torch.empty(Np, dtype=torch.float64, device=dev),
+        "points": torch.empty(3 * Nq, dtype=torch.float64, device=dev),
+        "charges": torch.empty(3 * Nq, dtype=torch.float64, device=dev),
+    }
+    cp = _c_params(p)
+    stream = torch.cuda.current_stream(dev)
+    rc = lib.vpbs_point_data_noalloc(
+        ct.byref(cp), len(fs), offsets.ctypes.data_as(_lib.c_int64_p), ct.c_void_p(x.data_ptr()),
+        ct.c_void_p(stream.cuda_stream),
+        *[ct.c_void_p(out[k].data_ptr()) for k in ("nodes", "idx_prev", "d1", "d2", "dm", "dp", "points", "charges")])
+    assert rc == 0, lib.vpbs_last_error(None)
+    torch.cuda.synchronize()
+    res = {}
+    for k, t in out.items():
+        a = t.cpu().numpy()
+        res[k] = a.reshape(3, -1).T if k in ("nodes", "d1", "d2", "points", "charges") else a
+    return res
+
+
+@pytest.mark.gpu
+def test_noalloc_matches_set_filaments_two_calls(vp, built_lib):
+    import torch
+    _, p = vp.configs.tangle20k()
+    tol = {"d2": 1e-10}  # same tolerances as test_gpu_parity.test_point_data_matches_oracle
+    for seed, nrings in ((7, 40), (8, 25)):  # two calls in a row, different sizes
+        fs = vp.configs.tangle(nrings, 200, seed=seed) + [vp.curves.ring(5, 0.3, center=(1, 1, 1))]
+        got = _call_noalloc(vp, p, fs, torch)
+        cache = vp.init_cache(p)
+        cache.set_filaments(fs)
+        ref = cache.pointdata()
+        cache.close()
+        for k in ("nodes", "d1", "d2", "dm", "dp", "points", "charges"):
+            assert rel(got[k], ref[k]) < tol.get(k, 1e-12), (seed, k)
+        np.testing.assert_array_equal(got["idx_prev"], ref["idx_prev"])
+
+
+def test_noalloc_rejects_oversized_input(vp, built_lib):
+    """Sizes beyond the fixed array are rejected before any device work (no GPU needed)."""
+    from vortexpasta_b200 import _lib
+    from vortexpasta_b200.biotsavart import _c_params
+    lib = _lib.load()
+    _, p = vp.configs.tangle20k()
+    n = 40000  # > VPBS_NOALLOC_MAX_NODES
+    offsets = np.array([0, n], dtype=np.int64)
+    dummy = ct.c_void_p(1)
+    rc = lib.vpbs_point_data_noalloc(ct.byref(_c_params(p)), 1, offsets.ctypes.data_as(_lib.c_int64_p), dummy, None,
+                                     *([dummy] * 8))
+    assert rc == -1
+    assert b"at most 32768 nodes" in lib.vpbs_last_error(None)

@@ -385,3 +385,117 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
 }
 
 }  // namespace vpbs
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free point data (vpbs_point_data_noalloc).
+//
+// For callers that cannot allocate device memory themselves or through this library: code
+// that runs where cudaMalloc is forbidden or unsafe (inside a stream-ordered region of another
+// runtime, under an external memory pool that owns all device memory, or in a host language
+// binding that only hands over pre-allocated buffers).  The intermediate arrays of the spline
+// solve (knots, B-spline coefficients, the banded factorisation) live in one file-scope device
+// array of fixed size instead of cudaMalloc'd buffers; every GPU that loads the library holds
+// this array (about 6 MB) until the process exits.
+// ---------------------------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+constexpr int64_t kNoAllocMaxNodes = VPBS_NOALLOC_MAX_NODES;
+constexpr int64_t kNoAllocMaxFil = VPBS_NOALLOC_MAX_FILAMENTS;
+// layout (in doubles): offsets (int64) | knots + periods | fil_of_node (int32) | coefs |
+// dcoef1 | dcoef2 | spline scratch (12 per node) | status
+constexpr int64_t kNoAllocDoubles =
+    (kNoAllocMaxFil + 1) + (kNoAllocMaxNodes + kNoAllocMaxFil) + (kNoAllocMaxNodes + 1) / 2 + 9 * kNoAllocMaxNodes +
+    12 * kNoAllocMaxNodes + 8;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device.  In
+// host code the symbol itself is only a host-side stand-in, never a device address.
+int noalloc_scratch(double** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+        return vpbs::set_error(nullptr, VPBS_ERR_CUDA, "vpbs_point_data_noalloc: no usable CUDA device");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return vpbs::set_error(nullptr, VPBS_ERR_CUDA,
+                                   std::string("vpbs_point_data_noalloc: cudaGetSymbolAddress failed: ") +
+                                       cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = (double*)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int vpbs_point_data_noalloc(const vpbs_params* params, int64_t nfil, const int64_t* offsets,
+                                       const double* nodes_xyz, void* stream, double* nodes, int32_t* node_idx_prev,
+                                       double* deriv1, double* deriv2, double* delta_minus, double* delta_plus,
+                                       double* points, double* charges) {
+    using namespace vpbs;
+    if (!params || !offsets || !nodes_xyz || !nodes || !node_idx_prev || !deriv1 || !deriv2 || !delta_minus ||
+        !delta_plus || !points || !charges)
+        return set_error(nullptr, VPBS_ERR_ARG, "vpbs_point_data_noalloc: null argument");
+    const vpbs_params& P = *params;
+    if (nfil < 1 || offsets[0] != 0) return set_error(nullptr, VPBS_ERR_ARG, "vpbs_point_data_noalloc: bad offsets");
+    for (int64_t f = 0; f < nfil; ++f)
+        if (offsets[f + 1] - offsets[f] < 5)
+            return set_error(nullptr, VPBS_ERR_ARG, "each filament needs at least 5 nodes (quintic splines)");
+    const int64_t Np = offsets[nfil];
+    if (nfil > kNoAllocMaxFil || Np > kNoAllocMaxNodes)
+        return set_error(nullptr, VPBS_ERR_ARG,
+                         "vpbs_point_data_noalloc: at most " + std::to_string(kNoAllocMaxNodes) + " nodes and " +
+                             std::to_string(kNoAllocMaxFil) + " filaments (got " + std::to_string(Np) + " nodes, " +
+                             std::to_string(nfil) + " filaments); use vpbs_set_filaments for larger systems");
+    if (P.nquad < 1 || P.nquad > kMaxQuad) return set_error(nullptr, VPBS_ERR_PARAMS, "nquad must be in 1:16");
+    if (P.lia_segment_fraction > 1.0) return set_error(nullptr, VPBS_ERR_PARAMS, "lia_segment_fraction must be in (0, 1]");
+    KParams K{};
+    K.Gamma = P.Gamma;
+    K.open_domain = P.alpha > 0 ? 0 : 1;
+    for (int d = 0; d < 3; ++d) {
+        K.L[d] = K.open_domain ? 0.0 : P.L[d];
+        K.Lh[d] = K.L[d] / 2;
+        if (!K.open_domain && !(P.L[d] > 0)) return set_error(nullptr, VPBS_ERR_PARAMS, "periods L must be positive");
+    }
+    K.nquad = P.nquad;
+    for (int q = 0; q < P.nquad; ++q) { K.qz[q] = P.quad_zeta[q]; K.qw[q] = P.quad_w[q]; }
+    K.nquad_near = K.nquad;
+    K.lia_fraction = P.lia_segment_fraction > 0 ? P.lia_segment_fraction : 0.0;
+    if (cudaSetDevice(P.device) != cudaSuccess)
+        return set_error(nullptr, VPBS_ERR_CUDA, "vpbs_point_data_noalloc: cudaSetDevice failed");
+    double* base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    int64_t* d_offsets = (int64_t*)base;
+    double* knots = base + (kNoAllocMaxFil + 1);
+    double* periods = knots + Np;
+    int32_t* fil_of_node = (int32_t*)(knots + kNoAllocMaxNodes + kNoAllocMaxFil);
+    double* coefs = knots + kNoAllocMaxNodes + kNoAllocMaxFil + (kNoAllocMaxNodes + 1) / 2;
+    double* dcoef1 = coefs + 3 * kNoAllocMaxNodes;
+    double* dcoef2 = dcoef1 + 3 * kNoAllocMaxNodes;
+    double* scratch = dcoef2 + 3 * kNoAllocMaxNodes;
+    int32_t* status = (int32_t*)(scratch + 12 * kNoAllocMaxNodes);
+    cudaError_t e = cudaMemcpyAsync(d_offsets, offsets, sizeof(int64_t) * (nfil + 1), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, sizeof(int32_t), s);  // the array keeps the last call's data
+    if (e != cudaSuccess)
+        return set_error(nullptr, VPBS_ERR_CUDA, std::string("vpbs_point_data_noalloc: ") + cudaGetErrorString(e));
+    spline_solve_kernel<<<grid_for(nfil, 4), 128, 0, s>>>(nfil, d_offsets, nodes_xyz, knots, periods, fil_of_node, coefs,
+                                                          dcoef1, dcoef2, scratch, status);
+    point_data_kernel<<<grid_for(Np, 128), 128, 0, s>>>(K, Np, d_offsets, fil_of_node, nodes_xyz, knots, periods, coefs,
+                                                        dcoef1, dcoef2, nodes, node_idx_prev, deriv1, deriv2,
+                                                        delta_minus, delta_plus, points, charges, nullptr, nullptr, 0);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return set_error(nullptr, VPBS_ERR_CUDA, std::string("vpbs_point_data_noalloc: ") + cudaGetErrorString(e));
+    return 0;
+}
