@@ -186,6 +186,9 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
     int rc = activate(h);
     if (!rc) rc = check_cuda(h, cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!rc) rc = check_cuda(h, cudaEventCreateWithFlags(&h->h2d_done, cudaEventDisableTiming), "cudaEventCreate");
+    if (!rc) rc = check_cuda(h, cudaStreamCreateWithFlags(&h->aux_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (cudaEvent_t* e : {&h->ev_fork, &h->ev_short, &h->ev_long})
+        if (!rc) rc = check_cuda(h, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
     h->stream = h->own_stream;
     if (!rc && !open) rc = longrange_init(h);
     if (rc) {
@@ -212,6 +215,14 @@ int vpbs_destroy(vpbs_handle* h) {
     if (h->pin_in) cudaFreeHost(h->pin_in);
     if (h->pin_out) cudaFreeHost(h->pin_out);
     if (h->h2d_done) cudaEventDestroy(h->h2d_done);
+    if (h->aux_stream) cudaStreamSynchronize(h->aux_stream);
+    for (cudaEvent_t e : {h->ev_fork, h->ev_short, h->ev_long})
+        if (e) cudaEventDestroy(e);
+    if (h->aux_stream) cudaStreamDestroy(h->aux_stream);
+    if (h->tev[0][0][0])
+        for (int s = 0; s < ST_COUNT; ++s)
+            for (int k = 0; k < 4; ++k)
+                for (int e = 0; e < 2; ++e) cudaEventDestroy(h->tev[s][k][e]);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return 0;
@@ -317,8 +328,14 @@ int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t short
     if (fields & VPBS_STREAMFUNCTION)
         if ((rc = check_cuda(h, cudaMemsetAsync(h->psi.p, 0, sizeof(double) * 3 * Np, h->stream), "memset"))) return rc;
     const bool with_long = longrange && lia_mode != VPBS_LIA_ONLY && !h->K.open_domain;
-    if (with_long)
-        if ((rc = longrange_compute(h, fields))) return rc;
+    // The long range (spread, FFTs, Fourier operators) runs on the auxiliary stream while the
+    // short range runs on the main stream; only the long-range interpolation, which adds into
+    // the same outputs, waits for the short range.  The main stream then joins.
+    cudaStream_t main = h->stream;
+    if (with_long) {
+        if ((rc = check_cuda(h, cudaEventRecord(h->ev_fork, main), "fork"))) return rc;
+        if ((rc = check_cuda(h, cudaStreamWaitEvent(h->aux_stream, h->ev_fork, 0), "fork"))) return rc;
+    }
     if (shortrange) {
         const bool pairs = lia_mode != VPBS_LIA_ONLY;
         KParams saved = h->K;
@@ -328,6 +345,17 @@ int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t short
         if (rc) return rc;
         if (pairs)
             if ((rc = pair_interactions(h, fields))) return rc;
+    }
+    if (with_long) {
+        if ((rc = check_cuda(h, cudaEventRecord(h->ev_short, main), "short done"))) return rc;
+        h->stream = h->aux_stream;
+        h->interp_wait = h->ev_short;
+        rc = longrange_compute(h, fields);
+        h->interp_wait = nullptr;
+        h->stream = main;
+        if (rc) return rc;
+        if ((rc = check_cuda(h, cudaEventRecord(h->ev_long, h->aux_stream), "long done"))) return rc;
+        if ((rc = check_cuda(h, cudaStreamWaitEvent(main, h->ev_long, 0), "join"))) return rc;
     }
     h->last_fields = fields;
     return 0;

@@ -173,30 +173,50 @@ __global__ void __launch_bounds__(128) spline_solve_kernel(
     }
     __syncwarp();
 
-    // 3. banded elimination without pivoting (serial, lane 0)
+    // 3. pentadiagonal LU without pivoting (serial, lane 0), as a register recurrence: row i of
+    //    the band (e, d, c, b, a at columns i-2..i+2) becomes (l2, l1, 1/u0, u1, u2):
+    //    l2 = e/u0[i-2], l1 = (d - l2 u1[i-2])/u0[i-1], u0 = c - l2 u2[i-2] - l1 u1[i-1],
+    //    u1 = b - l1 u2[i-1], u2 = a.
     if (lane == 0) {
+        double iu0_m2 = 0.0, u1_m2 = 0.0, u2_m2 = 0.0;  // row i-2
+        double iu0_m1 = 0.0, u1_m1 = 0.0, u2_m1 = 0.0;  // row i-1
         for (int i = 0; i < n; ++i) {
-            double piv = band[5 * i + 2];
-            for (int r = i + 1; r <= i + 2 && r < n; ++r) {
-                double fct = band[5 * r + (i - r + 2)] / piv;
-                band[5 * r + (i - r + 2)] = fct;
-                for (int cc = i + 1; cc <= i + 2 && cc < n; ++cc) band[5 * r + (cc - r + 2)] -= fct * band[5 * i + (cc - i + 2)];
-            }
+            double* r = band + 5 * i;
+            const double e = r[0], d = r[1], c = r[2], b = r[3], a = r[4];
+            const double l2 = e * iu0_m2;
+            const double l1 = (d - l2 * u1_m2) * iu0_m1;
+            const double u0 = c - l2 * u2_m2 - l1 * u1_m1;
+            const double u1 = b - l1 * u2_m1;
+            const double iu0 = 1.0 / u0;
+            r[0] = l2;
+            r[1] = l1;
+            r[2] = iu0;
+            r[3] = u1;
+            r[4] = a;
+            iu0_m2 = iu0_m1; u1_m2 = u1_m1; u2_m2 = u2_m1;
+            iu0_m1 = iu0; u1_m1 = u1; u2_m1 = a;
         }
     }
     __syncwarp();
 
-    // 4. forward / backward sweeps, one right-hand side per lane
+    // 4. forward / backward sweeps, one right-hand side per lane (register recurrences)
     if (lane < 7) {
         const int q = lane;
+        double z1 = 0.0, z2 = 0.0;  // z[i-1], z[i-2]
         for (int i = 0; i < n; ++i) {
-            double yi = Y[7 * i + q];
-            for (int r = i + 1; r <= i + 2 && r < n; ++r) Y[7 * r + q] -= band[5 * r + (i - r + 2)] * yi;
+            const double* r = band + 5 * i;
+            const double z = Y[7 * i + q] - r[1] * z1 - r[0] * z2;
+            Y[7 * i + q] = z;
+            z2 = z1;
+            z1 = z;
         }
+        double x1 = 0.0, x2 = 0.0;  // x[i+1], x[i+2]
         for (int i = n - 1; i >= 0; --i) {
-            double yi = Y[7 * i + q];
-            for (int cc = i + 1; cc <= i + 2 && cc < n; ++cc) yi -= band[5 * i + (cc - i + 2)] * Y[7 * cc + q];
-            Y[7 * i + q] = yi / band[5 * i + 2];
+            const double* r = band + 5 * i;
+            const double x = (Y[7 * i + q] - r[3] * x1 - r[4] * x2) * r[2];
+            Y[7 * i + q] = x;
+            x2 = x1;
+            x1 = x;
         }
     }
     __syncwarp();

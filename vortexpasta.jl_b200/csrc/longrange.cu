@@ -196,6 +196,174 @@ __global__ void __launch_bounds__(256) fourier_kernel_f64(
     }
 }
 
+// ---- atomic-free spreading ("brick gather") ----
+// The oversampled grid is tiled into bricks of B^3 points.  Points are binned by the brick
+// holding the first grid point of their footprint; a footprint of w <= B points can then only
+// reach the brick of its bin and the next one in each direction, so brick b gathers the points
+// of bins b and b-1 (per dimension, periodic).  Each thread of the B*B-thread CTA owns one
+// x-line of the brick in registers; every grid value is written exactly once, with plain stores.
+
+__device__ __forceinline__ int footprint_start(double x, double scale, int n, int m) {
+    const double xh = (x * scale) / (2.0 * kPi / n);
+    return wrapi((int)floor(xh) - m + 1, n);
+}
+
+__global__ void spread_bin_count_kernel(LRSizes S, int B, int nb0, int nb1, int nb2, int64_t Nq,
+                                        const double* __restrict__ src, double sx0, double sx1, double sx2,
+                                        int32_t* __restrict__ bin, int32_t* __restrict__ rank,
+                                        int32_t* __restrict__ counts) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= Nq) return;
+    const int b0 = footprint_start(src[j], sx0, S.n[0], S.m) / B;
+    const int b1 = footprint_start(src[Nq + j], sx1, S.n[1], S.m) / B;
+    const int b2 = footprint_start(src[2 * Nq + j], sx2, S.n[2], S.m) / B;
+    const int32_t b = (b2 * nb1 + b1) * nb0 + b0;
+    bin[j] = b;
+    rank[j] = atomicAdd(&counts[b], 1);
+}
+
+__global__ void spread_bin_scatter_kernel(int64_t Nq, const double* __restrict__ src, const int32_t* __restrict__ bin,
+                                          const int32_t* __restrict__ rank, const int32_t* __restrict__ start,
+                                          double* __restrict__ binned) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= Nq) return;
+    const int64_t pos = (int64_t)start[bin[j]] + rank[j];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) binned[c * Nq + pos] = src[c * Nq + j];
+}
+
+constexpr int kGatherChunk = 32;
+
+template <int B>
+__global__ void __launch_bounds__(B * B) spread_gather_kernel_f64(
+    LRSizes S, int nb0, int nb1, int nb2, int64_t Nq, const int32_t* __restrict__ bin_start,
+    const double* __restrict__ binned, double sx0, double sx1, double sx2, double* __restrict__ grid) {
+    __shared__ double row[kGatherChunk][B];                     // x-profile aligned to the brick
+    __shared__ double phy[kGatherChunk][2 * kMaxHalfSupport];
+    __shared__ double phz[kGatherChunk][2 * kMaxHalfSupport];
+    __shared__ double qs[kGatherChunk][3];
+    __shared__ int oys[kGatherChunk], ozs[kGatherChunk];
+    const int w = 2 * S.m;
+    const int bx = blockIdx.x % nb0;
+    const int by = (blockIdx.x / nb0) % nb1;
+    const int bz = blockIdx.x / (nb0 * nb1);
+    const int bs[3] = {bx * B, by * B, bz * B};
+    const int ly = threadIdx.x % B, lz = threadIdx.x / B;
+    const double scale[3] = {sx0, sx1, sx2};
+    double acc[3][B];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int i = 0; i < B; ++i) acc[c][i] = 0.0;
+    for (int nbr = 0; nbr < 8; ++nbr) {
+        const int cx = (bx - (nbr & 1) + nb0) % nb0;
+        const int cy = (by - ((nbr >> 1) & 1) + nb1) % nb1;
+        const int cz = (bz - ((nbr >> 2) & 1) + nb2) % nb2;
+        const int b = (cz * nb1 + cy) * nb0 + cx;
+        const int64_t p0 = bin_start[b], p1 = bin_start[b + 1];
+        for (int64_t base = p0; base < p1; base += kGatherChunk) {
+            const int np = (int)((p1 - base) < kGatherChunk ? (p1 - base) : kGatherChunk);
+            __syncthreads();
+            for (int idx = threadIdx.x; idx < np * 3; idx += B * B) {
+                const int p = idx / 3, d = idx % 3;
+                const int64_t j = base + p;
+                const double xh = (binned[d * Nq + j] * scale[d]) / (2.0 * kPi / S.n[d]);
+                const int i0 = (int)floor(xh) - S.m + 1;
+                int o = wrapi(i0, S.n[d]) - bs[d];
+                if (o >= B) o -= S.n[d];  // footprint starts in the previous brick (periodic)
+                if (d == 0) {
+                    for (int ix = 0; ix < B; ++ix) {
+                        const int s = ix - o;
+                        row[p][ix] = (s >= 0 && s < w) ? es_kernel(xh - (i0 + s), S.m, S.beta, S.edge) : 0.0;
+                    }
+                } else {
+                    double* ph = d == 1 ? phy[p] : phz[p];
+                    for (int s = 0; s < w; ++s) ph[s] = es_kernel(xh - (i0 + s), S.m, S.beta, S.edge);
+                    if (d == 1) oys[p] = o;
+                    else ozs[p] = o;
+                }
+                qs[p][d] = binned[(3 + d) * Nq + j];
+            }
+            __syncthreads();
+            for (int p = 0; p < np; ++p) {
+                const int sy = ly - oys[p], sz = lz - ozs[p];
+                if ((unsigned)sy < (unsigned)w && (unsigned)sz < (unsigned)w) {
+                    const double f = phy[p][sy] * phz[p][sz];
+                    const double f0 = qs[p][0] * f, f1 = qs[p][1] * f, f2 = qs[p][2] * f;
+#pragma unroll
+                    for (int ix = 0; ix < B; ++ix) {
+                        const double r = row[p][ix];
+                        acc[0][ix] += f0 * r;
+                        acc[1][ix] += f1 * r;
+                        acc[2][ix] += f2 * r;
+                    }
+                }
+            }
+        }
+    }
+    const int64_t ng = S.ngrid;
+    const int64_t line = ((int64_t)(bs[2] + lz) * S.n[1] + (bs[1] + ly)) * S.n[0] + bs[0];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int ix = 0; ix < B; ++ix) grid[c * ng + line + ix] = acc[c][ix];
+}
+
+// Type-2 interpolation, one warp per node (cell order when available): lanes take (sy, sz)
+// pairs of the footprint, loop over x, and the warp reduces the three components.
+__global__ void __launch_bounds__(256) interp_warp_kernel_f64(
+    LRSizes S, int64_t Np, const int32_t* __restrict__ order, const double* __restrict__ nodes, double sx0,
+    double sx1, double sx2, const double* __restrict__ grid, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (t >= Np) return;
+    const int64_t i = order ? order[t] : t;
+    const int w = 2 * S.m;
+    const double scale[3] = {sx0, sx1, sx2};
+    double xh[3];
+    int i0[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        xh[d] = (nodes[d * Np + i] * scale[d]) / (2.0 * kPi / S.n[d]);
+        i0[d] = (int)floor(xh[d]) - S.m + 1;
+    }
+    double phx[2 * kMaxHalfSupport];
+    int ixs[2 * kMaxHalfSupport];
+    for (int s = 0; s < w; ++s) {
+        phx[s] = es_kernel(xh[0] - (i0[0] + s), S.m, S.beta, S.edge);
+        ixs[s] = wrapi(i0[0] + s, S.n[0]);
+    }
+    double a0 = 0, a1 = 0, a2 = 0;
+    const int64_t ng = S.ngrid;
+    for (int l = lane; l < w * w; l += 32) {
+        const int sy = l % w, sz = l / w;
+        const double f = es_kernel(xh[1] - (i0[1] + sy), S.m, S.beta, S.edge) *
+                         es_kernel(xh[2] - (i0[2] + sz), S.m, S.beta, S.edge);
+        const int64_t rowi = ((int64_t)wrapi(i0[2] + sz, S.n[2]) * S.n[1] + wrapi(i0[1] + sy, S.n[1])) * S.n[0];
+        double b0 = 0, b1 = 0, b2 = 0;
+        for (int sx = 0; sx < w; ++sx) {
+            const int64_t g = rowi + ixs[sx];
+            b0 += phx[sx] * grid[g];
+            b1 += phx[sx] * grid[ng + g];
+            b2 += phx[sx] * grid[2 * ng + g];
+        }
+        a0 += f * b0;
+        a1 += f * b1;
+        a2 += f * b2;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if (lane == 0) {
+        out[i] += a0;
+        out[Np + i] += a1;
+        out[2 * Np + i] += a2;
+    }
+}
+
 // Type-2 interpolation: one thread per node (visited in cell order when available).
 __global__ void __launch_bounds__(128) interp_kernel_f64(
     LRSizes S, int64_t Np, const int32_t* __restrict__ order, const double* __restrict__ nodes, double sx0,
@@ -258,6 +426,17 @@ int longrange_init(vpbs_handle* h) {
     S.m = P.m;
     S.beta = 0.97 * kPi * (1.0 - 1.0 / (2.0 * P.sigma)) * (2.0 * P.m);
     S.edge = std::exp(-S.beta);
+    // brick edge for atomic-free spreading: divides every grid size, >= kernel width, >= 2 bricks
+    h->gatherB = 0;
+    for (int B : {16, 12, 10, 8}) {
+        bool ok = B >= 2 * S.m;
+        for (int d = 0; d < 3; ++d) ok = ok && S.n[d] % B == 0 && S.n[d] / B >= 2;
+        if (ok) {
+            h->gatherB = B;
+            for (int d = 0; d < 3; ++d) h->nbrick[d] = S.n[d] / B;
+            break;
+        }
+    }
     int rc;
     if ((rc = ensure(h, h->grid_r, sizeof(double) * 3 * S.ngrid, "real grid"))) return rc;
     if ((rc = ensure(h, h->grid_c, sizeof(double2) * 3 * S.ncgrid, "complex grid"))) return rc;
@@ -316,7 +495,37 @@ int longrange_compute(vpbs_handle* h, int fields) {
     double2* gc2 = (double2*)h->grid_c2.p;
     // sources: cell-sorted copy (SoA x,y,z,qx,qy,qz), built by build_cell_lists
     const double* src = (const double*)h->src_sorted.p;
-    {
+    if (h->gatherB) {
+        StageScope st(h, ST_SPREAD);
+        const int B = h->gatherB, nb0 = h->nbrick[0], nb1 = h->nbrick[1], nb2 = h->nbrick[2];
+        const int64_t nbins = (int64_t)nb0 * nb1 * nb2, Nq = h->Nq;
+        if ((rc = ensure(h, h->spread_bin, sizeof(int32_t) * 2 * Nq, "spread bins"))) return rc;
+        if ((rc = ensure(h, h->spread_counts, sizeof(int32_t) * nbins, "spread bin counts"))) return rc;
+        if ((rc = ensure(h, h->spread_start, sizeof(int32_t) * (nbins + 1), "spread bin starts"))) return rc;
+        if ((rc = ensure(h, h->binned, sizeof(double) * 6 * Nq, "binned points"))) return rc;
+        int32_t* bin = (int32_t*)h->spread_bin.p;
+        int32_t* rank = bin + Nq;
+        int32_t* counts = (int32_t*)h->spread_counts.p;
+        int32_t* start = (int32_t*)h->spread_start.p;
+        if ((rc = check_cuda(h, cudaMemsetAsync(counts, 0, sizeof(int32_t) * nbins, h->stream), "memset"))) return rc;
+        spread_bin_count_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(S, B, nb0, nb1, nb2, Nq, src, sx[0], sx[1],
+                                                                           sx[2], bin, rank, counts);
+        h->launches++;
+        if ((rc = exclusive_scan(h, counts, start, nbins))) return rc;
+        spread_bin_scatter_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(Nq, src, bin, rank, start,
+                                                                             (double*)h->binned.p);
+        h->launches++;
+        const unsigned nblk = (unsigned)nbins;
+        const double* bsrc = (const double*)h->binned.p;
+        switch (B) {
+            case 16: spread_gather_kernel_f64<16><<<nblk, 256, 0, h->stream>>>(S, nb0, nb1, nb2, Nq, start, bsrc, sx[0], sx[1], sx[2], grid); break;
+            case 12: spread_gather_kernel_f64<12><<<nblk, 144, 0, h->stream>>>(S, nb0, nb1, nb2, Nq, start, bsrc, sx[0], sx[1], sx[2], grid); break;
+            case 10: spread_gather_kernel_f64<10><<<nblk, 100, 0, h->stream>>>(S, nb0, nb1, nb2, Nq, start, bsrc, sx[0], sx[1], sx[2], grid); break;
+            default: spread_gather_kernel_f64<8><<<nblk, 64, 0, h->stream>>>(S, nb0, nb1, nb2, Nq, start, bsrc, sx[0], sx[1], sx[2], grid); break;
+        }
+        h->launches++;
+        if ((rc = check_cuda(h, cudaGetLastError(), "spread gather kernels"))) return rc;
+    } else {
         StageScope st(h, ST_SPREAD);
         if ((rc = check_cuda(h, cudaMemsetAsync(grid, 0, sizeof(double) * 3 * S.ngrid, h->stream), "memset grid")))
             return rc;
@@ -359,9 +568,12 @@ int longrange_compute(vpbs_handle* h, int fields) {
             StageScope st(h, ST_FFT_INVERSE);
             if ((rc = check_fft(h, cufftExecZ2D(h->plan_c2r, (cufftDoubleComplex*)in, grid), "exec Z2D"))) return rc;
         }
+        if (h->interp_wait) {
+            if ((rc = check_cuda(h, cudaStreamWaitEvent(h->stream, h->interp_wait, 0), "wait short range"))) return rc;
+        }
         StageScope st(h, ST_INTERP);
-        interp_kernel_f64<<<grid_for(h->Np, 128), 128, 0, h->stream>>>(S, h->Np, order, (const double*)h->nodes.p,
-                                                                      sx[0], sx[1], sx[2], grid, out);
+        interp_warp_kernel_f64<<<grid_for(h->Np, 8), 256, 0, h->stream>>>(S, h->Np, order, (const double*)h->nodes.p,
+                                                                          sx[0], sx[1], sx[2], grid, out);
         h->launches++;
         if ((rc = check_cuda(h, cudaGetLastError(), "interp kernel"))) return rc;
     }

@@ -324,6 +324,12 @@ int build_cell_lists(vpbs_handle* h) {
     return check_cuda(h, cudaGetLastError(), "cell list kernels");
 }
 
+int exclusive_scan(vpbs_handle* h, const int32_t* counts, int32_t* start, int64_t n) {
+    scan_kernel<<<1, 1024, 0, h->stream>>>(counts, start, n);
+    h->launches++;
+    return check_cuda(h, cudaGetLastError(), "scan kernel");
+}
+
 int pair_interactions(vpbs_handle* h, int fields) {
     const int64_t Np = h->Np, Nq = h->Nq;
     const bool open = h->K.open_domain;

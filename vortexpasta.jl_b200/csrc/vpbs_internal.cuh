@@ -84,6 +84,9 @@ struct vpbs_handle {
     // long range
     vpbs::LRSizes lr{};
     vpbs::DevBuf grid_r, grid_c, grid_c2, uhat, decx, decy, decz, nodes_lr;
+    vpbs::DevBuf spread_bin, spread_counts, spread_start, binned;  // brick-gather spreading
+    int gatherB = 0;   // brick edge of the atomic-free spreading (0: atomic fallback)
+    int nbrick[3] = {0, 0, 0};
     cufftHandle plan_r2c = 0, plan_c2r = 0, plan_c2r_6 = 0;
     bool have_plans = false;
     bool have_uhat = false;
@@ -99,6 +102,11 @@ struct vpbs_handle {
     size_t pin_out_bytes = 0;
     cudaEvent_t h2d_done = nullptr;
     bool li_valid = false;  // lia_segment_fraction integrals available (filament input only)
+
+    // the long range runs on aux_stream concurrently with the short range (fork/join events)
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_short = nullptr, ev_long = nullptr;
+    cudaEvent_t interp_wait = nullptr;  // event the interpolation waits for (outputs are shared)
 
     // optional per-stage CUDA-event timing (vpbs_stage_timing)
     bool timing = false;
@@ -120,6 +128,7 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
 
 // shortrange.cu
 int build_cell_lists(vpbs_handle* h);
+int exclusive_scan(vpbs_handle* h, const int32_t* counts, int32_t* start, int64_t n);  // start[0..n]
 int local_and_self(vpbs_handle* h, int fields, int lia_mode, int with_pairs_self, double integration_cutoff);
 int pair_interactions(vpbs_handle* h, int fields);
 int add_local_integrals(vpbs_handle* h, int fields);
