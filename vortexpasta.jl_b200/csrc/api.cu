@@ -2,6 +2,7 @@
 // the compute_on_nodes! orchestration (src/BiotSavart/BiotSavart.jl:395-612).
 #include <cmath>
 #include <cstring>
+#include <algorithm>
 #include <new>
 #include <string>
 
@@ -210,7 +211,8 @@ int vpbs_destroy(vpbs_handle* h) {
                       &h->charges, &h->li_vel, &h->li_psi, &h->src_cell, &h->src_start, &h->src_fill, &h->src_sorted,
                       &h->src_seg, &h->dst_cell, &h->dst_start, &h->dst_fill, &h->dst_order, &h->counters,
                       &h->grid_r, &h->grid_c, &h->grid_c2, &h->uhat, &h->decx, &h->decy, &h->decz, &h->nodes_lr,
-                      &h->vel, &h->psi};
+                      &h->vel, &h->psi, &h->spread_bin, &h->spread_counts, &h->spread_start, &h->binned,
+                      &h->spread_foot};
     for (DevBuf* b : bufs) free_buf(*b);
     if (h->pin_in) cudaFreeHost(h->pin_in);
     if (h->pin_out) cudaFreeHost(h->pin_out);
@@ -266,7 +268,9 @@ int vpbs_set_filaments(vpbs_handle* h, int64_t nfil, const int64_t* offsets, con
     }
     if ((rc = check_cuda(h, cudaEventRecord(h->h2d_done, h->stream), "event record"))) return rc;
     h->nfil = nfil;
-    if ((rc = geometry_from_filaments(h, nfil, (const int64_t*)h->offsets.p, d_nodes))) return rc;
+    int64_t nmax = 0;
+    for (int64_t f = 0; f < nfil; ++f) nmax = std::max<int64_t>(nmax, offsets[f + 1] - offsets[f]);
+    if ((rc = geometry_from_filaments(h, nfil, (const int64_t*)h->offsets.p, d_nodes, nmax))) return rc;
     h->li_valid = h->K.lia_fraction > 0;
     return process_point_charges(h);
 }

@@ -106,24 +106,26 @@ __device__ void solve4(double H[4][4], double r[4][3]) {
         }
 }
 
-// One warp per filament.  scratch: 12 doubles per node (5 band + 7 right-hand sides).
+// One warp per filament.  Work space: 12 doubles per node (5 band + 7 right-hand sides), in
+// dynamic shared memory (smem_n doubles x 12 per warp) when smem_n > 0, else in `scratch`.
 __global__ void __launch_bounds__(128) spline_solve_kernel(
     int64_t nfil, const int64_t* __restrict__ offsets, const double* __restrict__ X,
     double* __restrict__ knots, double* __restrict__ periods, int32_t* __restrict__ fil_of_node,
     double* __restrict__ coef, double* __restrict__ dcoef1, double* __restrict__ dcoef2,
-    double* __restrict__ scratch, int32_t* __restrict__ status) {
+    double* __restrict__ scratch, int32_t* __restrict__ status, int smem_n) {
+    extern __shared__ double sm_work[];
     const int lane = threadIdx.x & 31;
     const int64_t fidx = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (fidx >= nfil) return;
     const int64_t off = offsets[fidx];
     const int n = (int)(offsets[fidx + 1] - off);
-    if (n < 5) {
+    if (n < 5 || (smem_n > 0 && n > smem_n)) {
         if (lane == 0) atomicExch(status, 1);
         return;
     }
     const double* Xf = X + 3 * off;
     double* t = knots + off;
-    double* band = scratch + 12 * off;      // [n][5]
+    double* band = smem_n > 0 ? sm_work + (size_t)(threadIdx.x >> 5) * 12 * smem_n : scratch + 12 * off;  // [n][5]
     double* Y = band + 5 * (int64_t)n;      // [n][7]
     double* c = coef + 3 * off;
     double* c1 = dcoef1 + 3 * off;
@@ -327,18 +329,9 @@ __global__ void __launch_bounds__(128) point_data_kernel(
     const bool has_g = g > 0;
     dm[k] = seg_len(f, c1, i - 1, K.nquad, K.qz, K.qw, has_g ? 1.0 - g : 0.0, 1.0);
     dp[k] = seg_len(f, c1, i, K.nquad, K.qz, K.qw, 0.0, has_g ? g : 1.0);
-    const double dt = knot_at(f, i + 1) - knot_at(f, i);
-    for (int q = 0; q < K.nquad; ++q) {
-        const int64_t mq = k * K.nquad + q;
-        double s[3], sp[3];
-        eval_seg<0>(f, c, i, K.qz[q], s);
-        eval_seg<1>(f, c1, i, K.qz[q], sp);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            points[d * Nq + mq] = fold(s[d], K.L[d], K.open_domain);
-            charges[d * Nq + mq] = K.qw[q] * dt * sp[d];
-        }
-    }
+    (void)Nq;
+    (void)points;
+    (void)charges;
     if (want_li) {
         // nonlia_integration_limits: ((0, 1-g), (g, 1))  (local_integrals.jl:103-104)
         double v[3] = {0, 0, 0}, ps[3] = {0, 0, 0};
@@ -374,11 +367,55 @@ __global__ void __launch_bounds__(128) point_data_kernel(
     }
 }
 
+// One thread per quadrature point: points = fold(s(zeta_q)), charges = w_q dt s'(zeta_q) on the
+// segment to the right of node i (pointdata_impl.jl:93-103).
+__global__ void __launch_bounds__(128) quad_points_kernel(
+    KParams K, int64_t Np, const int64_t* __restrict__ offsets, const int32_t* __restrict__ fil_of_node,
+    const double* __restrict__ knots, const double* __restrict__ periods, const double* __restrict__ coef,
+    const double* __restrict__ dcoef1, double* __restrict__ points, double* __restrict__ charges) {
+    const int64_t Nq = Np * K.nquad;
+    const int64_t mq = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (mq >= Nq) return;
+    const int64_t k = mq / K.nquad;
+    const int q = (int)(mq - k * K.nquad);
+    const int fidx = fil_of_node[k];
+    const int64_t off = offsets[fidx];
+    const int n = (int)(offsets[fidx + 1] - off);
+    const int i = (int)(k - off);
+    FilView f{knots + off, periods[fidx], n};
+    double s[3], sp[3];
+    eval_seg<0>(f, coef + 3 * off, i, K.qz[q], s);
+    eval_seg<1>(f, dcoef1 + 3 * off, i, K.qz[q], sp);
+    const double dt = knot_at(f, i + 1) - knot_at(f, i);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        points[d * Nq + mq] = fold(s[d], K.L[d], K.open_domain);
+        charges[d * Nq + mq] = K.qw[q] * dt * sp[d];
+    }
+}
+
 }  // namespace
 
-int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offsets, const double* d_nodes) {
+// Shared-memory work space of the spline solve for filaments of at most nmax nodes (4 warps per
+// block, 12 doubles per node each); 0 when it does not fit and the global scratch is used.
+static int solve_smem_n(int64_t nmax, size_t* bytes) {
+    const size_t b = (size_t)4 * 12 * nmax * sizeof(double);
+    if (nmax > 0 && b <= 200 * 1024) {
+        *bytes = b;
+        return (int)nmax;
+    }
+    *bytes = 0;
+    return 0;
+}
+
+int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offsets, const double* d_nodes,
+                            int64_t nmax) {
     const int64_t Np = h->Np;
     int rc;
+    size_t smem_bytes = 0;
+    const int smem_n = solve_smem_n(nmax, &smem_bytes);
+    if (smem_bytes > 48 * 1024)
+        cudaFuncSetAttribute(spline_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
     if ((rc = ensure(h, h->knots, sizeof(double) * (Np + nfil), "knots"))) return rc;
     if ((rc = ensure(h, h->fil_of_node, sizeof(int32_t) * Np, "fil_of_node"))) return rc;
     if ((rc = ensure(h, h->coefs, sizeof(double) * 3 * Np, "coefs"))) return rc;
@@ -390,9 +427,9 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
     int32_t* status = (int32_t*)((double*)h->spline_scratch.p + 12 * Np);
     StageScope st(h, ST_GEOMETRY);
     if ((rc = check_cuda(h, cudaMemsetAsync(status, 0, sizeof(int32_t), h->stream), "memset"))) return rc;
-    spline_solve_kernel<<<grid_for(nfil, 4), 128, 0, h->stream>>>(
+    spline_solve_kernel<<<grid_for(nfil, 4), 128, smem_bytes, h->stream>>>(
         nfil, d_offsets, d_nodes, knots, periods, (int32_t*)h->fil_of_node.p, (double*)h->coefs.p,
-        (double*)h->dcoef1.p, (double*)h->dcoef2.p, (double*)h->spline_scratch.p, status);
+        (double*)h->dcoef1.p, (double*)h->dcoef2.p, (double*)h->spline_scratch.p, status, smem_n);
     h->launches++;
     const bool want_li = h->K.lia_fraction > 0;
     point_data_kernel<<<grid_for(Np, 128), 128, 0, h->stream>>>(
@@ -400,7 +437,10 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
         (const double*)h->dcoef1.p, (const double*)h->dcoef2.p, (double*)h->nodes.p, (int32_t*)h->idx_prev.p,
         (double*)h->d1.p, (double*)h->d2.p, (double*)h->dm.p, (double*)h->dp.p, (double*)h->points.p,
         (double*)h->charges.p, (double*)h->li_vel.p, (double*)h->li_psi.p, want_li ? 1 : 0);
-    h->launches++;
+    quad_points_kernel<<<grid_for(Np * h->K.nquad, 128), 128, 0, h->stream>>>(
+        h->K, Np, d_offsets, (const int32_t*)h->fil_of_node.p, knots, periods, (const double*)h->coefs.p,
+        (const double*)h->dcoef1.p, (double*)h->points.p, (double*)h->charges.p);
+    h->launches += 2;
     return check_cuda(h, cudaGetLastError(), "geometry kernels");
 }
 
@@ -510,10 +550,12 @@ extern "C" int vpbs_point_data_noalloc(const vpbs_params* params, int64_t nfil, 
     if (e != cudaSuccess)
         return set_error(nullptr, VPBS_ERR_CUDA, std::string("vpbs_point_data_noalloc: ") + cudaGetErrorString(e));
     spline_solve_kernel<<<grid_for(nfil, 4), 128, 0, s>>>(nfil, d_offsets, nodes_xyz, knots, periods, fil_of_node, coefs,
-                                                          dcoef1, dcoef2, scratch, status);
+                                                          dcoef1, dcoef2, scratch, status, 0);
     point_data_kernel<<<grid_for(Np, 128), 128, 0, s>>>(K, Np, d_offsets, fil_of_node, nodes_xyz, knots, periods, coefs,
                                                         dcoef1, dcoef2, nodes, node_idx_prev, deriv1, deriv2,
                                                         delta_minus, delta_plus, points, charges, nullptr, nullptr, 0);
+    quad_points_kernel<<<grid_for(Np * K.nquad, 128), 128, 0, s>>>(K, Np, d_offsets, fil_of_node, knots, periods, coefs,
+                                                                   dcoef1, points, charges);
     e = cudaGetLastError();
     if (e != cudaSuccess)
         return set_error(nullptr, VPBS_ERR_CUDA, std::string("vpbs_point_data_noalloc: ") + cudaGetErrorString(e));

@@ -196,12 +196,12 @@ __global__ void __launch_bounds__(256) fourier_kernel_f64(
     }
 }
 
-// ---- atomic-free spreading ("brick gather") ----
+// ---- brick spreading (no global atomics) ----
 // The oversampled grid is tiled into bricks of B^3 points.  Points are binned by the brick
 // holding the first grid point of their footprint; a footprint of w <= B points can then only
-// reach the brick of its bin and the next one in each direction, so brick b gathers the points
-// of bins b and b-1 (per dimension, periodic).  Each thread of the B*B-thread CTA owns one
-// x-line of the brick in registers; every grid value is written exactly once, with plain stores.
+// reach the brick of its bin and the next one in each direction, so brick b collects the points
+// of bins b and b-1 (per dimension, periodic).  Every grid value is written exactly once, with
+// plain stores, by the CTA that owns its brick.
 
 __device__ __forceinline__ int footprint_start(double x, double scale, int n, int m) {
     const double xh = (x * scale) / (2.0 * kPi / n);
@@ -222,95 +222,108 @@ __global__ void spread_bin_count_kernel(LRSizes S, int B, int nb0, int nb1, int 
     rank[j] = atomicAdd(&counts[b], 1);
 }
 
-__global__ void spread_bin_scatter_kernel(int64_t Nq, const double* __restrict__ src, const int32_t* __restrict__ bin,
+// Scatter the points into bin order, with everything the brick kernel needs per point: the
+// wrapped footprint start per dimension, the 3 x w kernel values and the 3 charges.
+// binned layout per slot: [3 charges][3 w kernel values] (doubles), foot: [3] int32.
+__global__ void spread_bin_scatter_kernel(LRSizes S, int64_t Nq, const double* __restrict__ src, double sx0,
+                                          double sx1, double sx2, const int32_t* __restrict__ bin,
                                           const int32_t* __restrict__ rank, const int32_t* __restrict__ start,
-                                          double* __restrict__ binned) {
+                                          double* __restrict__ binned, int32_t* __restrict__ foot) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= Nq) return;
     const int64_t pos = (int64_t)start[bin[j]] + rank[j];
+    const int w = 2 * S.m;
+    const int stride = 3 + 3 * w;
+    double* out = binned + pos * stride;
 #pragma unroll
-    for (int c = 0; c < 6; ++c) binned[c * Nq + pos] = src[c * Nq + j];
+    for (int c = 0; c < 3; ++c) out[c] = src[(3 + c) * Nq + j];
+    const double scale[3] = {sx0, sx1, sx2};
+    for (int d = 0; d < 3; ++d) {
+        const double xh = (src[d * Nq + j] * scale[d]) / (2.0 * kPi / S.n[d]);
+        const int i0 = (int)floor(xh) - S.m + 1;
+        foot[3 * pos + d] = wrapi(i0, S.n[d]);
+        for (int s = 0; s < w; ++s) out[3 + d * w + s] = es_kernel(xh - (i0 + s), S.m, S.beta, S.edge);
+    }
 }
 
-constexpr int kGatherChunk = 32;
+// Shared-memory brick spreading: one CTA per brick keeps the brick's three components in
+// shared memory (x rows padded to B+1 against bank conflicts), adds the part of every nearby
+// footprint that falls inside the brick with shared-memory atomics (one warp per point, lanes
+// over the footprint's (y, z) lines), then writes the brick to the grid with plain stores.
+constexpr int kBrickThreads = 256;
 
 template <int B>
-__global__ void __launch_bounds__(B * B) spread_gather_kernel_f64(
-    LRSizes S, int nb0, int nb1, int nb2, int64_t Nq, const int32_t* __restrict__ bin_start,
-    const double* __restrict__ binned, double sx0, double sx1, double sx2, double* __restrict__ grid) {
-    __shared__ double row[kGatherChunk][B];                     // x-profile aligned to the brick
-    __shared__ double phy[kGatherChunk][2 * kMaxHalfSupport];
-    __shared__ double phz[kGatherChunk][2 * kMaxHalfSupport];
-    __shared__ double qs[kGatherChunk][3];
-    __shared__ int oys[kGatherChunk], ozs[kGatherChunk];
+__global__ void __launch_bounds__(kBrickThreads) spread_brick_kernel_f64(
+    LRSizes S, int nb0, int nb1, int nb2, const int32_t* __restrict__ bin_start, const double* __restrict__ binned,
+    const int32_t* __restrict__ foot, double* __restrict__ grid) {
+    extern __shared__ double tile[];  // [3][B][PZ] with rows of RX doubles
+    __shared__ double phw[kBrickThreads / 32][3 + 6 * kMaxHalfSupport];
+    constexpr int RX = B + 1;        // x-row stride (bank spread along y)
+    constexpr int PZ = B * RX + 8;   // z-plane stride (16-word bank shift between planes)
+    constexpr int TC = B * PZ;       // doubles per component
     const int w = 2 * S.m;
+    const int stride = 3 + 3 * w;
     const int bx = blockIdx.x % nb0;
     const int by = (blockIdx.x / nb0) % nb1;
     const int bz = blockIdx.x / (nb0 * nb1);
     const int bs[3] = {bx * B, by * B, bz * B};
-    const int ly = threadIdx.x % B, lz = threadIdx.x / B;
-    const double scale[3] = {sx0, sx1, sx2};
-    double acc[3][B];
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int i = 0; i < B; ++i) acc[c][i] = 0.0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < 3 * TC; i += kBrickThreads) tile[i] = 0.0;
+    __syncthreads();
+    double* ph = phw[warp];  // [q0 q1 q2 | phi_x[w] | phi_y[w] | phi_z[w]]
     for (int nbr = 0; nbr < 8; ++nbr) {
         const int cx = (bx - (nbr & 1) + nb0) % nb0;
         const int cy = (by - ((nbr >> 1) & 1) + nb1) % nb1;
         const int cz = (bz - ((nbr >> 2) & 1) + nb2) % nb2;
         const int b = (cz * nb1 + cy) * nb0 + cx;
-        const int64_t p0 = bin_start[b], p1 = bin_start[b + 1];
-        for (int64_t base = p0; base < p1; base += kGatherChunk) {
-            const int np = (int)((p1 - base) < kGatherChunk ? (p1 - base) : kGatherChunk);
-            __syncthreads();
-            for (int idx = threadIdx.x; idx < np * 3; idx += B * B) {
-                const int p = idx / 3, d = idx % 3;
-                const int64_t j = base + p;
-                const double xh = (binned[d * Nq + j] * scale[d]) / (2.0 * kPi / S.n[d]);
-                const int i0 = (int)floor(xh) - S.m + 1;
-                int o = wrapi(i0, S.n[d]) - bs[d];
-                if (o >= B) o -= S.n[d];  // footprint starts in the previous brick (periodic)
-                if (d == 0) {
-                    for (int ix = 0; ix < B; ++ix) {
-                        const int s = ix - o;
-                        row[p][ix] = (s >= 0 && s < w) ? es_kernel(xh - (i0 + s), S.m, S.beta, S.edge) : 0.0;
-                    }
-                } else {
-                    double* ph = d == 1 ? phy[p] : phz[p];
-                    for (int s = 0; s < w; ++s) ph[s] = es_kernel(xh - (i0 + s), S.m, S.beta, S.edge);
-                    if (d == 1) oys[p] = o;
-                    else ozs[p] = o;
-                }
-                qs[p][d] = binned[(3 + d) * Nq + j];
-            }
-            __syncthreads();
-            for (int p = 0; p < np; ++p) {
-                const int sy = ly - oys[p], sz = lz - ozs[p];
-                if ((unsigned)sy < (unsigned)w && (unsigned)sz < (unsigned)w) {
-                    const double f = phy[p][sy] * phz[p][sz];
-                    const double f0 = qs[p][0] * f, f1 = qs[p][1] * f, f2 = qs[p][2] * f;
+        const int64_t p1 = bin_start[b + 1];
+        for (int64_t j = bin_start[b] + warp; j < p1; j += kBrickThreads / 32) {
+            // footprint offset relative to the brick (periodic) and overlap range, per dimension
+            int o[3], lo[3], hi[3];
+            bool empty = false;
 #pragma unroll
-                    for (int ix = 0; ix < B; ++ix) {
-                        const double r = row[p][ix];
-                        acc[0][ix] += f0 * r;
-                        acc[1][ix] += f1 * r;
-                        acc[2][ix] += f2 * r;
-                    }
+            for (int d = 0; d < 3; ++d) {
+                o[d] = foot[3 * j + d] - bs[d];
+                if (o[d] >= B) o[d] -= S.n[d];
+                lo[d] = o[d] < 0 ? -o[d] : 0;
+                hi[d] = B - o[d] < w ? B - o[d] : w;
+                empty = empty || lo[d] >= hi[d];
+            }
+            if (empty) continue;  // warp-uniform
+            for (int it = lane; it < stride; it += 32) ph[it] = binned[j * stride + it];
+            __syncwarp();
+            const double q0 = ph[0], q1 = ph[1], q2 = ph[2];
+            const double* phx = ph + 3;
+            const double* phy = phx + w;
+            const double* phz = phy + w;
+            const int ny = hi[1] - lo[1], nz = hi[2] - lo[2];
+            for (int l = lane; l < ny * nz; l += 32) {
+                const int sy = lo[1] + l % ny, sz = lo[2] + l / ny;
+                const double f = phy[sy] * phz[sz];
+                double* row = tile + (o[2] + sz) * PZ + (o[1] + sy) * RX + o[0];
+                for (int sx = lo[0]; sx < hi[0]; ++sx) {
+                    const double g = f * phx[sx];
+                    atomicAdd(row + sx, q0 * g);
+                    atomicAdd(row + TC + sx, q1 * g);
+                    atomicAdd(row + 2 * TC + sx, q2 * g);
                 }
             }
+            __syncwarp();
         }
     }
+    __syncthreads();
     const int64_t ng = S.ngrid;
-    const int64_t line = ((int64_t)(bs[2] + lz) * S.n[1] + (bs[1] + ly)) * S.n[0] + bs[0];
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int ix = 0; ix < B; ++ix) grid[c * ng + line + ix] = acc[c][ix];
+    for (int i = threadIdx.x; i < 3 * B * B * B; i += kBrickThreads) {
+        const int c = i / (B * B * B), r = i % (B * B * B);
+        const int x = r % B, y = (r / B) % B, z = r / (B * B);
+        grid[c * ng + ((int64_t)(bs[2] + z) * S.n[1] + (bs[1] + y)) * S.n[0] + bs[0] + x] =
+            tile[c * TC + z * PZ + y * RX + x];
+    }
 }
 
 // Type-2 interpolation, one warp per node (cell order when available): lanes take (sy, sz)
 // pairs of the footprint, loop over x, and the warp reduces the three components.
+template <int W>  // kernel width 2m (compile-time, so the per-lane tables stay in registers)
 __global__ void __launch_bounds__(256) interp_warp_kernel_f64(
     LRSizes S, int64_t Np, const int32_t* __restrict__ order, const double* __restrict__ nodes, double sx0,
     double sx1, double sx2, const double* __restrict__ grid, double* __restrict__ out) {
@@ -318,7 +331,7 @@ __global__ void __launch_bounds__(256) interp_warp_kernel_f64(
     const int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (t >= Np) return;
     const int64_t i = order ? order[t] : t;
-    const int w = 2 * S.m;
+    constexpr int w = W;
     const double scale[3] = {sx0, sx1, sx2};
     double xh[3];
     int i0[3];
@@ -327,8 +340,9 @@ __global__ void __launch_bounds__(256) interp_warp_kernel_f64(
         xh[d] = (nodes[d * Np + i] * scale[d]) / (2.0 * kPi / S.n[d]);
         i0[d] = (int)floor(xh[d]) - S.m + 1;
     }
-    double phx[2 * kMaxHalfSupport];
-    int ixs[2 * kMaxHalfSupport];
+    double phx[w];
+    int ixs[w];
+#pragma unroll
     for (int s = 0; s < w; ++s) {
         phx[s] = es_kernel(xh[0] - (i0[0] + s), S.m, S.beta, S.edge);
         ixs[s] = wrapi(i0[0] + s, S.n[0]);
@@ -341,6 +355,7 @@ __global__ void __launch_bounds__(256) interp_warp_kernel_f64(
                          es_kernel(xh[2] - (i0[2] + sz), S.m, S.beta, S.edge);
         const int64_t rowi = ((int64_t)wrapi(i0[2] + sz, S.n[2]) * S.n[1] + wrapi(i0[1] + sy, S.n[1])) * S.n[0];
         double b0 = 0, b1 = 0, b2 = 0;
+#pragma unroll
         for (int sx = 0; sx < w; ++sx) {
             const int64_t g = rowi + ixs[sx];
             b0 += phx[sx] * grid[g];
@@ -362,46 +377,6 @@ __global__ void __launch_bounds__(256) interp_warp_kernel_f64(
         out[Np + i] += a1;
         out[2 * Np + i] += a2;
     }
-}
-
-// Type-2 interpolation: one thread per node (visited in cell order when available).
-__global__ void __launch_bounds__(128) interp_kernel_f64(
-    LRSizes S, int64_t Np, const int32_t* __restrict__ order, const double* __restrict__ nodes, double sx0,
-    double sx1, double sx2, const double* __restrict__ grid, double* __restrict__ out) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= Np) return;
-    const int64_t i = order ? order[t] : t;
-    const int w = 2 * S.m;
-    const double scale[3] = {sx0, sx1, sx2};
-    double phi[3][2 * kMaxHalfSupport];
-    int i0[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const double h = 2.0 * kPi / S.n[d];
-        const double xh = (nodes[d * Np + i] * scale[d]) / h;
-        i0[d] = (int)floor(xh) - S.m + 1;
-        for (int s = 0; s < w; ++s) phi[d][s] = es_kernel(xh - (i0[d] + s), S.m, S.beta, S.edge);
-    }
-    double a0 = 0, a1 = 0, a2 = 0;
-    const int64_t ng = S.ngrid;
-    for (int sz = 0; sz < w; ++sz) {
-        const int iz = wrapi(i0[2] + sz, S.n[2]);
-        for (int sy = 0; sy < w; ++sy) {
-            const int iy = wrapi(i0[1] + sy, S.n[1]);
-            const double fyz = phi[2][sz] * phi[1][sy];
-            const int64_t row = ((int64_t)iz * S.n[1] + iy) * S.n[0];
-            for (int sx = 0; sx < w; ++sx) {
-                const int ix = wrapi(i0[0] + sx, S.n[0]);
-                const double f = fyz * phi[0][sx];
-                a0 += f * grid[row + ix];
-                a1 += f * grid[ng + row + ix];
-                a2 += f * grid[2 * ng + row + ix];
-            }
-        }
-    }
-    out[i] += a0;
-    out[Np + i] += a1;
-    out[2 * Np + i] += a2;
 }
 
 int check_fft(vpbs_handle* h, cufftResult r, const char* what) {
@@ -502,26 +477,34 @@ int longrange_compute(vpbs_handle* h, int fields) {
         if ((rc = ensure(h, h->spread_bin, sizeof(int32_t) * 2 * Nq, "spread bins"))) return rc;
         if ((rc = ensure(h, h->spread_counts, sizeof(int32_t) * nbins, "spread bin counts"))) return rc;
         if ((rc = ensure(h, h->spread_start, sizeof(int32_t) * (nbins + 1), "spread bin starts"))) return rc;
-        if ((rc = ensure(h, h->binned, sizeof(double) * 6 * Nq, "binned points"))) return rc;
+        const int stride = 3 + 6 * S.m;  // doubles per binned point
+        if ((rc = ensure(h, h->binned, sizeof(double) * stride * Nq, "binned points"))) return rc;
+        if ((rc = ensure(h, h->spread_foot, sizeof(int32_t) * 3 * Nq, "footprints"))) return rc;
         int32_t* bin = (int32_t*)h->spread_bin.p;
         int32_t* rank = bin + Nq;
         int32_t* counts = (int32_t*)h->spread_counts.p;
         int32_t* start = (int32_t*)h->spread_start.p;
+        int32_t* foot = (int32_t*)h->spread_foot.p;
         if ((rc = check_cuda(h, cudaMemsetAsync(counts, 0, sizeof(int32_t) * nbins, h->stream), "memset"))) return rc;
         spread_bin_count_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(S, B, nb0, nb1, nb2, Nq, src, sx[0], sx[1],
                                                                            sx[2], bin, rank, counts);
         h->launches++;
         if ((rc = exclusive_scan(h, counts, start, nbins))) return rc;
-        spread_bin_scatter_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(Nq, src, bin, rank, start,
-                                                                             (double*)h->binned.p);
+        spread_bin_scatter_kernel<<<grid_for(Nq, 128), 128, 0, h->stream>>>(S, Nq, src, sx[0], sx[1], sx[2], bin, rank,
+                                                                             start, (double*)h->binned.p, foot);
         h->launches++;
         const unsigned nblk = (unsigned)nbins;
         const double* bsrc = (const double*)h->binned.p;
+        const size_t smem = sizeof(double) * 3 * B * (B * (B + 1) + 8);
+        auto launch = [&](auto kern) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            kern<<<nblk, kBrickThreads, smem, h->stream>>>(S, nb0, nb1, nb2, start, bsrc, foot, grid);
+        };
         switch (B) {
-            case 16: spread_gather_kernel_f64<16><<<nblk, 256, 0, h->stream>>>(S, nb0, nb1, nb2, Nq, start, bsrc, sx[0], sx[1], sx[2], grid); break;
-            case 12: spread_gather_kernel_f64<12><<<nblk, 144, 0, h->stream>>>(S, nb0, nb1, nb2, Nq, start, bsrc, sx[0], sx[1], sx[2], grid); break;
-            case 10: spread_gather_kernel_f64<10><<<nblk, 100, 0, h->stream>>>(S, nb0, nb1, nb2, Nq, start, bsrc, sx[0], sx[1], sx[2], grid); break;
-            default: spread_gather_kernel_f64<8><<<nblk, 64, 0, h->stream>>>(S, nb0, nb1, nb2, Nq, start, bsrc, sx[0], sx[1], sx[2], grid); break;
+            case 16: launch(spread_brick_kernel_f64<16>); break;
+            case 12: launch(spread_brick_kernel_f64<12>); break;
+            case 10: launch(spread_brick_kernel_f64<10>); break;
+            default: launch(spread_brick_kernel_f64<8>); break;
         }
         h->launches++;
         if ((rc = check_cuda(h, cudaGetLastError(), "spread gather kernels"))) return rc;
@@ -572,8 +555,20 @@ int longrange_compute(vpbs_handle* h, int fields) {
             if ((rc = check_cuda(h, cudaStreamWaitEvent(h->stream, h->interp_wait, 0), "wait short range"))) return rc;
         }
         StageScope st(h, ST_INTERP);
-        interp_warp_kernel_f64<<<grid_for(h->Np, 8), 256, 0, h->stream>>>(S, h->Np, order, (const double*)h->nodes.p,
-                                                                          sx[0], sx[1], sx[2], grid, out);
+        auto launch_interp = [&](auto kern) {
+            kern<<<grid_for(h->Np, 8), 256, 0, h->stream>>>(S, h->Np, order, (const double*)h->nodes.p, sx[0], sx[1],
+                                                            sx[2], grid, out);
+        };
+        switch (S.m) {
+            case 1: launch_interp(interp_warp_kernel_f64<2>); break;
+            case 2: launch_interp(interp_warp_kernel_f64<4>); break;
+            case 3: launch_interp(interp_warp_kernel_f64<6>); break;
+            case 4: launch_interp(interp_warp_kernel_f64<8>); break;
+            case 5: launch_interp(interp_warp_kernel_f64<10>); break;
+            case 6: launch_interp(interp_warp_kernel_f64<12>); break;
+            case 7: launch_interp(interp_warp_kernel_f64<14>); break;
+            default: launch_interp(interp_warp_kernel_f64<16>); break;
+        }
         h->launches++;
         if ((rc = check_cuda(h, cudaGetLastError(), "interp kernel"))) return rc;
     }

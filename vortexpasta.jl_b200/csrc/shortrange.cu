@@ -98,40 +98,82 @@ struct PairAcc {
     unsigned long long inr, cand;
 };
 
+// Per-warp queue of in-range pairs: the separations and source indices of candidates that
+// passed the r^2 <= r_cut^2 test are compacted here (ballot + prefix popcount), so that the
+// erfc/exp evaluation always runs on 32 live lanes instead of on the ~30% of lanes whose
+// candidate happened to be in range.
+constexpr int kPairThreads = 256;
+constexpr int kQueue = 64;
+struct PairQueue {
+    double r[3][kQueue];
+    int32_t j[kQueue];
+};
+
 template <bool VEL, bool PSI>
-__device__ __forceinline__ void pair_range(const KParams& K, const double x[3], int64_t i, int32_t iprev, bool skip_local,
-                                           const double* __restrict__ src, int64_t Ns, const int32_t* __restrict__ seg,
-                                           int64_t b, int64_t e, int lane, PairAcc& acc) {
+__device__ __forceinline__ void pair_eval(const KParams& K, const double* __restrict__ src, int64_t Ns,
+                                          const PairQueue& Q, int k, PairAcc& acc) {
     const double two_over_sqrt_pi = 1.1283791670955126;  // 2/sqrt(pi)
-    for (int64_t j = b + lane; j < e; j += 32) {
-        if (skip_local) {
-            int32_t sj = seg[j];
-            if (sj == i || sj == iprev) continue;
+    const double r0 = Q.r[0][k], r1 = Q.r[1][k], r2 = Q.r[2][k];
+    const int64_t j = Q.j[k];
+    const double q0 = src[3 * Ns + j], q1 = src[4 * Ns + j], q2 = src[5 * Ns + j];
+    const double r = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
+    const double rinv = 1.0 / r;
+    const double ar = K.alpha * r;
+    const double wa = erfc(ar);
+    if (VEL) {
+        const double wb = two_over_sqrt_pi * ar * exp(-(ar * ar));
+        const double f = (wa + wb) * rinv * rinv * rinv;
+        acc.v[0] += f * (q1 * r2 - q2 * r1);
+        acc.v[1] += f * (q2 * r0 - q0 * r2);
+        acc.v[2] += f * (q0 * r1 - q1 * r0);
+    }
+    if (PSI) {
+        const double f = wa * rinv;
+        acc.p[0] += f * q0;
+        acc.p[1] += f * q1;
+        acc.p[2] += f * q2;
+    }
+}
+
+template <bool VEL, bool PSI>
+__device__ __forceinline__ void pair_range_q(const KParams& K, const double x[3], int64_t i, int32_t iprev,
+                                             bool skip_local, const double* __restrict__ src, int64_t Ns,
+                                             const int32_t* __restrict__ seg, int64_t b, int64_t e, int lane,
+                                             PairAcc& acc, PairQueue& Q, int& qcount) {
+    for (int64_t base = b; base < e; base += 32) {
+        const int64_t j = base + lane;
+        bool inr = false;
+        double r0 = 0, r1 = 0, r2 = 0;
+        if (j < e && !(skip_local && (seg[j] == i || seg[j] == iprev))) {
+            r0 = deper(x[0] - src[j], K.L[0], K.Lh[0], K.open_domain);
+            r1 = deper(x[1] - src[Ns + j], K.L[1], K.Lh[1], K.open_domain);
+            r2 = deper(x[2] - src[2 * Ns + j], K.L[2], K.Lh[2], K.open_domain);
+            acc.cand++;
+            inr = r0 * r0 + r1 * r1 + r2 * r2 <= K.rcut2;
         }
-        double r0 = deper(x[0] - src[j], K.L[0], K.Lh[0], K.open_domain);
-        double r1 = deper(x[1] - src[Ns + j], K.L[1], K.Lh[1], K.open_domain);
-        double r2 = deper(x[2] - src[2 * Ns + j], K.L[2], K.Lh[2], K.open_domain);
-        double rr2 = r0 * r0 + r1 * r1 + r2 * r2;
-        acc.cand++;
-        if (!(rr2 <= K.rcut2)) continue;
-        acc.inr++;
-        double q0 = src[3 * Ns + j], q1 = src[4 * Ns + j], q2 = src[5 * Ns + j];
-        double r = sqrt(rr2);
-        double rinv = 1.0 / r;
-        double ar = K.alpha * r;
-        double wa = erfc(ar);
-        if (VEL) {
-            double wb = two_over_sqrt_pi * ar * exp(-(ar * ar));
-            double f = (wa + wb) * rinv * rinv * rinv;
-            acc.v[0] += f * (q1 * r2 - q2 * r1);
-            acc.v[1] += f * (q2 * r0 - q0 * r2);
-            acc.v[2] += f * (q0 * r1 - q1 * r0);
+        const unsigned m = __ballot_sync(0xffffffffu, inr);
+        if (inr) {
+            const int pos = qcount + __popc(m & ((1u << lane) - 1u));
+            Q.r[0][pos] = r0;
+            Q.r[1][pos] = r1;
+            Q.r[2][pos] = r2;
+            Q.j[pos] = (int32_t)j;
+            acc.inr++;
         }
-        if (PSI) {
-            double f = wa * rinv;
-            acc.p[0] += f * q0;
-            acc.p[1] += f * q1;
-            acc.p[2] += f * q2;
+        qcount += __popc(m);
+        __syncwarp();
+        if (qcount >= 32) {
+            pair_eval<VEL, PSI>(K, src, Ns, Q, lane, acc);
+            __syncwarp();
+            const int rest = qcount - 32;
+            if (lane < rest) {
+                Q.r[0][lane] = Q.r[0][32 + lane];
+                Q.r[1][lane] = Q.r[1][32 + lane];
+                Q.r[2][lane] = Q.r[2][32 + lane];
+                Q.j[lane] = Q.j[32 + lane];
+            }
+            __syncwarp();
+            qcount = rest;
         }
     }
 }
@@ -155,15 +197,18 @@ __global__ void __launch_bounds__(256) pair_kernel_f64(
     const double* __restrict__ nodes, const int32_t* __restrict__ idx_prev, const double* __restrict__ src,
     const int32_t* __restrict__ src_start, const int32_t* __restrict__ seg, int use_cells, int skip_local,
     double* __restrict__ vel, double* __restrict__ psi, unsigned long long* __restrict__ counters) {
+    __shared__ PairQueue queues[kPairThreads / 32];
     const int lane = threadIdx.x & 31;
     const int64_t w = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (w >= Np) return;
+    PairQueue& Q = queues[threadIdx.x >> 5];
+    int qcount = 0;
     const int64_t i = use_cells ? dst_order[w] : w;
     const double x[3] = {nodes[i], nodes[Np + i], nodes[2 * Np + i]};
     const int32_t iprev = idx_prev[i];
     PairAcc acc = {{0, 0, 0}, {0, 0, 0}, 0ull, 0ull};
     if (!use_cells) {
-        pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, 0, Ns, lane, acc);
+        pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, 0, Ns, lane, acc, Q, qcount);
     } else {
         const int M = cg.M;
         const int nc0 = cg.nc[0], nc1 = cg.nc[1], nc2 = cg.nc[2];
@@ -179,22 +224,23 @@ __global__ void __launch_bounds__(256) pair_kernel_f64(
                 const int64_t base = ((int64_t)zz * nc1 + yy) * nc0;
                 const int lo = cx - M, hi = cx + M;
                 if (lo >= 0 && hi < nc0) {
-                    pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo],
-                                         src_start[base + hi + 1], lane, acc);
+                    pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo],
+                                         src_start[base + hi + 1], lane, acc, Q, qcount);
                 } else if (lo < 0) {
-                    pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo + nc0],
-                                         src_start[base + nc0], lane, acc);
-                    pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base],
-                                         src_start[base + hi + 1], lane, acc);
+                    pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo + nc0],
+                                         src_start[base + nc0], lane, acc, Q, qcount);
+                    pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base],
+                                         src_start[base + hi + 1], lane, acc, Q, qcount);
                 } else {
-                    pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo],
-                                         src_start[base + nc0], lane, acc);
-                    pair_range<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base],
-                                         src_start[base + hi - nc0 + 1], lane, acc);
+                    pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo],
+                                         src_start[base + nc0], lane, acc, Q, qcount);
+                    pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base],
+                                         src_start[base + hi - nc0 + 1], lane, acc, Q, qcount);
                 }
             }
         }
     }
+    if (lane < qcount) pair_eval<VEL, PSI>(K, src, Ns, Q, lane, acc);  // queue remainder
     const double pref = K.Gamma / (4.0 * kPi);
     double v0 = 0, v1 = 0, v2 = 0, p0 = 0, p1 = 0, p2 = 0;
     if (VEL) { v0 = warp_sum(acc.v[0]); v1 = warp_sum(acc.v[1]); v2 = warp_sum(acc.v[2]); }

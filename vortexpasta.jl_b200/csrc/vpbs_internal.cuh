@@ -84,7 +84,7 @@ struct vpbs_handle {
     // long range
     vpbs::LRSizes lr{};
     vpbs::DevBuf grid_r, grid_c, grid_c2, uhat, decx, decy, decz, nodes_lr;
-    vpbs::DevBuf spread_bin, spread_counts, spread_start, binned;  // brick-gather spreading
+    vpbs::DevBuf spread_bin, spread_counts, spread_start, binned, spread_foot;  // brick spreading
     int gatherB = 0;   // brick edge of the atomic-free spreading (0: atomic fallback)
     int nbrick[3] = {0, 0, 0};
     cufftHandle plan_r2c = 0, plan_c2r = 0, plan_c2r_6 = 0;
@@ -124,7 +124,8 @@ int ensure_pinned(vpbs_handle* h, void** buf, size_t* cap, size_t bytes);
 inline unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
 
 // geometry.cu
-int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offsets, const double* d_nodes);
+int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offsets, const double* d_nodes,
+                            int64_t nmax);  // nmax: largest node count of a filament
 
 // shortrange.cu
 int build_cell_lists(vpbs_handle* h);
