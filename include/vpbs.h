@@ -197,6 +197,13 @@ int vpbs_point_data_noalloc(const vpbs_params* params, int64_t nfil, const int64
                             void* stream, double* nodes, int32_t* node_idx_prev, double* deriv1, double* deriv2,
                             double* delta_minus, double* delta_plus, double* points, double* charges);
 
+/* Host evaluation of the pair kernel's Ewald weight tables (same coefficients and Horner/FMA
+ * order as on the device): erfc(x) and erfc(x) + 2/sqrt(pi) x exp(-x^2) for x in [0, xmax]
+ * (xmax = alpha * rcut).  The device replaces the reference's erfc/exp calls
+ * (splitting/gaussian.jl:273-279) by these degree-9 Taylor tables; this entry exists to test
+ * them.  No counterpart in the reference. */
+int vpbs_ewald_table_eval(double xmax, const double* x, int64_t n, double* erfc_out, double* g_out);
+
 /* Measured CUDA-core FMA throughput of `device` in TFLOP/s (fp64 = 1: double, 0: float); the
  * denominator of the pair kernel's roofline.  Measurement support; no counterpart in the
  * reference. */

@@ -106,3 +106,24 @@ def test_gaussian_splitting_derivations(vp):
     g3 = vp.GaussianSplitting(Ls=L, rtol=g.rtol, alpha=9.0)
     assert abs(g3.rcut - g.rcut) < 1e-12
     assert vp.maximum_wavenumber((128,) * 3, (L,) * 3) == pytest.approx(63.0)
+
+
+def test_ewald_weight_tables_accuracy(vp):
+    """The pair kernel's Taylor tables of erfc(x) and erfc(x) + 2/sqrt(pi) x exp(-x^2)
+    (replacing the reference's erfc/exp calls, splitting/gaussian.jl:273-279) against scipy."""
+    import numpy as np
+    from scipy.special import erfc
+    from vortexpasta_b200 import _lib
+    lib = _lib.load()
+    for xmax in (3.5, 4.0, 6.5):
+        x = np.concatenate([np.linspace(0, xmax, 20001), np.random.default_rng(1).uniform(0, xmax, 20000)])
+        a = np.empty_like(x)
+        g = np.empty_like(x)
+        assert lib.vpbs_ewald_table_eval(xmax, _lib.dptr(x), len(x), _lib.dptr(a), _lib.dptr(g)) == 0
+        ea = erfc(x)
+        eg = ea + 2 / np.sqrt(np.pi) * x * np.exp(-x * x)
+        # absolute error (the weights multiply 1/r^3 and 1/r; they are <= 1 and smooth)
+        assert np.max(np.abs(a - ea)) < 1e-15  # a few ulp of 1
+        assert np.max(np.abs(g - eg)) < 1e-15
+        small = x <= 4.0  # relative accuracy where erfc is not yet negligible (erfc(4) ~ 1.5e-8)
+        assert np.max(np.abs(a - ea)[small] / ea[small]) < 1e-13

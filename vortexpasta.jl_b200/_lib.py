@@ -61,6 +61,7 @@ SIGNATURES = {
     "vpbs_stage_times": (ct.c_int, [ct.c_void_p, c_double_p, ct.c_int32]),
     "vpbs_stage_name": (ct.c_char_p, [ct.c_int32]),
     "vpbs_fma_throughput": (ct.c_int, [ct.c_int32, ct.c_int32, c_double_p]),
+    "vpbs_ewald_table_eval": (ct.c_int, [ct.c_double, c_double_p, ct.c_int64, c_double_p, c_double_p]),
     "vpbs_point_data_noalloc": (ct.c_int, [ct.POINTER(VpbsParams), ct.c_int64, c_int64_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p]),

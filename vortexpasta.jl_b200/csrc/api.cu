@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "vpbs_internal.cuh"
 
@@ -192,6 +193,20 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
         if (!rc) rc = check_cuda(h, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
     h->stream = h->own_stream;
     if (!rc && !open) rc = longrange_init(h);
+    if (!rc && !open) {
+        // Ewald weight tables over x = alpha r in [0, alpha rcut]
+        int ntab = 0;
+        const double xmax = P.alpha * P.rcut;
+        ewald_table_host(xmax, &ntab, nullptr);
+        std::vector<double> tab((size_t)2 * ntab * kEwaldNC);
+        ewald_table_host(xmax, &ntab, tab.data());
+        rc = ensure(h, h->ewald_tab, sizeof(double) * tab.size(), "Ewald tables");
+        if (!rc)
+            rc = check_cuda(h, cudaMemcpy(h->ewald_tab.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice),
+                            "copy Ewald tables");
+        h->K.ewald_tab = (const double*)h->ewald_tab.p;
+        h->K.ewald_ntab = ntab;
+    }
     if (rc) {
         g_create_error = h->err;
         vpbs_destroy(h);
@@ -212,7 +227,7 @@ int vpbs_destroy(vpbs_handle* h) {
                       &h->src_seg, &h->dst_cell, &h->dst_start, &h->dst_fill, &h->dst_order, &h->counters,
                       &h->grid_r, &h->grid_c, &h->grid_c2, &h->uhat, &h->decx, &h->decy, &h->decz, &h->nodes_lr,
                       &h->vel, &h->psi, &h->spread_bin, &h->spread_counts, &h->spread_start, &h->binned,
-                      &h->spread_foot};
+                      &h->spread_foot, &h->ewald_tab};
     for (DevBuf* b : bufs) free_buf(*b);
     if (h->pin_in) cudaFreeHost(h->pin_in);
     if (h->pin_out) cudaFreeHost(h->pin_out);
@@ -477,6 +492,30 @@ int vpbs_get_pointdata(vpbs_handle* h, int32_t which, void* out, int64_t n_elems
 }
 
 int64_t vpbs_launch_count(const vpbs_handle* h) { return h ? h->launches : 0; }
+
+int vpbs_ewald_table_eval(double xmax, const double* x, int64_t n, double* erfc_out, double* g_out) {
+    if (!x || !erfc_out || !g_out || n < 0 || !(xmax > 0)) return set_error(nullptr, VPBS_ERR_ARG, "bad arguments");
+    int K = 0;
+    ewald_table_host(xmax, &K, nullptr);
+    std::vector<double> tab((size_t)2 * K * kEwaldNC);
+    ewald_table_host(xmax, &K, tab.data());
+    for (int64_t i = 0; i < n; ++i) {
+        if (!(x[i] >= 0.0 && x[i] <= xmax)) return set_error(nullptr, VPBS_ERR_ARG, "x outside [0, xmax]");
+        int k = (int)(x[i] * kEwaldInvH);
+        k = k < K ? k : K - 1;
+        const double t = x[i] - (k + 0.5) * kEwaldH;
+        const double* ce = tab.data() + (size_t)k * kEwaldNC;
+        const double* cg = tab.data() + (size_t)(K + k) * kEwaldNC;
+        double a = ce[kEwaldNC - 1], g = cg[kEwaldNC - 1];
+        for (int m = kEwaldNC - 2; m >= 0; --m) {
+            a = std::fma(a, t, ce[m]);
+            g = std::fma(g, t, cg[m]);
+        }
+        erfc_out[i] = a;
+        g_out[i] = g;
+    }
+    return 0;
+}
 
 int vpbs_stage_timing(vpbs_handle* h, int32_t enable) {
     if (!h) return VPBS_ERR_ARG;

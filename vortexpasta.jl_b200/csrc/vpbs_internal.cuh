@@ -26,7 +26,33 @@ struct KParams {
     double lia_fraction;  // <= 0: nothing
     int avoid_explicit_erf;
     int open_domain;      // NoSplitting
+    // piecewise Taylor tables of erfc(x) and erfc(x) + 2/sqrt(pi) x exp(-x^2), x = alpha r
+    const double* ewald_tab;
+    int ewald_ntab;       // number of intervals (0: no splitting, weights are 1)
 };
+
+// Ewald weight tables: intervals of width 1/16 in x = alpha r, degree-9 Taylor polynomials
+// about the interval centres (coefficients from the closed-form derivatives of erfc).
+constexpr int kEwaldNC = 10;
+constexpr double kEwaldInvH = 16.0;
+constexpr double kEwaldH = 1.0 / 16.0;
+void ewald_table_host(double xmax, int* ntab, double* tab);  // tab: 2 * ntab * kEwaldNC doubles
+int ewald_table_size(double xmax);
+
+__device__ __forceinline__ void ewald_weights(const KParams& K, double x, double& a, double& g) {
+    int k = (int)(x * kEwaldInvH);
+    k = k < K.ewald_ntab ? k : K.ewald_ntab - 1;
+    const double t = x - (k + 0.5) * kEwaldH;
+    const double* ce = K.ewald_tab + k * kEwaldNC;
+    const double* cg = K.ewald_tab + (K.ewald_ntab + k) * kEwaldNC;
+    a = __ldg(ce + kEwaldNC - 1);
+    g = __ldg(cg + kEwaldNC - 1);
+#pragma unroll
+    for (int n = kEwaldNC - 2; n >= 0; --n) {
+        a = fma(a, t, __ldg(ce + n));
+        g = fma(g, t, __ldg(cg + n));
+    }
+}
 
 // Cell-list geometry.
 struct CellGrid {
@@ -80,6 +106,7 @@ struct vpbs_handle {
     vpbs::CellGrid cg{};
     vpbs::DevBuf src_cell, src_start, src_fill, src_sorted, src_seg, dst_cell, dst_start, dst_fill, dst_order;
     vpbs::DevBuf counters;  // [0] in-range pairs, [1] candidates (unsigned long long)
+    vpbs::DevBuf ewald_tab;  // Taylor tables of the Ewald weights (KParams::ewald_tab)
 
     // long range
     vpbs::LRSizes lr{};
