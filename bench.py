@@ -193,6 +193,24 @@ def read_traffic(kernel_stage):
     return None
 
 
+def rank_workload(vp, workload: str, rank: int):
+    """Each rank evaluates its own independent system (weak scaling): same generator and
+    parameters, seed 42 + rank."""
+    if workload == "ring64":
+        return vp.configs.ring64()
+    return vp.configs.WORKLOADS[workload](seed=42 + rank)
+
+
+def max_over_ranks(values, device, world):
+    """Element-wise max over ranks of per-rank timings (the job's time is its slowest rank)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -206,8 +224,7 @@ def run_ours(args):
     dev = torch.device("cuda", local_rank)
     vp = load_package()
     from vortexpasta_b200 import _lib
-    fs, p = vp.configs.WORKLOADS[args.workload](seed=42 + rank) if args.workload != "ring64" else \
-        vp.configs.ring64()
+    fs, p = rank_workload(vp, args.workload, rank)
     p = p.with_(device=local_rank)
     Np = sum(len(f) for f in fs)
     Nq = Np * len(p.quadrature)
@@ -271,10 +288,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = sum(s.elapsed_time(e) for s, e in zip(e_starts, e_ends))
 
-    tot = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-    total_ms, e2e_ms = tot.tolist()
+    total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], dev, world)
     ms_per_step = total_ms / args.steps
     value = world * Np * args.steps / (total_ms * 1e-3)
     e2e_value = world * Np * args.steps / (e2e_ms * 1e-3)
