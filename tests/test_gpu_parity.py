@@ -158,6 +158,31 @@ def test_repeatable(vp, built_lib):
     assert rel(a, b) < 1e-14
 
 
+MIXED_TOL = 1e-5  # relative L2 of the mixed (FP32 bulk) form vs the FP64 oracle
+
+
+@pytest.mark.parametrize("workload", ["ring64", "tangle20k"])
+def test_mixed_precision_form(vp, oracle, built_lib, workload):
+    """Precision form: FP32 pair sum, spreading, FFT and interpolation; FP64 positions,
+    separations, local/self terms and final accumulation.  Target: <= 1e-5 relative L2."""
+    fs, p = vp.configs.WORKLOADS[workload](precision="mixed")
+    v, psi, _ = gpu_fields(vp, p, fs)
+    vo, po, _ = oracle.compute_on_nodes(p, fs, streamfunction=True)
+    ev, ep = rel(v, vo), rel(psi, po)
+    print(f"{workload} mixed: velocity rel L2 {ev:.2e} (max {np.abs(v - vo).max() / np.abs(vo).max():.2e}), "
+          f"streamfunction rel L2 {ep:.2e}")
+    assert ev < MIXED_TOL and ep < MIXED_TOL
+
+
+@pytest.mark.parametrize("LIA", [True, False, "only"])
+def test_mixed_precision_flags(vp, oracle, built_lib, LIA):
+    fs, p = vp.configs.tangle20k(precision="mixed")
+    fs = fs[:25]
+    v, psi, _ = gpu_fields(vp, p, fs, LIA=LIA)
+    vo, po, _ = oracle.compute_on_nodes(p, fs, streamfunction=True, LIA=LIA)
+    assert rel(v, vo) < MIXED_TOL and rel(psi, po) < MIXED_TOL
+
+
 def test_errors_surface(vp, built_lib):
     fs, p = vp.configs.ring64()
     cache = vp.init_cache(p)

@@ -116,8 +116,10 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
         return set_error(nullptr, VPBS_ERR_PARAMS, "nquad_near must be in 0:16");
     if (P.lia_segment_fraction > 1.0)
         return set_error(nullptr, VPBS_ERR_PARAMS, "lia_segment_fraction must be in (0, 1]");
-    if (P.precision != VPBS_PRECISION_FP64)
-        return set_error(nullptr, VPBS_ERR_PARAMS, "only the FP64 form (VPBS_PRECISION_FP64) is available in this build");
+    if (P.precision != VPBS_PRECISION_FP64 && P.precision != VPBS_PRECISION_MIXED)
+        return set_error(nullptr, VPBS_ERR_PARAMS, "precision must be VPBS_PRECISION_FP64 or VPBS_PRECISION_MIXED");
+    if (P.precision == VPBS_PRECISION_MIXED && !(P.alpha > 0))
+        return set_error(nullptr, VPBS_ERR_PARAMS, "the mixed-precision form needs Ewald splitting (alpha > 0)");
     const bool open = !(P.alpha > 0);
     KParams K{};
     K.Gamma = P.Gamma;
@@ -133,7 +135,10 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
         K.qnw[q] = P.nquad_near > 0 ? P.quad_near_w[q] : P.quad_w[q];
     }
     K.lia_fraction = P.lia_segment_fraction > 0 ? P.lia_segment_fraction : 0.0;
-    K.avoid_explicit_erf = P.avoid_explicit_erf;
+    // The mixed form always uses the explicit-erf bookkeeping internally (mathematically the same
+    // result): pairs on the two local segments are left out of the FP32 pair sum and their
+    // long-range part is removed in FP64, so no near-singular pair is ever summed in FP32.
+    K.avoid_explicit_erf = P.precision == VPBS_PRECISION_MIXED ? 0 : P.avoid_explicit_erf;
     CellGrid cg{};
     if (open) {
         for (int d = 0; d < 3; ++d) { K.L[d] = 0.0; K.Lh[d] = 0.0; }
@@ -200,11 +205,19 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
         ewald_table_host(xmax, &ntab, nullptr);
         std::vector<double> tab((size_t)2 * ntab * kEwaldNC);
         ewald_table_host(xmax, &ntab, tab.data());
-        rc = ensure(h, h->ewald_tab, sizeof(double) * tab.size(), "Ewald tables");
+        // FP32 copy: the leading kEwaldNCf coefficients of each interval, stored after the FP64 table
+        std::vector<float> tabf((size_t)2 * ntab * kEwaldNCf);
+        for (size_t k = 0; k < (size_t)2 * ntab; ++k)
+            for (int n = 0; n < kEwaldNCf; ++n) tabf[k * kEwaldNCf + n] = (float)tab[k * kEwaldNC + n];
+        const size_t bytes_d = sizeof(double) * tab.size(), bytes_f = sizeof(float) * tabf.size();
+        rc = ensure(h, h->ewald_tab, bytes_d + bytes_f, "Ewald tables");
         if (!rc)
-            rc = check_cuda(h, cudaMemcpy(h->ewald_tab.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice),
+            rc = check_cuda(h, cudaMemcpy(h->ewald_tab.p, tab.data(), bytes_d, cudaMemcpyHostToDevice), "copy Ewald tables");
+        if (!rc)
+            rc = check_cuda(h, cudaMemcpy((char*)h->ewald_tab.p + bytes_d, tabf.data(), bytes_f, cudaMemcpyHostToDevice),
                             "copy Ewald tables");
         h->K.ewald_tab = (const double*)h->ewald_tab.p;
+        h->K.ewald_tab_f = (const float*)((const char*)h->ewald_tab.p + bytes_d);
         h->K.ewald_ntab = ntab;
     }
     if (rc) {

@@ -11,6 +11,7 @@
 //     deconvolution, written straight into the complex-to-real FFT input;
 //  3. batched complex-to-real FFT and ES-kernel interpolation at the nodes (type 2).
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "vpbs_internal.cuh"
@@ -83,12 +84,21 @@ __device__ __forceinline__ int wrapi(int i, int n) {
 
 constexpr int kSpreadBatch = 32;
 
-// Type-1 spreading: each block takes kSpreadBatch points; kernel values are tabulated in shared
-// memory, then every thread adds the charges along x-lines of the (2m)^3 footprint with
-// double-precision atomics.
-__global__ void __launch_bounds__(256) spread_kernel_f64(
+// Complex value of the grid precision T from double parts.
+template <typename C>
+__device__ __forceinline__ C mkc(double x, double y);
+template <>
+__device__ __forceinline__ double2 mkc<double2>(double x, double y) { return make_double2(x, y); }
+template <>
+__device__ __forceinline__ float2 mkc<float2>(double x, double y) { return make_float2((float)x, (float)y); }
+
+// Type-1 spreading with global atomics (fallback when the grid cannot be tiled into bricks):
+// each block takes kSpreadBatch points; kernel values are tabulated in shared memory, then
+// every thread adds the charges along x-lines of the (2m)^3 footprint.
+template <typename T>
+__global__ void __launch_bounds__(256) spread_kernel_atomic(
     LRSizes S, int64_t Nq, const double* __restrict__ src, double sx0, double sx1, double sx2,
-    double* __restrict__ grid) {
+    T* __restrict__ grid) {
     __shared__ double phi[kSpreadBatch][3][2 * kMaxHalfSupport];
     __shared__ int i0s[kSpreadBatch][3];
     __shared__ double qs[kSpreadBatch][3];
@@ -120,19 +130,21 @@ __global__ void __launch_bounds__(256) spread_kernel_f64(
         for (int sx = 0; sx < w; ++sx) {
             const int ix = wrapi(i0s[p][0] + sx, S.n[0]);
             const double f = phi[p][0][sx];
-            atomicAdd(grid + row + ix, q0 * f);
-            atomicAdd(grid + ng + row + ix, q1 * f);
-            atomicAdd(grid + 2 * ng + row + ix, q2 * f);
+            atomicAdd(grid + row + ix, (T)(q0 * f));
+            atomicAdd(grid + ng + row + ix, (T)(q1 * f));
+            atomicAdd(grid + 2 * ng + row + ix, (T)(q2 * f));
         }
     }
 }
 
-// Fused Fourier-space kernel over the r2c grid [n2][n1][n0/2+1].
-__global__ void __launch_bounds__(256) fourier_kernel_f64(
+// Fused Fourier-space kernel over the r2c grid [n2][n1][n0/2+1] (C: double2 or float2; the
+// arithmetic is FP64 in both forms, only the grids are stored in the grid precision).
+template <typename C>
+__global__ void __launch_bounds__(256) fourier_kernel(
     LRSizes S, double pref, double k0x, double k0y, double k0z, int truncate, double kmax2, int fields,
     const double* __restrict__ dec0, const double* __restrict__ dec1, const double* __restrict__ dec2,
     const double* __restrict__ decE0, const double* __restrict__ decE1, const double* __restrict__ decE2,
-    double2* __restrict__ gc, double2* __restrict__ gc2, double2* __restrict__ uhat, int store_uhat) {
+    C* __restrict__ gc, C* __restrict__ gc2, double2* __restrict__ uhat, int store_uhat) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= S.ncgrid) return;
     const int ix = (int)(idx % S.nxc);
@@ -158,8 +170,8 @@ __global__ void __launch_bounds__(256) fourier_kernel_f64(
             const double f = pref * (dec0[ix] * dec1[ry] * dec2[rz]);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const double2 F = gc[c * cstride + idx];
-                w[c] = make_double2(F.x * f, F.y * f);
+                const C F = gc[c * cstride + idx];
+                w[c] = make_double2((double)F.x * f, (double)F.y * f);
             }
         }
         if (store_uhat) {
@@ -175,24 +187,24 @@ __global__ void __launch_bounds__(256) fourier_kernel_f64(
                 const double2 iw0 = make_double2(-w[0].y, w[0].x), iw1 = make_double2(-w[1].y, w[1].x),
                               iw2 = make_double2(-w[2].y, w[2].x);
                 const double fk = k2inv * g;
-                gc[idx] = make_double2((kyy * iw2.x - kzz * iw1.x) * fk, (kyy * iw2.y - kzz * iw1.y) * fk);
-                gc[cstride + idx] = make_double2((kzz * iw0.x - kx * iw2.x) * fk, (kzz * iw0.y - kx * iw2.y) * fk);
-                gc[2 * cstride + idx] = make_double2((kx * iw1.x - kyy * iw0.x) * fk, (kx * iw1.y - kyy * iw0.y) * fk);
+                gc[idx] = mkc<C>((kyy * iw2.x - kzz * iw1.x) * fk, (kyy * iw2.y - kzz * iw1.y) * fk);
+                gc[cstride + idx] = mkc<C>((kzz * iw0.x - kx * iw2.x) * fk, (kzz * iw0.y - kx * iw2.y) * fk);
+                gc[2 * cstride + idx] = mkc<C>((kx * iw1.x - kyy * iw0.x) * fk, (kx * iw1.y - kyy * iw0.y) * fk);
             }
             if (fields & VPBS_STREAMFUNCTION) {
                 const double fk = k2inv * g;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) gc2[c * cstride + idx] = make_double2(w[c].x * fk, w[c].y * fk);
+                for (int c = 0; c < 3; ++c) gc2[c * cstride + idx] = mkc<C>(w[c].x * fk, w[c].y * fk);
             }
         }
     }
     if (!live) {
         if (fields & VPBS_VELOCITY)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) gc[c * cstride + idx] = make_double2(0.0, 0.0);
+            for (int c = 0; c < 3; ++c) gc[c * cstride + idx] = mkc<C>(0.0, 0.0);
         if (fields & VPBS_STREAMFUNCTION)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) gc2[c * cstride + idx] = make_double2(0.0, 0.0);
+            for (int c = 0; c < 3; ++c) gc2[c * cstride + idx] = mkc<C>(0.0, 0.0);
     }
 }
 
@@ -224,25 +236,27 @@ __global__ void spread_bin_count_kernel(LRSizes S, int B, int nb0, int nb1, int 
 
 // Scatter the points into bin order, with everything the brick kernel needs per point: the
 // wrapped footprint start per dimension, the 3 x w kernel values and the 3 charges.
-// binned layout per slot: [3 charges][3 w kernel values] (doubles), foot: [3] int32.
+// binned layout per slot: [3 charges][3 w kernel values] (grid precision T), foot: [3] int32.
+// Positions and kernel values are computed in FP64 and stored in T.
+template <typename T>
 __global__ void spread_bin_scatter_kernel(LRSizes S, int64_t Nq, const double* __restrict__ src, double sx0,
                                           double sx1, double sx2, const int32_t* __restrict__ bin,
                                           const int32_t* __restrict__ rank, const int32_t* __restrict__ start,
-                                          double* __restrict__ binned, int32_t* __restrict__ foot) {
+                                          T* __restrict__ binned, int32_t* __restrict__ foot) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= Nq) return;
     const int64_t pos = (int64_t)start[bin[j]] + rank[j];
     const int w = 2 * S.m;
     const int stride = 3 + 3 * w;
-    double* out = binned + pos * stride;
+    T* out = binned + pos * stride;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) out[c] = src[(3 + c) * Nq + j];
+    for (int c = 0; c < 3; ++c) out[c] = (T)src[(3 + c) * Nq + j];
     const double scale[3] = {sx0, sx1, sx2};
     for (int d = 0; d < 3; ++d) {
         const double xh = (src[d * Nq + j] * scale[d]) / (2.0 * kPi / S.n[d]);
         const int i0 = (int)floor(xh) - S.m + 1;
         foot[3 * pos + d] = wrapi(i0, S.n[d]);
-        for (int s = 0; s < w; ++s) out[3 + d * w + s] = es_kernel(xh - (i0 + s), S.m, S.beta, S.edge);
+        for (int s = 0; s < w; ++s) out[3 + d * w + s] = (T)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge);
     }
 }
 
@@ -252,12 +266,13 @@ __global__ void spread_bin_scatter_kernel(LRSizes S, int64_t Nq, const double* _
 // over the footprint's (y, z) lines), then writes the brick to the grid with plain stores.
 constexpr int kBrickThreads = 256;
 
-template <int B>
-__global__ void __launch_bounds__(kBrickThreads) spread_brick_kernel_f64(
-    LRSizes S, int nb0, int nb1, int nb2, const int32_t* __restrict__ bin_start, const double* __restrict__ binned,
-    const int32_t* __restrict__ foot, double* __restrict__ grid) {
-    extern __shared__ double tile[];  // [3][B][PZ] with rows of RX doubles
-    __shared__ double phw[kBrickThreads / 32][3 + 6 * kMaxHalfSupport];
+template <int B, typename T>
+__global__ void __launch_bounds__(kBrickThreads) spread_brick_kernel(
+    LRSizes S, int nb0, int nb1, int nb2, const int32_t* __restrict__ bin_start, const T* __restrict__ binned,
+    const int32_t* __restrict__ foot, T* __restrict__ grid) {
+    extern __shared__ __align__(16) unsigned char tile_raw[];
+    T* tile = reinterpret_cast<T*>(tile_raw);  // [3][B][PZ] with rows of RX values
+    __shared__ T phw[kBrickThreads / 32][3 + 6 * kMaxHalfSupport];
     constexpr int RX = B + 1;        // x-row stride (bank spread along y)
     constexpr int PZ = B * RX + 8;   // z-plane stride (16-word bank shift between planes)
     constexpr int TC = B * PZ;       // doubles per component
@@ -268,9 +283,9 @@ __global__ void __launch_bounds__(kBrickThreads) spread_brick_kernel_f64(
     const int bz = blockIdx.x / (nb0 * nb1);
     const int bs[3] = {bx * B, by * B, bz * B};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < 3 * TC; i += kBrickThreads) tile[i] = 0.0;
+    for (int i = threadIdx.x; i < 3 * TC; i += kBrickThreads) tile[i] = (T)0;
     __syncthreads();
-    double* ph = phw[warp];  // [q0 q1 q2 | phi_x[w] | phi_y[w] | phi_z[w]]
+    T* ph = phw[warp];  // [q0 q1 q2 | phi_x[w] | phi_y[w] | phi_z[w]]
     for (int nbr = 0; nbr < 8; ++nbr) {
         const int cx = (bx - (nbr & 1) + nb0) % nb0;
         const int cy = (by - ((nbr >> 1) & 1) + nb1) % nb1;
@@ -292,17 +307,17 @@ __global__ void __launch_bounds__(kBrickThreads) spread_brick_kernel_f64(
             if (empty) continue;  // warp-uniform
             for (int it = lane; it < stride; it += 32) ph[it] = binned[j * stride + it];
             __syncwarp();
-            const double q0 = ph[0], q1 = ph[1], q2 = ph[2];
-            const double* phx = ph + 3;
-            const double* phy = phx + w;
-            const double* phz = phy + w;
+            const T q0 = ph[0], q1 = ph[1], q2 = ph[2];
+            const T* phx = ph + 3;
+            const T* phy = phx + w;
+            const T* phz = phy + w;
             const int ny = hi[1] - lo[1], nz = hi[2] - lo[2];
             for (int l = lane; l < ny * nz; l += 32) {
                 const int sy = lo[1] + l % ny, sz = lo[2] + l / ny;
-                const double f = phy[sy] * phz[sz];
-                double* row = tile + (o[2] + sz) * PZ + (o[1] + sy) * RX + o[0];
+                const T f = phy[sy] * phz[sz];
+                T* row = tile + (o[2] + sz) * PZ + (o[1] + sy) * RX + o[0];
                 for (int sx = lo[0]; sx < hi[0]; ++sx) {
-                    const double g = f * phx[sx];
+                    const T g = f * phx[sx];
                     atomicAdd(row + sx, q0 * g);
                     atomicAdd(row + TC + sx, q1 * g);
                     atomicAdd(row + 2 * TC + sx, q2 * g);
@@ -323,10 +338,10 @@ __global__ void __launch_bounds__(kBrickThreads) spread_brick_kernel_f64(
 
 // Type-2 interpolation, one warp per node (cell order when available): lanes take (sy, sz)
 // pairs of the footprint, loop over x, and the warp reduces the three components.
-template <int W>  // kernel width 2m (compile-time, so the per-lane tables stay in registers)
-__global__ void __launch_bounds__(256) interp_warp_kernel_f64(
+template <int W, typename T>  // kernel width 2m (compile-time: per-lane tables stay in registers)
+__global__ void __launch_bounds__(256) interp_warp_kernel(
     LRSizes S, int64_t Np, const int32_t* __restrict__ order, const double* __restrict__ nodes, double sx0,
-    double sx1, double sx2, const double* __restrict__ grid, double* __restrict__ out) {
+    double sx1, double sx2, const T* __restrict__ grid, double* __restrict__ out) {
     const int lane = threadIdx.x & 31;
     const int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (t >= Np) return;
@@ -340,11 +355,11 @@ __global__ void __launch_bounds__(256) interp_warp_kernel_f64(
         xh[d] = (nodes[d * Np + i] * scale[d]) / (2.0 * kPi / S.n[d]);
         i0[d] = (int)floor(xh[d]) - S.m + 1;
     }
-    double phx[w];
+    T phx[w];
     int ixs[w];
 #pragma unroll
     for (int s = 0; s < w; ++s) {
-        phx[s] = es_kernel(xh[0] - (i0[0] + s), S.m, S.beta, S.edge);
+        phx[s] = (T)es_kernel(xh[0] - (i0[0] + s), S.m, S.beta, S.edge);
         ixs[s] = wrapi(i0[0] + s, S.n[0]);
     }
     double a0 = 0, a1 = 0, a2 = 0;
@@ -354,7 +369,7 @@ __global__ void __launch_bounds__(256) interp_warp_kernel_f64(
         const double f = es_kernel(xh[1] - (i0[1] + sy), S.m, S.beta, S.edge) *
                          es_kernel(xh[2] - (i0[2] + sz), S.m, S.beta, S.edge);
         const int64_t rowi = ((int64_t)wrapi(i0[2] + sz, S.n[2]) * S.n[1] + wrapi(i0[1] + sy, S.n[1])) * S.n[0];
-        double b0 = 0, b1 = 0, b2 = 0;
+        T b0 = 0, b1 = 0, b2 = 0;
 #pragma unroll
         for (int sx = 0; sx < w; ++sx) {
             const int64_t g = rowi + ixs[sx];
@@ -362,9 +377,9 @@ __global__ void __launch_bounds__(256) interp_warp_kernel_f64(
             b1 += phx[sx] * grid[ng + g];
             b2 += phx[sx] * grid[2 * ng + g];
         }
-        a0 += f * b0;
-        a1 += f * b1;
-        a2 += f * b2;
+        a0 += f * (double)b0;
+        a1 += f * (double)b1;
+        a2 += f * (double)b2;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -413,9 +428,11 @@ int longrange_init(vpbs_handle* h) {
         }
     }
     int rc;
-    if ((rc = ensure(h, h->grid_r, sizeof(double) * 3 * S.ngrid, "real grid"))) return rc;
-    if ((rc = ensure(h, h->grid_c, sizeof(double2) * 3 * S.ncgrid, "complex grid"))) return rc;
-    if ((rc = ensure(h, h->grid_c2, sizeof(double2) * 3 * S.ncgrid, "complex grid (streamfunction)"))) return rc;
+    const bool mixed = P.precision == VPBS_PRECISION_MIXED;
+    const size_t rsz = mixed ? sizeof(float) : sizeof(double);  // grid precision
+    if ((rc = ensure(h, h->grid_r, rsz * 3 * S.ngrid, "real grid"))) return rc;
+    if ((rc = ensure(h, h->grid_c, 2 * rsz * 3 * S.ncgrid, "complex grid"))) return rc;
+    if ((rc = ensure(h, h->grid_c2, 2 * rsz * 3 * S.ncgrid, "complex grid (streamfunction)"))) return rc;
     if ((rc = ensure(h, h->uhat, sizeof(double2) * 3 * S.nmodes, "uhat"))) return rc;
     // separable deconvolution factors 1/psi_hat and 1/psi_hat * exp(-k^2 / 4 alpha^2)
     std::vector<double> tab[6];
@@ -443,10 +460,10 @@ int longrange_init(vpbs_handle* h) {
         return rc;
     int nrev[3] = {S.n[2], S.n[1], S.n[0]};
     if ((rc = check_fft(h, cufftPlanMany(&h->plan_r2c, 3, nrev, nullptr, 1, (int)S.ngrid, nullptr, 1, (int)S.ncgrid,
-                                         CUFFT_D2Z, 3), "plan D2Z")))
+                                         mixed ? CUFFT_R2C : CUFFT_D2Z, 3), "plan r2c")))
         return rc;
     if ((rc = check_fft(h, cufftPlanMany(&h->plan_c2r, 3, nrev, nullptr, 1, (int)S.ncgrid, nullptr, 1, (int)S.ngrid,
-                                         CUFFT_Z2D, 3), "plan Z2D")))
+                                         mixed ? CUFFT_C2R : CUFFT_Z2D, 3), "plan c2r")))
         return rc;
     h->have_plans = true;
     return 0;
@@ -460,14 +477,28 @@ void longrange_free(vpbs_handle* h) {
     }
 }
 
-int longrange_compute(vpbs_handle* h, int fields) {
+namespace {
+inline cufftResult exec_r2c(cufftHandle p, double* in, double2* out) {
+    return cufftExecD2Z(p, in, (cufftDoubleComplex*)out);
+}
+inline cufftResult exec_r2c(cufftHandle p, float* in, float2* out) { return cufftExecR2C(p, in, (cufftComplex*)out); }
+inline cufftResult exec_c2r(cufftHandle p, double2* in, double* out) {
+    return cufftExecZ2D(p, (cufftDoubleComplex*)in, out);
+}
+inline cufftResult exec_c2r(cufftHandle p, float2* in, float* out) { return cufftExecC2R(p, (cufftComplex*)in, out); }
+}  // namespace
+
+// T: grid precision (double for the plain form, float for the mixed form).
+template <typename T>
+int longrange_compute_t(vpbs_handle* h, int fields) {
+    using C = typename std::conditional<std::is_same<T, double>::value, double2, float2>::type;
     const LRSizes& S = h->lr;
     const vpbs_params& P = h->P;
     int rc;
     const double sx[3] = {2.0 * kPi / P.L[0], 2.0 * kPi / P.L[1], 2.0 * kPi / P.L[2]};
-    double* grid = (double*)h->grid_r.p;
-    double2* gc = (double2*)h->grid_c.p;
-    double2* gc2 = (double2*)h->grid_c2.p;
+    T* grid = (T*)h->grid_r.p;
+    C* gc = (C*)h->grid_c.p;
+    C* gc2 = (C*)h->grid_c2.p;
     // sources: cell-sorted copy (SoA x,y,z,qx,qy,qz), built by build_cell_lists
     const double* src = (const double*)h->src_sorted.p;
     if (h->gatherB) {
@@ -477,8 +508,8 @@ int longrange_compute(vpbs_handle* h, int fields) {
         if ((rc = ensure(h, h->spread_bin, sizeof(int32_t) * 2 * Nq, "spread bins"))) return rc;
         if ((rc = ensure(h, h->spread_counts, sizeof(int32_t) * nbins, "spread bin counts"))) return rc;
         if ((rc = ensure(h, h->spread_start, sizeof(int32_t) * (nbins + 1), "spread bin starts"))) return rc;
-        const int stride = 3 + 6 * S.m;  // doubles per binned point
-        if ((rc = ensure(h, h->binned, sizeof(double) * stride * Nq, "binned points"))) return rc;
+        const int stride = 3 + 6 * S.m;  // values per binned point
+        if ((rc = ensure(h, h->binned, sizeof(T) * stride * Nq, "binned points"))) return rc;
         if ((rc = ensure(h, h->spread_foot, sizeof(int32_t) * 3 * Nq, "footprints"))) return rc;
         int32_t* bin = (int32_t*)h->spread_bin.p;
         int32_t* rank = bin + Nq;
@@ -490,36 +521,37 @@ int longrange_compute(vpbs_handle* h, int fields) {
                                                                            sx[2], bin, rank, counts);
         h->launches++;
         if ((rc = exclusive_scan(h, counts, start, nbins))) return rc;
-        spread_bin_scatter_kernel<<<grid_for(Nq, 128), 128, 0, h->stream>>>(S, Nq, src, sx[0], sx[1], sx[2], bin, rank,
-                                                                             start, (double*)h->binned.p, foot);
+        spread_bin_scatter_kernel<T><<<grid_for(Nq, 128), 128, 0, h->stream>>>(S, Nq, src, sx[0], sx[1], sx[2], bin,
+                                                                                rank, start, (T*)h->binned.p, foot);
         h->launches++;
         const unsigned nblk = (unsigned)nbins;
-        const double* bsrc = (const double*)h->binned.p;
-        const size_t smem = sizeof(double) * 3 * B * (B * (B + 1) + 8);
+        const T* bsrc = (const T*)h->binned.p;
+        const size_t smem = sizeof(T) * 3 * B * (B * (B + 1) + 8);
         auto launch = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             kern<<<nblk, kBrickThreads, smem, h->stream>>>(S, nb0, nb1, nb2, start, bsrc, foot, grid);
         };
         switch (B) {
-            case 16: launch(spread_brick_kernel_f64<16>); break;
-            case 12: launch(spread_brick_kernel_f64<12>); break;
-            case 10: launch(spread_brick_kernel_f64<10>); break;
-            default: launch(spread_brick_kernel_f64<8>); break;
+            case 16: launch(spread_brick_kernel<16, T>); break;
+            case 12: launch(spread_brick_kernel<12, T>); break;
+            case 10: launch(spread_brick_kernel<10, T>); break;
+            default: launch(spread_brick_kernel<8, T>); break;
         }
         h->launches++;
         if ((rc = check_cuda(h, cudaGetLastError(), "spread gather kernels"))) return rc;
     } else {
         StageScope st(h, ST_SPREAD);
-        if ((rc = check_cuda(h, cudaMemsetAsync(grid, 0, sizeof(double) * 3 * S.ngrid, h->stream), "memset grid")))
+        if ((rc = check_cuda(h, cudaMemsetAsync(grid, 0, sizeof(T) * 3 * S.ngrid, h->stream), "memset grid")))
             return rc;
-        spread_kernel_f64<<<grid_for(h->Nq, kSpreadBatch), 256, 0, h->stream>>>(S, h->Nq, src, sx[0], sx[1], sx[2], grid);
+        spread_kernel_atomic<T><<<grid_for(h->Nq, kSpreadBatch), 256, 0, h->stream>>>(S, h->Nq, src, sx[0], sx[1], sx[2],
+                                                                                      grid);
         h->launches++;
         if ((rc = check_cuda(h, cudaGetLastError(), "spread kernel"))) return rc;
     }
     {
         StageScope st(h, ST_FFT_FORWARD);
         if ((rc = check_fft(h, cufftSetStream(h->plan_r2c, h->stream), "set stream"))) return rc;
-        if ((rc = check_fft(h, cufftExecD2Z(h->plan_r2c, grid, (cufftDoubleComplex*)gc), "exec D2Z"))) return rc;
+        if ((rc = check_fft(h, exec_r2c(h->plan_r2c, grid, gc), "exec r2c"))) return rc;
     }
     double kmax = INFINITY;
     for (int d = 0; d < 3; ++d) kmax = fmin(kmax, 2.0 * kPi * ((P.Ns[d] - 1) / 2) / P.L[d]);
@@ -533,7 +565,7 @@ int longrange_compute(vpbs_handle* h, int fields) {
     const double* decE2 = decE1 + S.Ns[1];
     {
         StageScope st(h, ST_FOURIER);
-        fourier_kernel_f64<<<grid_for(S.ncgrid, 256), 256, 0, h->stream>>>(
+        fourier_kernel<C><<<grid_for(S.ncgrid, 256), 256, 0, h->stream>>>(
             S, pref, sx[0], sx[1], sx[2], P.truncate_spherical, kmax * kmax, fields, dec0, dec1, dec2, decE0, decE1,
             decE2, gc, gc2, (double2*)h->uhat.p, 1);
         h->launches++;
@@ -545,11 +577,11 @@ int longrange_compute(vpbs_handle* h, int fields) {
     for (int f = 0; f < 2; ++f) {
         const int field = f == 0 ? VPBS_STREAMFUNCTION : VPBS_VELOCITY;
         if (!(fields & field)) continue;
-        double2* in = field == VPBS_VELOCITY ? gc : gc2;
+        C* in = field == VPBS_VELOCITY ? gc : gc2;
         double* out = (double*)(field == VPBS_VELOCITY ? h->vel.p : h->psi.p);
         {
             StageScope st(h, ST_FFT_INVERSE);
-            if ((rc = check_fft(h, cufftExecZ2D(h->plan_c2r, (cufftDoubleComplex*)in, grid), "exec Z2D"))) return rc;
+            if ((rc = check_fft(h, exec_c2r(h->plan_c2r, in, grid), "exec c2r"))) return rc;
         }
         if (h->interp_wait) {
             if ((rc = check_cuda(h, cudaStreamWaitEvent(h->stream, h->interp_wait, 0), "wait short range"))) return rc;
@@ -560,19 +592,24 @@ int longrange_compute(vpbs_handle* h, int fields) {
                                                             sx[2], grid, out);
         };
         switch (S.m) {
-            case 1: launch_interp(interp_warp_kernel_f64<2>); break;
-            case 2: launch_interp(interp_warp_kernel_f64<4>); break;
-            case 3: launch_interp(interp_warp_kernel_f64<6>); break;
-            case 4: launch_interp(interp_warp_kernel_f64<8>); break;
-            case 5: launch_interp(interp_warp_kernel_f64<10>); break;
-            case 6: launch_interp(interp_warp_kernel_f64<12>); break;
-            case 7: launch_interp(interp_warp_kernel_f64<14>); break;
-            default: launch_interp(interp_warp_kernel_f64<16>); break;
+            case 1: launch_interp(interp_warp_kernel<2, T>); break;
+            case 2: launch_interp(interp_warp_kernel<4, T>); break;
+            case 3: launch_interp(interp_warp_kernel<6, T>); break;
+            case 4: launch_interp(interp_warp_kernel<8, T>); break;
+            case 5: launch_interp(interp_warp_kernel<10, T>); break;
+            case 6: launch_interp(interp_warp_kernel<12, T>); break;
+            case 7: launch_interp(interp_warp_kernel<14, T>); break;
+            default: launch_interp(interp_warp_kernel<16, T>); break;
         }
         h->launches++;
         if ((rc = check_cuda(h, cudaGetLastError(), "interp kernel"))) return rc;
     }
     return 0;
+}
+
+int longrange_compute(vpbs_handle* h, int fields) {
+    return h->P.precision == VPBS_PRECISION_MIXED ? longrange_compute_t<float>(h, fields)
+                                                  : longrange_compute_t<double>(h, fields);
 }
 
 }  // namespace vpbs

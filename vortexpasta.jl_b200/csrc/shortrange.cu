@@ -95,11 +95,41 @@ __global__ void scatter_nodes_kernel(int64_t Np, const int32_t* __restrict__ cel
     order[(int64_t)start[cell[i]] + rank[i]] = (int32_t)i;
 }
 
+// Per-lane accumulators in the evaluation precision R; in FP32 they are Kahan-compensated
+// (c holds the running compensation), in FP64 plain sums.
+template <typename R>
 struct PairAcc {
-    double v[3];
-    double p[3];
+    R v[3], p[3];
+    R cv[3], cp[3];
     unsigned long long inr, cand;
 };
+
+template <typename R>
+__device__ __forceinline__ void acc_add(R& s, R& c, R x) {
+    if constexpr (std::is_same<R, float>::value) {
+        const R y = x - c;
+        const R t = s + y;
+        c = (t - s) - y;
+        s = t;
+    } else {
+        s += x;
+    }
+}
+
+__device__ __forceinline__ void ewald_weights_f(const KParams& K, float x, float& a, float& g) {
+    int k = (int)(x * (float)kEwaldInvH);
+    k = k < K.ewald_ntab ? k : K.ewald_ntab - 1;
+    const float t = x - (k + 0.5f) * (float)kEwaldH;
+    const float* ce = K.ewald_tab_f + k * kEwaldNCf;
+    const float* cg = K.ewald_tab_f + (K.ewald_ntab + k) * kEwaldNCf;
+    a = __ldg(ce + kEwaldNCf - 1);
+    g = __ldg(cg + kEwaldNCf - 1);
+#pragma unroll
+    for (int n = kEwaldNCf - 2; n >= 0; --n) {
+        a = fmaf(a, t, __ldg(ce + n));
+        g = fmaf(g, t, __ldg(cg + n));
+    }
+}
 
 // Per-warp queue of in-range pairs: the separations and source indices of candidates that
 // passed the r^2 <= r_cut^2 test are compacted here (ballot + prefix popcount), so that the
@@ -112,37 +142,42 @@ struct PairQueue {
     int32_t j[kQueue];
 };
 
-template <bool VEL, bool PSI>
+// Pair integrand of entry k of the queue (short_range_integrand, integrands.jl:2-18).  R is
+// the evaluation precision: the separation was formed in FP64 and is cast to R here.
+template <bool VEL, bool PSI, typename R>
 __device__ __forceinline__ void pair_eval(const KParams& K, const double* __restrict__ src, int64_t Ns,
-                                          const PairQueue& Q, int k, PairAcc& acc) {
-    const double two_over_sqrt_pi = 1.1283791670955126;  // 2/sqrt(pi)
-    const double r0 = Q.r[0][k], r1 = Q.r[1][k], r2 = Q.r[2][k];
+                                          const PairQueue& Q, int k, PairAcc<R>& acc) {
+    const R r0 = (R)Q.r[0][k], r1 = (R)Q.r[1][k], r2 = (R)Q.r[2][k];
     const int64_t j = Q.j[k];
-    const double q0 = src[3 * Ns + j], q1 = src[4 * Ns + j], q2 = src[5 * Ns + j];
-    const double r = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
-    const double rinv = 1.0 / r;
-    double wa = 1.0, wg = 1.0;  // erfc(alpha r) and erfc(alpha r) + 2/sqrt(pi) alpha r exp(-(alpha r)^2)
-    if (K.ewald_ntab > 0) ewald_weights(K, K.alpha * r, wa, wg);
-    (void)two_over_sqrt_pi;
+    const R q0 = (R)src[3 * Ns + j], q1 = (R)src[4 * Ns + j], q2 = (R)src[5 * Ns + j];
+    R rinv, wa = 1, wg = 1;  // erfc(alpha r) and erfc(alpha r) + 2/sqrt(pi) alpha r exp(-(alpha r)^2)
+    if constexpr (std::is_same<R, float>::value) {
+        rinv = rsqrtf(r0 * r0 + r1 * r1 + r2 * r2);
+        if (K.ewald_ntab > 0) ewald_weights_f(K, (float)K.alpha / rinv, wa, wg);
+    } else {
+        const double r = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
+        rinv = 1.0 / r;
+        if (K.ewald_ntab > 0) ewald_weights(K, K.alpha * r, wa, wg);
+    }
     if (VEL) {
-        const double f = wg * rinv * rinv * rinv;
-        acc.v[0] += f * (q1 * r2 - q2 * r1);
-        acc.v[1] += f * (q2 * r0 - q0 * r2);
-        acc.v[2] += f * (q0 * r1 - q1 * r0);
+        const R f = wg * rinv * rinv * rinv;
+        acc_add<R>(acc.v[0], acc.cv[0], f * (q1 * r2 - q2 * r1));
+        acc_add<R>(acc.v[1], acc.cv[1], f * (q2 * r0 - q0 * r2));
+        acc_add<R>(acc.v[2], acc.cv[2], f * (q0 * r1 - q1 * r0));
     }
     if (PSI) {
-        const double f = wa * rinv;
-        acc.p[0] += f * q0;
-        acc.p[1] += f * q1;
-        acc.p[2] += f * q2;
+        const R f = wa * rinv;
+        acc_add<R>(acc.p[0], acc.cp[0], f * q0);
+        acc_add<R>(acc.p[1], acc.cp[1], f * q1);
+        acc_add<R>(acc.p[2], acc.cp[2], f * q2);
     }
 }
 
-template <bool VEL, bool PSI>
+template <bool VEL, bool PSI, typename R>
 __device__ __forceinline__ void pair_range_q(const KParams& K, const double x[3], int64_t i, int32_t iprev,
                                              bool skip_local, const double* __restrict__ src, int64_t Ns,
                                              const int32_t* __restrict__ seg, int64_t b, int64_t e, int lane,
-                                             PairAcc& acc, PairQueue& Q, int& qcount) {
+                                             PairAcc<R>& acc, PairQueue& Q, int& qcount) {
     for (int64_t base = b; base < e; base += 32) {
         const int64_t j = base + lane;
         bool inr = false;
@@ -166,7 +201,7 @@ __device__ __forceinline__ void pair_range_q(const KParams& K, const double x[3]
         qcount += __popc(m);
         __syncwarp();
         if (qcount >= 32) {
-            pair_eval<VEL, PSI>(K, src, Ns, Q, lane, acc);
+            pair_eval<VEL, PSI, R>(K, src, Ns, Q, lane, acc);
             __syncwarp();
             const int rest = qcount - 32;
             if (lane < rest) {
@@ -193,9 +228,10 @@ __device__ __forceinline__ unsigned long long warp_sum_u(unsigned long long v) {
     return v;
 }
 
-// One warp per destination node (visited in cell order when cell lists are used).
-template <bool VEL, bool PSI>
-__global__ void __launch_bounds__(256) pair_kernel_f64(
+// One warp per destination node (visited in cell order when cell lists are used).  R = double
+// for the plain form, float for the mixed form (separations always formed in FP64).
+template <bool VEL, bool PSI, typename R>
+__global__ void __launch_bounds__(256) pair_kernel(
     KParams K, CellGrid cg, int64_t Np, int64_t Ns, const int32_t* __restrict__ dst_order,
     const double* __restrict__ nodes, const int32_t* __restrict__ idx_prev, const double* __restrict__ src,
     const int32_t* __restrict__ src_start, const int32_t* __restrict__ seg, int use_cells, int skip_local,
@@ -209,9 +245,9 @@ __global__ void __launch_bounds__(256) pair_kernel_f64(
     const int64_t i = use_cells ? dst_order[w] : w;
     const double x[3] = {nodes[i], nodes[Np + i], nodes[2 * Np + i]};
     const int32_t iprev = idx_prev[i];
-    PairAcc acc = {{0, 0, 0}, {0, 0, 0}, 0ull, 0ull};
+    PairAcc<R> acc = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0ull, 0ull};
     if (!use_cells) {
-        pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, 0, Ns, lane, acc, Q, qcount);
+        pair_range_q<VEL, PSI, R>(K, x, i, iprev, skip_local, src, Ns, seg, 0, Ns, lane, acc, Q, qcount);
     } else {
         const int M = cg.M;
         const int nc0 = cg.nc[0], nc1 = cg.nc[1], nc2 = cg.nc[2];
@@ -227,27 +263,37 @@ __global__ void __launch_bounds__(256) pair_kernel_f64(
                 const int64_t base = ((int64_t)zz * nc1 + yy) * nc0;
                 const int lo = cx - M, hi = cx + M;
                 if (lo >= 0 && hi < nc0) {
-                    pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo],
+                    pair_range_q<VEL, PSI, R>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo],
                                          src_start[base + hi + 1], lane, acc, Q, qcount);
                 } else if (lo < 0) {
-                    pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo + nc0],
+                    pair_range_q<VEL, PSI, R>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo + nc0],
                                          src_start[base + nc0], lane, acc, Q, qcount);
-                    pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base],
+                    pair_range_q<VEL, PSI, R>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base],
                                          src_start[base + hi + 1], lane, acc, Q, qcount);
                 } else {
-                    pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo],
+                    pair_range_q<VEL, PSI, R>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo],
                                          src_start[base + nc0], lane, acc, Q, qcount);
-                    pair_range_q<VEL, PSI>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base],
+                    pair_range_q<VEL, PSI, R>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base],
                                          src_start[base + hi - nc0 + 1], lane, acc, Q, qcount);
                 }
             }
         }
     }
-    if (lane < qcount) pair_eval<VEL, PSI>(K, src, Ns, Q, lane, acc);  // queue remainder
+    if (lane < qcount) pair_eval<VEL, PSI, R>(K, src, Ns, Q, lane, acc);  // queue remainder
     const double pref = K.Gamma / (4.0 * kPi);
     double v0 = 0, v1 = 0, v2 = 0, p0 = 0, p1 = 0, p2 = 0;
-    if (VEL) { v0 = warp_sum(acc.v[0]); v1 = warp_sum(acc.v[1]); v2 = warp_sum(acc.v[2]); }
-    if (PSI) { p0 = warp_sum(acc.p[0]); p1 = warp_sum(acc.p[1]); p2 = warp_sum(acc.p[2]); }
+    // lane partial sums (compensated in FP32) are reduced across the warp in FP64
+    auto lane_total = [](R s, R c) { return (double)s - (double)c; };
+    if (VEL) {
+        v0 = warp_sum(lane_total(acc.v[0], acc.cv[0]));
+        v1 = warp_sum(lane_total(acc.v[1], acc.cv[1]));
+        v2 = warp_sum(lane_total(acc.v[2], acc.cv[2]));
+    }
+    if (PSI) {
+        p0 = warp_sum(lane_total(acc.p[0], acc.cp[0]));
+        p1 = warp_sum(lane_total(acc.p[1], acc.cp[1]));
+        p2 = warp_sum(lane_total(acc.p[2], acc.cp[2]));
+    }
     unsigned long long inr = warp_sum_u(acc.inr), cand = warp_sum_u(acc.cand);
     if (lane == 0) {
         if (VEL) { vel[i] += pref * v0; vel[Np + i] += pref * v1; vel[2 * Np + i] += pref * v2; }
@@ -440,9 +486,15 @@ int pair_interactions(vpbs_handle* h, int fields) {
                                           skip_local, (double*)h->vel.p, (double*)h->psi.p,
                                           (unsigned long long*)h->counters.p);
     };
-    if (v && p) launch(pair_kernel_f64<true, true>);
-    else if (v) launch(pair_kernel_f64<true, false>);
-    else launch(pair_kernel_f64<false, true>);
+    if (h->P.precision == VPBS_PRECISION_MIXED) {
+        if (v && p) launch(pair_kernel<true, true, float>);
+        else if (v) launch(pair_kernel<true, false, float>);
+        else launch(pair_kernel<false, true, float>);
+    } else {
+        if (v && p) launch(pair_kernel<true, true, double>);
+        else if (v) launch(pair_kernel<true, false, double>);
+        else launch(pair_kernel<false, true, double>);
+    }
     h->launches++;
     return check_cuda(h, cudaGetLastError(), "pair kernel");
 }

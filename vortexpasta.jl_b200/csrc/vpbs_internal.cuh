@@ -28,12 +28,14 @@ struct KParams {
     int open_domain;      // NoSplitting
     // piecewise Taylor tables of erfc(x) and erfc(x) + 2/sqrt(pi) x exp(-x^2), x = alpha r
     const double* ewald_tab;
+    const float* ewald_tab_f;  // FP32 copy (first kEwaldNCf coefficients) for the mixed form
     int ewald_ntab;       // number of intervals (0: no splitting, weights are 1)
 };
 
 // Ewald weight tables: intervals of width 1/16 in x = alpha r, degree-9 Taylor polynomials
 // about the interval centres (coefficients from the closed-form derivatives of erfc).
 constexpr int kEwaldNC = 10;
+constexpr int kEwaldNCf = 6;  // FP32 tables: degree 5 (remainder < 1e-9 on |x - c| <= 1/32)
 constexpr double kEwaldInvH = 16.0;
 constexpr double kEwaldH = 1.0 / 16.0;
 void ewald_table_host(double xmax, int* ntab, double* tab);  // tab: 2 * ntab * kEwaldNC doubles
