@@ -211,25 +211,13 @@ def max_over_ranks(values, device, world):
     return t.tolist()
 
 
-def run_ours(args):
+def measure_form(vp, p, fs, args, dev, world, local_rank):
+    """Time one arithmetic form: device-resident steps (with per-stage events) and end-to-end
+    steps through velocity_on_nodes_.  Returns per-rank-max timings and the velocities."""
     import torch
     import torch.distributed as dist
-    rank, local_rank, world = dist_env()
-    if world > 1:
-        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
-                                timeout=__import__("datetime").timedelta(seconds=120))
-    if not torch.cuda.is_available():
-        raise RuntimeError("bench.py needs a CUDA GPU")
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    vp = load_package()
     from vortexpasta_b200 import _lib
-    fs, p = rank_workload(vp, args.workload, rank)
-    p = p.with_(device=local_rank)
-    Np = sum(len(f) for f in fs)
-    Nq = Np * len(p.quadrature)
     nodes, offsets = vp.curves.concat(fs)
-
     stream = torch.cuda.Stream(device=dev)
     cache = vp.init_cache(p)
     cache.set_stream(stream.cuda_stream)
@@ -288,13 +276,42 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = sum(s.elapsed_time(e) for s, e in zip(e_starts, e_ends))
 
+    v_api = np.concatenate(vs)
+    cache.close()
     total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], dev, world)
+    return {"total_ms": total_ms, "e2e_ms": e2e_ms, "stage_ms": stage_ms, "launches": launches,
+            "pairs_in_range": pairs_in_range, "v": v_dev.copy(), "v_api": v_api, "clk": clk}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    rank, local_rank, world = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA GPU")
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    vp = load_package()
+    from vortexpasta_b200 import _lib
+    fs, p = rank_workload(vp, args.workload, rank)
+    p = p.with_(device=local_rank)
+    Np = sum(len(f) for f in fs)
+    Nq = Np * len(p.quadrature)
+    nodes, offsets = vp.curves.concat(fs)
+
+    m64 = measure_form(vp, p, fs, args, dev, world, local_rank)
+    mixed = measure_form(vp, p.with_(precision="mixed"), fs, args, dev, world, local_rank) if args.mixed else None
+    total_ms, e2e_ms, stage_ms, clk = m64["total_ms"], m64["e2e_ms"], m64["stage_ms"], m64["clk"]
+    launches, pairs_in_range, v_dev = m64["launches"], m64["pairs_in_range"], m64["v"]
     ms_per_step = total_ms / args.steps
     value = world * Np * args.steps / (total_ms * 1e-3)
     e2e_value = world * Np * args.steps / (e2e_ms * 1e-3)
 
     if rank == 0:
-        lr = cache.params.splitting
+        lr = p.splitting
         n = [_lib.load().vpbs_fft_size(N, p.backend_long.sigma) for N in lr.Ns]
         S = {"Np": Np, "Nq": Nq, "n3": n[0] * n[1] * n[2], "nc3": (n[0] // 2 + 1) * n[1] * n[2], "pairs": pairs_in_range,
              "nq": len(p.quadrature)}
@@ -342,6 +359,26 @@ def run_ours(args):
             "clocks": clk.summary(),
             "pairs_in_range": int(pairs_in_range),
         }
+        if mixed is not None:
+            vm = mixed["v"]
+            line["forms"] = {
+                "fp64": {"value": value, "ms_per_step": ms_per_step, "e2e_value": e2e_value},
+                "mixed": {
+                    "value": world * Np * args.steps / (mixed["total_ms"] * 1e-3),
+                    "ms_per_step": mixed["total_ms"] / args.steps,
+                    "e2e_value": world * Np * args.steps / (mixed["e2e_ms"] * 1e-3),
+                    "speedup_vs_fp64": total_ms / mixed["total_ms"],
+                    "rel_l2_vs_fp64": float(np.linalg.norm(vm - v_dev) / np.linalg.norm(v_dev)),
+                    "max_err_vs_fp64": float(np.abs(vm - v_dev).max() / np.abs(v_dev).max()),
+                    "rel_l2_e2e_vs_fp64": float(np.linalg.norm(mixed["v_api"] - m64["v_api"]) /
+                                                np.linalg.norm(m64["v_api"])),
+                    "stages_ms": {k: statistics.mean(x) for k, x in mixed["stage_ms"].items()},
+                    "description": "FP32 pair sum / spreading / FFT / interpolation; FP64 positions, separations, "
+                                   "local and self terms, final accumulation",
+                },
+            }
+        if args.workload == "tangle1m":
+            args.no_cpu_baseline = True  # one oracle evaluation of 1M nodes takes minutes: not a bounded sample
         if world == 1 and not args.no_cpu_baseline:
             cores = host_cores()
             t_cpu, v_cpu = cpu_oracle_time(fs, p, cores, args.cpu_reps)
@@ -350,7 +387,6 @@ def run_ours(args):
                                               "(CPU FP64 restatement, OpenMP), best taken"}
             line["accuracy"] = {"rel_l2_vs_oracle": float(np.linalg.norm(v_dev - v_cpu) / np.linalg.norm(v_cpu))}
         print(json.dumps(line), flush=True)
-    cache.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
@@ -365,6 +401,8 @@ def main():
     ap.add_argument("--workload", default="tangle20k", choices=sorted(WORKLOAD_DESC))
     ap.add_argument("--cpu-reps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", dest="mixed", action="store_false",
+                    help="skip the mixed-precision (FP32 bulk) form reported under 'forms'")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
