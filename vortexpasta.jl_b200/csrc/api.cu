@@ -362,9 +362,11 @@ int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t short
     const bool with_long = longrange && lia_mode != VPBS_LIA_ONLY && !h->K.open_domain;
     // The long range (spread, FFTs, Fourier operators) runs on the auxiliary stream while the
     // short range runs on the main stream; only the long-range interpolation, which adds into
-    // the same outputs, waits for the short range.  The main stream then joins.
+    // the same outputs, waits for the short range.  The main stream then joins.  With stage
+    // timing on, everything runs in order on the main stream so that each stage is timed alone.
     cudaStream_t main = h->stream;
-    if (with_long) {
+    const bool fork = with_long && !h->timing;
+    if (fork) {
         if ((rc = check_cuda(h, cudaEventRecord(h->ev_fork, main), "fork"))) return rc;
         if ((rc = check_cuda(h, cudaStreamWaitEvent(h->aux_stream, h->ev_fork, 0), "fork"))) return rc;
     }
@@ -378,7 +380,9 @@ int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t short
         if (pairs)
             if ((rc = pair_interactions(h, fields))) return rc;
     }
-    if (with_long) {
+    if (with_long && !fork) {
+        if ((rc = longrange_compute(h, fields))) return rc;
+    } else if (with_long) {
         if ((rc = check_cuda(h, cudaEventRecord(h->ev_short, main), "short done"))) return rc;
         h->stream = h->aux_stream;
         h->interp_wait = h->ev_short;

@@ -336,6 +336,126 @@ __global__ void __launch_bounds__(kBrickThreads) spread_brick_kernel(
     }
 }
 
+// Register-column brick spreading for 16^3 bricks (no atomics at all): the 256 threads of a CTA
+// are the 16 x 16 (x, y) columns of the brick and each keeps its column's 16 z values of the
+// three components in registers.  The points whose footprint meets the brick are staged in
+// batches in shared memory as brick-aligned, zero-padded kernel rows phi_x[16], phi_y[16],
+// phi_z[16], so every point is one unconditional rank-1 update per thread:
+//     acc_c[z] += q_c phi_x[x] phi_y[y] * phi_z[z].
+// A warp covers two y rows and skips the points whose footprint misses both.
+constexpr int kColB = 16;
+constexpr int kColThreads = 256;
+constexpr int kColBatch = 32;
+
+template <typename T>
+struct ColSlot {
+    T q[4];          // charges (q[3] unused)
+    T px[kColB];     // brick-aligned kernel rows, zero outside the footprint
+    T py[kColB];
+    T pz[kColB];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kColThreads, 2) spread_column_kernel(
+    LRSizes S, int nb0, int nb1, int nb2, const int32_t* __restrict__ bin_start, const T* __restrict__ binned,
+    const int32_t* __restrict__ foot, T* __restrict__ grid) {
+    __shared__ __align__(16) ColSlot<T> slot[kColBatch];
+    __shared__ int2 yrange[kColBatch];  // overlap rows [lo, hi) in y; (0, 0) when the overlap is empty
+    __shared__ int nbin_start[8], nbin_base[9];
+    const int w = 2 * S.m;
+    const int stride = 3 + 3 * w;
+    const int bx = blockIdx.x % nb0;
+    const int by = (blockIdx.x / nb0) % nb1;
+    const int bz = blockIdx.x / (nb0 * nb1);
+    const int bs[3] = {bx * kColB, by * kColB, bz * kColB};
+    const int tx = threadIdx.x & (kColB - 1), ty = threadIdx.x / kColB;
+    const int y0 = 2 * (threadIdx.x >> 5);  // the warp's rows: y0, y0 + 1
+    if (threadIdx.x < 8) {
+        const int nbr = threadIdx.x;
+        const int cx = (bx - (nbr & 1) + nb0) % nb0;
+        const int cy = (by - ((nbr >> 1) & 1) + nb1) % nb1;
+        const int cz = (bz - ((nbr >> 2) & 1) + nb2) % nb2;
+        const int b = (cz * nb1 + cy) * nb0 + cx;
+        nbin_start[nbr] = bin_start[b];
+        nbin_base[nbr + 1] = bin_start[b + 1] - bin_start[b];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        nbin_base[0] = 0;
+        for (int k = 1; k <= 8; ++k) nbin_base[k] += nbin_base[k - 1];
+    }
+    __syncthreads();
+    const int ntot = nbin_base[8];
+    T acc0[kColB], acc1[kColB], acc2[kColB];
+#pragma unroll
+    for (int z = 0; z < kColB; ++z) acc0[z] = acc1[z] = acc2[z] = (T)0;
+    for (int k0 = 0; k0 < ntot; k0 += kColBatch) {
+        // ---- stage: 8 threads per point slot ----
+        {
+            const int s = threadIdx.x >> 3, part = threadIdx.x & 7;
+            const int k = k0 + s;
+            ColSlot<T>& sl = slot[s];
+            if (k < ntot) {
+                int nb = 0;
+#pragma unroll
+                for (int i = 1; i < 8; ++i) nb += k >= nbin_base[i];
+                const int64_t j = nbin_start[nb] + (k - nbin_base[nb]);
+                int o[3];
+                bool empty = false;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    o[d] = foot[3 * j + d] - bs[d];
+                    if (o[d] >= kColB) o[d] -= S.n[d];
+                    const int lo = o[d] < 0 ? 0 : o[d];
+                    const int hi = o[d] + w < kColB ? o[d] + w : kColB;
+                    empty = empty || lo >= hi;
+                }
+                const T* src = binned + j * stride;
+                for (int e = part; e < 3 * kColB; e += 8) {
+                    const int d = e / kColB, t = e % kColB, r = t - o[d];
+                    const T v = (r >= 0 && r < w) ? src[3 + d * w + r] : (T)0;
+                    (d == 0 ? sl.px : d == 1 ? sl.py : sl.pz)[t] = v;
+                }
+                if (part < 3) sl.q[part] = src[part];
+                if (part == 3) {
+                    const int lo = o[1] < 0 ? 0 : o[1];
+                    const int hi = o[1] + w < kColB ? o[1] + w : kColB;
+                    yrange[s] = empty ? make_int2(0, 0) : make_int2(lo, hi);
+                }
+            } else if (part == 0) {
+                yrange[s] = make_int2(0, 0);
+            }
+        }
+        __syncthreads();
+        // ---- accumulate ----
+        const int nbatch = ntot - k0 < kColBatch ? ntot - k0 : kColBatch;
+        for (int s = 0; s < nbatch; ++s) {
+            const int2 yr = yrange[s];
+            if (y0 + 2 <= yr.x || y0 >= yr.y) continue;  // warp-uniform
+            const ColSlot<T>& sl = slot[s];
+            const T fxy = sl.px[tx] * sl.py[ty];
+            const T c0 = sl.q[0] * fxy, c1 = sl.q[1] * fxy, c2 = sl.q[2] * fxy;
+#pragma unroll
+            for (int z = 0; z < kColB; ++z) {
+                const T f = sl.pz[z];
+                acc0[z] = fma(c0, f, acc0[z]);
+                acc1[z] = fma(c1, f, acc1[z]);
+                acc2[z] = fma(c2, f, acc2[z]);
+            }
+        }
+        __syncthreads();
+    }
+    const int64_t ng = S.ngrid;
+    const int64_t plane = (int64_t)S.n[1] * S.n[0];
+    T* g = grid + ((int64_t)bs[2] * S.n[1] + bs[1] + ty) * S.n[0] + bs[0] + tx;
+#pragma unroll
+    for (int z = 0; z < kColB; ++z) {
+        g[z * plane] = acc0[z];
+        g[ng + z * plane] = acc1[z];
+        g[2 * ng + z * plane] = acc2[z];
+    }
+}
+
 // Type-2 interpolation, one warp per node (cell order when available): lanes take (sy, sz)
 // pairs of the footprint, loop over x, and the warp reduces the three components.
 template <int W, typename T>  // kernel width 2m (compile-time: per-lane tables stay in registers)
@@ -532,7 +652,9 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
             kern<<<nblk, kBrickThreads, smem, h->stream>>>(S, nb0, nb1, nb2, start, bsrc, foot, grid);
         };
         switch (B) {
-            case 16: launch(spread_brick_kernel<16, T>); break;
+            case kColB:
+                spread_column_kernel<T><<<nblk, kColThreads, 0, h->stream>>>(S, nb0, nb1, nb2, start, bsrc, foot, grid);
+                break;
             case 12: launch(spread_brick_kernel<12, T>); break;
             case 10: launch(spread_brick_kernel<10, T>); break;
             default: launch(spread_brick_kernel<8, T>); break;
