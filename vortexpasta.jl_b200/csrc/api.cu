@@ -174,6 +174,13 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
             if (M > 0 && cg.nc[d] < 2 * M + 1)
                 return set_error(nullptr, VPBS_ERR_PARAMS, "cell lists: the cut-off distance r_cut is too large for periodic padding");
         }
+        // x slabs per cell: up to 4 while the (2M+1)^3-cell neighbourhood stays within 729 slabs
+        cg.G = 1;
+        if (M > 0) {
+            const int W = 2 * M + 1;
+            cg.G = std::max(1, std::min(4, 729 / (W * W * W)));
+            cg.nc[0] *= cg.G;
+        }
         cg.ncell = (int64_t)cg.nc[0] * cg.nc[1] * cg.nc[2];
         if (cg.ncell > (int64_t)1 << 30) return set_error(nullptr, VPBS_ERR_PARAMS, "too many cells (rcut too small)");
         if (!(P.sigma > 1.0)) return set_error(nullptr, VPBS_ERR_PARAMS, "NUFFT oversampling factor sigma must be > 1");
@@ -209,8 +216,18 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
         std::vector<float> tabf((size_t)2 * ntab * kEwaldNCf);
         for (size_t k = 0; k < (size_t)2 * ntab; ++k)
             for (int n = 0; n < kEwaldNCf; ++n) tabf[k * kEwaldNCf + n] = (float)tab[k * kEwaldNC + n];
+        // interleaved copy (erfc coefficient, g coefficient) per degree, stored after the FP32 table
+        std::vector<double> tab2((size_t)2 * ntab * kEwaldNC);
+        for (size_t k = 0; k < (size_t)ntab; ++k)
+            for (int n = 0; n < kEwaldNC; ++n) {
+                tab2[2 * (k * kEwaldNC + n)] = tab[k * kEwaldNC + n];
+                tab2[2 * (k * kEwaldNC + n) + 1] = tab[(ntab + k) * kEwaldNC + n];
+            }
         const size_t bytes_d = sizeof(double) * tab.size(), bytes_f = sizeof(float) * tabf.size();
-        rc = ensure(h, h->ewald_tab, bytes_d + bytes_f, "Ewald tables");
+        rc = ensure(h, h->ewald_tab, 2 * bytes_d + bytes_f, "Ewald tables");
+        if (!rc)
+            rc = check_cuda(h, cudaMemcpy((char*)h->ewald_tab.p + bytes_d + bytes_f, tab2.data(), bytes_d,
+                                          cudaMemcpyHostToDevice), "copy Ewald tables");
         if (!rc)
             rc = check_cuda(h, cudaMemcpy(h->ewald_tab.p, tab.data(), bytes_d, cudaMemcpyHostToDevice), "copy Ewald tables");
         if (!rc)
@@ -218,6 +235,7 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
                             "copy Ewald tables");
         h->K.ewald_tab = (const double*)h->ewald_tab.p;
         h->K.ewald_tab_f = (const float*)((const char*)h->ewald_tab.p + bytes_d);
+        h->K.ewald_tab2 = (const double2*)((const char*)h->ewald_tab.p + bytes_d + bytes_f);
         h->K.ewald_ntab = ntab;
     }
     if (rc) {

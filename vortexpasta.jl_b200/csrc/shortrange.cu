@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(256) pair_kernel(
                 int yy = cy + dy;
                 yy = yy < 0 ? yy + nc1 : (yy >= nc1 ? yy - nc1 : yy);
                 const int64_t base = ((int64_t)zz * nc1 + yy) * nc0;
-                const int lo = cx - M, hi = cx + M;
+                const int lo = cx - M * cg.G, hi = cx + M * cg.G;  // M cells = M G slabs in x
                 if (lo >= 0 && hi < nc0) {
                     pair_range_q<VEL, PSI, R>(K, x, i, iprev, skip_local, src, Ns, seg, src_start[base + lo],
                                          src_start[base + hi + 1], lane, acc, Q, qcount);
@@ -300,6 +300,355 @@ __global__ void __launch_bounds__(256) pair_kernel(
         if (PSI) { psi[i] += pref * p0; psi[Np + i] += pref * p1; psi[2 * Np + i] += pref * p2; }
         atomicAdd(&counters[0], inr);
         atomicAdd(&counters[1], cand);
+    }
+}
+
+// ---- cell-tiled pair kernel ----
+// One CTA per destination cell.  The sources of the (2M+1)^3 neighbour cells (in x: the G
+// slabs of each) are concatenated in (row (dy, dz), slab) order and streamed through shared
+// memory in tiles of kTile sources, as coordinates relative to the cell corner (already
+// shifted to the periodic image next to the cell) split into FP32 hi + lo parts.  Per
+// destination and row the candidate range is trimmed to the slabs within r_cut of the node.
+// Candidates are screened on the hi parts in FP32 against r_cut^2 (1 + 2e-5) -- the FP32
+// rounding of r^2 stays below 1e-6 r_cut^2 here, so no pair in range is lost -- and queued; the
+// queued pairs are decided (r^2 <= r_cut^2) and evaluated with the separation formed in FP64
+// from the hi + lo parts (relative error ~1e-15), two pairs per lane at a time so that their
+// dependency chains overlap.  Destinations are handled in passes of up to kPassDst nodes;
+// warps take (destination, row-part) items and add each item's warp-reduced sum to the
+// destination's shared-memory accumulator.
+constexpr int kTile = 2816;
+constexpr int kTilePad = kTile + 32;  // a chunk of 32 lanes may read past the tile end (masked)
+constexpr int kPassDst = 64;
+constexpr int kMaxNbCells = 729;  // neighbour slabs: (2M+1)^2 rows x (2M+1) G slabs
+constexpr int kMaxRows = 81;      // (2M+1)^2
+constexpr int kTileQueue = 128;   // screened pairs are evaluated 64 at a time (two per lane)
+constexpr double kScreenMargin = 2e-5;
+
+struct TileSmem {
+    // relative source position split as hi + lo FP32 parts (|lo| <= ulp(hi) / 2, together ~48
+    // significant bits); hi.w holds the cell-sorted index, lo.w the segment (int bits)
+    float4 hi[kTilePad];
+    float4 lo[kTilePad];
+    int32_t queue[kPairThreads / 32][kTileQueue];  // per warp: tile indices of screened pairs
+    double acc[kPassDst][6];  // per destination: velocity, streamfunction
+    double dx[kPassDst][3];   // destination positions
+    int32_t di[kPassDst], dprev[kPassDst];
+    int32_t off[kMaxNbCells + 1];  // concatenated offsets of the neighbour slabs
+    int32_t cstart[kMaxNbCells];   // first cell-sorted source of each neighbour slab
+    int2 rng[kPairThreads / 32][kMaxRows];  // per warp: candidate range of every row
+};
+
+// 1/sqrt(s) in FP64: FP32 hardware estimate refined by two Newton-Raphson steps
+// y <- y (3 - s y^2) / 2 (quadratic convergence: ~1e-7 -> ~1e-14 -> rounding level).
+__device__ __forceinline__ double rsqrt_nr(double s) {
+    double y = (double)rsqrtf((float)s);
+    double t = s * y;
+    y = y * fma(-0.5 * t, y, 1.5);
+    t = s * y;
+    y = y * fma(-0.5 * t, y, 1.5);
+    return y;
+}
+
+// Both Ewald weights from the interleaved table (one 16-byte load per degree).
+__device__ __forceinline__ void ewald_weights2(const KParams& K, double x, double& a, double& g) {
+    int k = (int)(x * kEwaldInvH);
+    k = k < K.ewald_ntab ? k : K.ewald_ntab - 1;
+    const double t = x - (k + 0.5) * kEwaldH;
+    const double2* c = K.ewald_tab2 + k * kEwaldNC;
+    double2 v = __ldg(c + kEwaldNC - 1);
+    a = v.x;
+    g = v.y;
+#pragma unroll
+    for (int n = kEwaldNC - 2; n >= 0; --n) {
+        v = __ldg(c + n);
+        a = fma(a, t, v.x);
+        g = fma(g, t, v.y);
+    }
+}
+
+// One of the Ewald weights (erfc for the streamfunction, g for the velocity).
+__device__ __forceinline__ double ewald_weight1(const KParams& K, double x, int which) {
+    int k = (int)(x * kEwaldInvH);
+    k = k < K.ewald_ntab ? k : K.ewald_ntab - 1;
+    const double t = x - (k + 0.5) * kEwaldH;
+    const double* c = K.ewald_tab + (which * K.ewald_ntab + k) * kEwaldNC;
+    double a = __ldg(c + kEwaldNC - 1);
+#pragma unroll
+    for (int n = kEwaldNC - 2; n >= 0; --n) a = fma(a, t, __ldg(c + n));
+    return a;
+}
+
+static_assert(sizeof(TileSmem) <= 113 * 1024, "two pair-kernel CTAs must fit in one SM's shared memory");
+
+// Distance from x to the cell [lo, lo + h], less a margin of 1e-9 h so that rounding in the
+// binning can never cull a source that is in range.
+__device__ __forceinline__ double box_gap(double x, double lo, double h) {
+    const double g = fmax(fmax(lo - x, x - (lo + h)), 0.0);
+    return fmax(g - 1e-9 * h, 0.0);
+}
+
+// Two queued pairs per lane (tile indices t0, t1; v0, v1 mark valid entries): the separation
+// formed in FP64 from the hi + lo parts, the r^2 <= r_cut^2 decision, and the pair integrand
+// (short_range_integrand, integrands.jl:2-18) in precision R.  Entries that are invalid or out
+// of range are evaluated at a harmless separation (r_cut, 0, 0) with zero charge, so both
+// chains run straight through.  Called by all lanes of the warp.
+template <bool VEL, bool PSI, typename R>
+__device__ __forceinline__ void tile_eval2(const KParams& K, const double xd[3], const TileSmem& S,
+                                           const double* __restrict__ src, int64_t Ns, int t0, bool v0, int t1,
+                                           bool v1, PairAcc<R>& acc, unsigned long long& ninr) {
+    const int tt[2] = {t0, t1};
+    const bool vv[2] = {v0, v1};
+    double d[2][3], q[2][3], s2[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        const float4 h = S.hi[tt[u]], l = S.lo[tt[u]];
+        const int64_t j = __float_as_int(h.w);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) q[u][c] = vv[u] ? src[(3 + c) * Ns + j] : 0.0;
+        d[u][0] = xd[0] - ((double)h.x + (double)l.x);
+        d[u][1] = xd[1] - ((double)h.y + (double)l.y);
+        d[u][2] = xd[2] - ((double)h.z + (double)l.z);
+        s2[u] = d[u][0] * d[u][0] + d[u][1] * d[u][1] + d[u][2] * d[u][2];
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        const bool ok = vv[u] && s2[u] <= K.rcut2;
+        ninr += __popc(__ballot_sync(0xffffffffu, ok));
+        if (!ok) {
+            d[u][0] = K.rcut;
+            d[u][1] = d[u][2] = 0.0;
+            s2[u] = K.rcut2;
+            q[u][0] = q[u][1] = q[u][2] = 0.0;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        const R r0 = (R)d[u][0], r1 = (R)d[u][1], r2 = (R)d[u][2];
+        R rinv, wa = 1, wg = 1;
+        if constexpr (std::is_same<R, float>::value) {
+            rinv = rsqrtf((float)s2[u]);
+            ewald_weights_f(K, (float)K.alpha / rinv, wa, wg);
+        } else {
+            rinv = rsqrt_nr(s2[u]);
+            const double xa = K.alpha * (s2[u] * rinv);
+            if (VEL && PSI) ewald_weights2(K, xa, wa, wg);
+            else if (VEL) wg = ewald_weight1(K, xa, 1);
+            else wa = ewald_weight1(K, xa, 0);
+        }
+        const R q0 = (R)q[u][0], q1 = (R)q[u][1], q2 = (R)q[u][2];
+        if (VEL) {
+            const R f = wg * rinv * rinv * rinv;
+            acc_add<R>(acc.v[0], acc.cv[0], f * (q1 * r2 - q2 * r1));
+            acc_add<R>(acc.v[1], acc.cv[1], f * (q2 * r0 - q0 * r2));
+            acc_add<R>(acc.v[2], acc.cv[2], f * (q0 * r1 - q1 * r0));
+        }
+        if (PSI) {
+            const R f = wa * rinv;
+            acc_add<R>(acc.p[0], acc.cp[0], f * q0);
+            acc_add<R>(acc.p[1], acc.cp[1], f * q1);
+            acc_add<R>(acc.p[2], acc.cp[2], f * q2);
+        }
+    }
+}
+
+// Candidates [a, b) of the tile against the destination (cell-relative position xd in FP64,
+// xr in FP32; node i, previous node iprev): FP32 screen on the hi parts, compaction of the
+// survivors into the warp's queue, evaluation 64 at a time.
+template <bool VEL, bool PSI, bool SKIP, typename R>
+__device__ __forceinline__ void tile_range_q(const KParams& K, const double xd[3], float3 xr, float rc2s, int i,
+                                             int iprev, const TileSmem& S, const double* __restrict__ src, int64_t Ns,
+                                             int a, int b, int lane, PairAcc<R>& acc, int32_t* Q, int& qcount,
+                                             unsigned long long& ninr) {
+    for (int base = a; base < b; base += 32) {
+        const int t = base + lane;
+        const float4 p = S.hi[t];
+        const float e0 = xr.x - p.x, e1 = xr.y - p.y, e2 = xr.z - p.z;
+        bool inr = t < b && fmaf(e0, e0, fmaf(e1, e1, e2 * e2)) <= rc2s;
+        if (SKIP) {
+            const int sg = __float_as_int(S.lo[t].w);
+            inr = inr && sg != i && sg != iprev;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, inr);
+        if (inr) Q[qcount + __popc(m & ((1u << lane) - 1u))] = t;
+        qcount += __popc(m);
+        __syncwarp();
+        if (qcount >= 64) {
+            tile_eval2<VEL, PSI, R>(K, xd, S, src, Ns, Q[lane], true, Q[32 + lane], true, acc, ninr);
+            __syncwarp();
+            if (lane < qcount - 64) Q[lane] = Q[64 + lane];
+            __syncwarp();
+            qcount -= 64;
+        }
+    }
+}
+
+template <bool VEL, bool PSI, bool SKIP, typename R>
+__global__ void __launch_bounds__(kPairThreads, 2) pair_cell_kernel(
+    KParams K, CellGrid cg, int64_t Np, int64_t Ns, const int32_t* __restrict__ dst_start,
+    const int32_t* __restrict__ dst_order, const double* __restrict__ nodes, const int32_t* __restrict__ idx_prev,
+    const double* __restrict__ src, const int32_t* __restrict__ src_start, const int32_t* __restrict__ seg,
+    double* __restrict__ vel, double* __restrict__ psi, unsigned long long* __restrict__ counters) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TileSmem& S = *reinterpret_cast<TileSmem*>(smem_raw);
+    const int M = cg.M, G = cg.G, W = 2 * M + 1, WX = W * G, nrow = W * W, ncb = nrow * WX;
+    const int nc0 = cg.nc[0], nc1 = cg.nc[1], nc2 = cg.nc[2];
+    const int ncc = nc0 / G;  // cells in x (each made of G slabs)
+    const int64_t cell = blockIdx.x;
+    const int c0 = (int)(cell % ncc), c1 = (int)((cell / ncc) % nc1), c2 = (int)(cell / ((int64_t)ncc * nc1));
+    const int64_t slab0 = ((int64_t)c2 * nc1 + c1) * nc0 + (int64_t)c0 * G;
+    const int d0 = dst_start[slab0], nd = dst_start[slab0 + G] - d0;
+    if (nd == 0) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double hx = K.L[0] / nc0, h1 = K.L[1] / nc1, h2 = K.L[2] / nc2, inv_hx = nc0 / K.L[0];
+    const int xs0 = c0 * G - M * G;  // first neighbour slab in x (unwrapped index)
+    const double o0 = c0 * G * hx, o1 = c1 * h1, o2 = c2 * h2;  // cell corner: origin of the FP32 coordinates
+    const float rc2s = (float)(K.rcut2 * (1.0 + kScreenMargin));
+    // neighbour slabs in (row, slab) order: first cell-sorted source and count
+    for (int ci = threadIdx.x; ci < ncb; ci += kPairThreads) {
+        const int r = ci / WX, k = ci % WX;
+        int xx = xs0 + k, yy = c1 + r % W - M, zz = c2 + r / W - M;
+        xx = xx < 0 ? xx + nc0 : (xx >= nc0 ? xx - nc0 : xx);
+        yy = yy < 0 ? yy + nc1 : (yy >= nc1 ? yy - nc1 : yy);
+        zz = zz < 0 ? zz + nc2 : (zz >= nc2 ? zz - nc2 : zz);
+        const int64_t c = ((int64_t)zz * nc1 + yy) * nc0 + xx;
+        const int s0 = src_start[c];
+        S.cstart[ci] = s0;
+        S.off[ci + 1] = src_start[c + 1] - s0;
+    }
+    __syncthreads();
+    if (warp == 0) {  // counts -> concatenated offsets
+        int carry = 0;
+        for (int base = 0; base < ncb; base += 32) {
+            const int ci = base + lane;
+            int v = ci < ncb ? S.off[ci + 1] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += t;
+            }
+            if (ci < ncb) S.off[ci + 1] = carry + v;
+            carry += __shfl_sync(0xffffffffu, v, 31);
+        }
+        if (lane == 0) S.off[0] = 0;
+    }
+    __syncthreads();
+    const int ntot = S.off[ncb];
+    const double pref = K.Gamma / (4.0 * kPi);
+    unsigned long long ninr = 0, ncand = 0;  // warp-uniform
+    for (int p0 = 0; p0 < nd; p0 += kPassDst) {
+        const int np = nd - p0 < kPassDst ? nd - p0 : kPassDst;
+        __syncthreads();  // the previous pass has written its results
+        for (int t = threadIdx.x; t < np; t += kPairThreads) {
+            const int i = dst_order[d0 + p0 + t];
+            S.di[t] = i;
+            S.dprev[t] = idx_prev[i];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) S.dx[t][d] = nodes[d * Np + i];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) S.acc[t][c] = 0.0;
+        }
+        const int P = np >= kPairThreads / 32 ? 1 : (kPairThreads / 32) / np;  // row parts per destination
+        const int nitems = np * P;
+        for (int T0 = 0; T0 < ntot; T0 += kTile) {
+            const int T1 = ntot - T0 < kTile ? ntot : T0 + kTile;
+            __syncthreads();  // previous tile consumed, destinations loaded
+            for (int ci = warp; ci < ncb; ci += kPairThreads / 32) {
+                const int o = S.off[ci];
+                const int a = o > T0 ? o : T0, b = S.off[ci + 1] < T1 ? S.off[ci + 1] : T1;
+                if (a >= b) continue;
+                // periodic image of this slab next to the destination cell
+                const int r = ci / WX, k = ci % WX;
+                const int xu = xs0 + k, yu = c1 + r % W - M, zu = c2 + r / W - M;
+                const double sx = xu < 0 ? -K.L[0] : (xu >= nc0 ? K.L[0] : 0.0);
+                const double sy = yu < 0 ? -K.L[1] : (yu >= nc1 ? K.L[1] : 0.0);
+                const double sz = zu < 0 ? -K.L[2] : (zu >= nc2 ? K.L[2] : 0.0);
+                const int g0 = S.cstart[ci] + (a - o);
+                for (int e = lane; e < b - a; e += 32) {
+                    const int j = g0 + e;
+                    const int t = a - T0 + e;
+                    const double u0 = src[j] + sx - o0, u1 = src[Ns + j] + sy - o1, u2 = src[2 * Ns + j] + sz - o2;
+                    const float f0 = (float)u0, f1 = (float)u1, f2 = (float)u2;
+                    S.hi[t] = make_float4(f0, f1, f2, __int_as_float(j));
+                    S.lo[t] = make_float4((float)(u0 - f0), (float)(u1 - f1), (float)(u2 - f2),
+                                          __int_as_float(SKIP ? seg[j] : 0));
+                }
+            }
+            __syncthreads();
+            for (int it = warp; it < nitems; it += kPairThreads / 32) {
+                const int dl = it % np, part = it / np;
+                const double x[3] = {S.dx[dl][0], S.dx[dl][1], S.dx[dl][2]};
+                // candidate range of every row, trimmed to the slabs within r_cut of the node
+                for (int r = lane; r < nrow; r += 32) {
+                    const double gy = box_gap(x[1], (c1 + r % W - M) * h1, h1);
+                    const double gz = box_gap(x[2], (c2 + r / W - M) * h2, h2);
+                    const double gyz = gy * gy + gz * gz;
+                    int a = 0, b = 0;
+                    if (gyz <= K.rcut2) {
+                        const double w = (double)sqrtf((float)(K.rcut2 - gyz)) * (1.0 + 1e-6) + 1e-9 * hx;
+                        int klo = (int)floor((x[0] - w) * inv_hx) - xs0;
+                        int khi = (int)floor((x[0] + w) * inv_hx) - xs0;
+                        klo = klo < 0 ? 0 : klo;
+                        khi = khi > WX - 1 ? WX - 1 : khi;
+                        if (klo <= khi) {
+                            a = S.off[r * WX + klo];
+                            b = S.off[r * WX + khi + 1];
+                        }
+                    }
+                    S.rng[warp][r] = make_int2(a, b);
+                }
+                __syncwarp();
+                PairAcc<R> acc = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0ull, 0ull};
+                int qcount = 0;
+                int32_t* Q = S.queue[warp];
+                const double xd[3] = {x[0] - o0, x[1] - o1, x[2] - o2};
+                const float3 xr = make_float3((float)xd[0], (float)xd[1], (float)xd[2]);
+                const int i = S.di[dl], iprev = S.dprev[dl];
+                for (int r = part; r < nrow; r += P) {
+                    const int2 ab = S.rng[warp][r];
+                    const int a = ab.x > T0 ? ab.x : T0, b = ab.y < T1 ? ab.y : T1;
+                    if (a < b) {
+                        ncand += b - a;
+                        tile_range_q<VEL, PSI, SKIP, R>(K, xd, xr, rc2s, i, iprev, S, src, Ns, a - T0, b - T0, lane, acc, Q,
+                                                        qcount, ninr);
+                    }
+                }
+                tile_eval2<VEL, PSI, R>(K, xd, S, src, Ns, lane < qcount ? Q[lane] : 0, lane < qcount,
+                                        32 + lane < qcount ? Q[32 + lane] : 0, 32 + lane < qcount, acc, ninr);
+                auto lane_total = [](R s, R c) { return (double)s - (double)c; };
+                double s[6] = {0, 0, 0, 0, 0, 0};
+                if (VEL)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) s[c] = warp_sum(lane_total(acc.v[c], acc.cv[c]));
+                if (PSI)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) s[3 + c] = warp_sum(lane_total(acc.p[c], acc.cp[c]));
+                if (lane == 0) {
+                    if (VEL)
+                        for (int c = 0; c < 3; ++c) atomicAdd(&S.acc[dl][c], s[c]);
+                    if (PSI)
+                        for (int c = 0; c < 3; ++c) atomicAdd(&S.acc[dl][3 + c], s[3 + c]);
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < np; t += kPairThreads) {
+            const int64_t i = S.di[t];
+            if (VEL) {
+                vel[i] += pref * S.acc[t][0];
+                vel[Np + i] += pref * S.acc[t][1];
+                vel[2 * Np + i] += pref * S.acc[t][2];
+            }
+            if (PSI) {
+                psi[i] += pref * S.acc[t][3];
+                psi[Np + i] += pref * S.acc[t][4];
+                psi[2 * Np + i] += pref * S.acc[t][5];
+            }
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&counters[0], ninr);
+        atomicAdd(&counters[1], ncand);
     }
 }
 
@@ -456,6 +805,11 @@ int exclusive_scan(vpbs_handle* h, const int32_t* counts, int32_t* start, int64_
     return check_cuda(h, cudaGetLastError(), "scan kernel");
 }
 
+template <typename T>
+struct PrecTag {
+    using type = T;
+};
+
 int pair_interactions(vpbs_handle* h, int fields) {
     const int64_t Np = h->Np, Nq = h->Nq;
     const bool open = h->K.open_domain;
@@ -479,6 +833,36 @@ int pair_interactions(vpbs_handle* h, int fields) {
     StageScope st(h, ST_PAIRS);
     const unsigned grid = grid_for(Np, 8);
     const bool v = fields & VPBS_VELOCITY, p = fields & VPBS_STREAMFUNCTION;
+    const int Wc = 2 * h->cg.M + 1;
+    if (!open && h->cg.M > 0 && Wc * Wc * Wc * h->cg.G <= kMaxNbCells) {
+        const size_t smem = sizeof(TileSmem);
+        const unsigned ncells = (unsigned)(h->cg.ncell / h->cg.G);
+        auto launch_tiled = [&](auto kern) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            kern<<<ncells, kPairThreads, smem, h->stream>>>(
+                h->K, h->cg, Np, Nq, (const int32_t*)h->dst_start.p, (const int32_t*)h->dst_order.p,
+                (const double*)h->nodes.p, (const int32_t*)h->idx_prev.p, (const double*)h->src_sorted.p,
+                (const int32_t*)h->src_start.p, (const int32_t*)h->src_seg.p, (double*)h->vel.p, (double*)h->psi.p,
+                (unsigned long long*)h->counters.p);
+        };
+        auto by_fields = [&](auto skip, auto prec) {
+            constexpr bool SK = decltype(skip)::value;
+            using R = typename decltype(prec)::type;
+            if (v && p) launch_tiled(pair_cell_kernel<true, true, SK, R>);
+            else if (v) launch_tiled(pair_cell_kernel<true, false, SK, R>);
+            else launch_tiled(pair_cell_kernel<false, true, SK, R>);
+        };
+        const bool mixed = h->P.precision == VPBS_PRECISION_MIXED;
+        if (skip_local) {
+            if (mixed) by_fields(std::true_type{}, PrecTag<float>{});
+            else by_fields(std::true_type{}, PrecTag<double>{});
+        } else {
+            if (mixed) by_fields(std::false_type{}, PrecTag<float>{});
+            else by_fields(std::false_type{}, PrecTag<double>{});
+        }
+        h->launches++;
+        return check_cuda(h, cudaGetLastError(), "pair kernel");
+    }
     auto launch = [&](auto kern) {
         kern<<<grid, 256, 0, h->stream>>>(h->K, h->cg, Np, Nq, (const int32_t*)h->dst_order.p, (const double*)h->nodes.p,
                                           (const int32_t*)h->idx_prev.p, (const double*)h->src_sorted.p,

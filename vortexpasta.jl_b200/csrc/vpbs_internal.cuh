@@ -29,6 +29,7 @@ struct KParams {
     // piecewise Taylor tables of erfc(x) and erfc(x) + 2/sqrt(pi) x exp(-x^2), x = alpha r
     const double* ewald_tab;
     const float* ewald_tab_f;  // FP32 copy (first kEwaldNCf coefficients) for the mixed form
+    const double2* ewald_tab2; // interleaved (erfc, g) coefficient pairs, for both weights at once
     int ewald_ntab;       // number of intervals (0: no splitting, weights are 1)
 };
 
@@ -56,10 +57,13 @@ __device__ __forceinline__ void ewald_weights(const KParams& K, double x, double
     }
 }
 
-// Cell-list geometry.
+// Cell-list geometry.  Cells are r_cut / M wide in y and z (M = nsubdiv); in x each such
+// cell is further split into G slabs (nc[0] counts the slabs), so the candidate range of a
+// node in a row of cells can be trimmed to the slabs within r_cut.
 struct CellGrid {
     int nc[3];
     int M;
+    int G;
     int64_t ncell;
 };
 
