@@ -380,6 +380,17 @@ __device__ __forceinline__ double ewald_weight1(const KParams& K, double x, int 
 
 static_assert(sizeof(TileSmem) <= 113 * 1024, "two pair-kernel CTAs must fit in one SM's shared memory");
 
+// Largest row r in [0, n] whose first concatenated index off[r W] is <= T (off[0] = 0 <= T).
+__device__ __forceinline__ int last_row_le(const int32_t* off, int W, int n, int T) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid * W] <= T) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 // Distance from x to the cell [lo, lo + h], less a margin of 1e-9 h so that rounding in the
 // binning can never cull a source that is in range.
 __device__ __forceinline__ double box_gap(double x, double lo, double h) {
@@ -395,7 +406,7 @@ __device__ __forceinline__ double box_gap(double x, double lo, double h) {
 template <bool VEL, bool PSI, typename R>
 __device__ __forceinline__ void tile_eval2(const KParams& K, const double xd[3], const TileSmem& S,
                                            const double* __restrict__ src, int64_t Ns, int t0, bool v0, int t1,
-                                           bool v1, PairAcc<R>& acc, unsigned long long& ninr) {
+                                           bool v1, PairAcc<double>& acc, unsigned long long& ninr) {
     const int tt[2] = {t0, t1};
     const bool vv[2] = {v0, v1};
     double d[2][3], q[2][3], s2[2];
@@ -435,18 +446,19 @@ __device__ __forceinline__ void tile_eval2(const KParams& K, const double xd[3],
             else if (VEL) wg = ewald_weight1(K, xa, 1);
             else wa = ewald_weight1(K, xa, 0);
         }
+        // each pair's contribution is formed in R and accumulated in FP64
         const R q0 = (R)q[u][0], q1 = (R)q[u][1], q2 = (R)q[u][2];
         if (VEL) {
             const R f = wg * rinv * rinv * rinv;
-            acc_add<R>(acc.v[0], acc.cv[0], f * (q1 * r2 - q2 * r1));
-            acc_add<R>(acc.v[1], acc.cv[1], f * (q2 * r0 - q0 * r2));
-            acc_add<R>(acc.v[2], acc.cv[2], f * (q0 * r1 - q1 * r0));
+            acc.v[0] += (double)(f * (q1 * r2 - q2 * r1));
+            acc.v[1] += (double)(f * (q2 * r0 - q0 * r2));
+            acc.v[2] += (double)(f * (q0 * r1 - q1 * r0));
         }
         if (PSI) {
             const R f = wa * rinv;
-            acc_add<R>(acc.p[0], acc.cp[0], f * q0);
-            acc_add<R>(acc.p[1], acc.cp[1], f * q1);
-            acc_add<R>(acc.p[2], acc.cp[2], f * q2);
+            acc.p[0] += (double)(f * q0);
+            acc.p[1] += (double)(f * q1);
+            acc.p[2] += (double)(f * q2);
         }
     }
 }
@@ -457,7 +469,7 @@ __device__ __forceinline__ void tile_eval2(const KParams& K, const double xd[3],
 template <bool VEL, bool PSI, bool SKIP, typename R>
 __device__ __forceinline__ void tile_range_q(const KParams& K, const double xd[3], float3 xr, float rc2s, int i,
                                              int iprev, const TileSmem& S, const double* __restrict__ src, int64_t Ns,
-                                             int a, int b, int lane, PairAcc<R>& acc, int32_t* Q, int& qcount,
+                                             int a, int b, int lane, PairAcc<double>& acc, int32_t* Q, int& qcount,
                                              unsigned long long& ninr) {
     for (int base = a; base < b; base += 32) {
         const int t = base + lane;
@@ -549,8 +561,12 @@ __global__ void __launch_bounds__(kPairThreads, 2) pair_cell_kernel(
         }
         const int P = np >= kPairThreads / 32 ? 1 : (kPairThreads / 32) / np;  // row parts per destination
         const int nitems = np * P;
-        for (int T0 = 0; T0 < ntot; T0 += kTile) {
-            const int T1 = ntot - T0 < kTile ? ntot : T0 + kTile;
+        for (int T0 = 0, T1 = 0; T0 < ntot; T0 = T1) {
+            // tile [T0, T1): whole rows [ra, rb) while they fit, else a kTile piece of one row
+            const int ra = min(last_row_le(S.off, WX, nrow, T0), nrow - 1);
+            const int rf = last_row_le(S.off, WX, nrow, T0 + kTile);
+            T1 = S.off[rf * WX] > T0 ? S.off[rf * WX] : min(T0 + kTile, ntot);
+            const int rb = min(last_row_le(S.off, WX, nrow, T1 - 1) + 1, nrow);
             __syncthreads();  // previous tile consumed, destinations loaded
             for (int ci = warp; ci < ncb; ci += kPairThreads / 32) {
                 const int o = S.off[ci];
@@ -578,7 +594,7 @@ __global__ void __launch_bounds__(kPairThreads, 2) pair_cell_kernel(
                 const int dl = it % np, part = it / np;
                 const double x[3] = {S.dx[dl][0], S.dx[dl][1], S.dx[dl][2]};
                 // candidate range of every row, trimmed to the slabs within r_cut of the node
-                for (int r = lane; r < nrow; r += 32) {
+                for (int r = ra + lane; r < rb; r += 32) {
                     const double gy = box_gap(x[1], (c1 + r % W - M) * h1, h1);
                     const double gz = box_gap(x[2], (c2 + r / W - M) * h2, h2);
                     const double gyz = gy * gy + gz * gz;
@@ -597,13 +613,13 @@ __global__ void __launch_bounds__(kPairThreads, 2) pair_cell_kernel(
                     S.rng[warp][r] = make_int2(a, b);
                 }
                 __syncwarp();
-                PairAcc<R> acc = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0ull, 0ull};
+                PairAcc<double> acc = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, 0ull, 0ull};
                 int qcount = 0;
                 int32_t* Q = S.queue[warp];
                 const double xd[3] = {x[0] - o0, x[1] - o1, x[2] - o2};
                 const float3 xr = make_float3((float)xd[0], (float)xd[1], (float)xd[2]);
                 const int i = S.di[dl], iprev = S.dprev[dl];
-                for (int r = part; r < nrow; r += P) {
+                for (int r = ra + part; r < rb; r += P) {
                     const int2 ab = S.rng[warp][r];
                     const int a = ab.x > T0 ? ab.x : T0, b = ab.y < T1 ? ab.y : T1;
                     if (a < b) {
@@ -612,16 +628,16 @@ __global__ void __launch_bounds__(kPairThreads, 2) pair_cell_kernel(
                                                         qcount, ninr);
                     }
                 }
-                tile_eval2<VEL, PSI, R>(K, xd, S, src, Ns, lane < qcount ? Q[lane] : 0, lane < qcount,
-                                        32 + lane < qcount ? Q[32 + lane] : 0, 32 + lane < qcount, acc, ninr);
-                auto lane_total = [](R s, R c) { return (double)s - (double)c; };
+                if (qcount > 0)  // warp-uniform
+                    tile_eval2<VEL, PSI, R>(K, xd, S, src, Ns, lane < qcount ? Q[lane] : 0, lane < qcount,
+                                            32 + lane < qcount ? Q[32 + lane] : 0, 32 + lane < qcount, acc, ninr);
                 double s[6] = {0, 0, 0, 0, 0, 0};
                 if (VEL)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) s[c] = warp_sum(lane_total(acc.v[c], acc.cv[c]));
+                    for (int c = 0; c < 3; ++c) s[c] = warp_sum(acc.v[c]);
                 if (PSI)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) s[3 + c] = warp_sum(lane_total(acc.p[c], acc.cp[c]));
+                    for (int c = 0; c < 3; ++c) s[3 + c] = warp_sum(acc.p[c]);
                 if (lane == 0) {
                     if (VEL)
                         for (int c = 0; c < 3; ++c) atomicAdd(&S.acc[dl][c], s[c]);
