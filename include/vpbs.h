@@ -209,6 +209,39 @@ int vpbs_ewald_table_eval(double xmax, const double* x, int64_t n, double* erfc_
  * reference. */
 int vpbs_fma_throughput(int32_t device, int32_t fp64, double* tflops);
 
+/* ---- Learned parameter predictor (no counterpart in the reference, which removed its alpha
+ * autotuner; the fallback is the default rule of splitting/gaussian.jl:133-200). ---- */
+
+/* Features of the configuration loaded in `h` (after vpbs_set_filaments / vpbs_set_points; needs
+ * a periodic domain with cell lists): log10 N, log10(line length / L^2), log10(mean and min
+ * segment chord / L), and a 12-bin histogram over log10(d / L) in [-3, 0) of the distance d from
+ * sampled nodes to their nearest non-local quadrature point (searched within r_cut).  Synchronous. */
+#define VPBS_NUM_FEATURES 16
+int vpbs_features(vpbs_handle* h, float* out, int32_t n);
+
+/* The predictor network: VPBS_MLP_IN -> VPBS_MLP_HIDDEN -> VPBS_MLP_HIDDEN -> VPBS_MLP_OUT, GELU
+ * hidden activations, FP32.  Parameters are one flat array [W1 (H x IN, row-major), b1, W2 (H x H),
+ * b2, W3 (OUT x H), b3].  Inputs X are row-major [n][IN], targets and outputs [n][OUT].  The loss
+ * is sum_o w_o (y_o - t_o)^2 averaged over the batch (w: vpbs_mlp_set_loss_weights, default 1).
+ * vpbs_mlp_train_step runs forward, backward and one Adam step (beta1 0.9, beta2 0.999, eps 1e-8)
+ * on the device; vpbs_mlp_gradient returns the loss and its gradient without updating.  n must not
+ * exceed the max_batch given at creation.  Errors: vpbs_mlp_last_error. */
+#define VPBS_MLP_IN 16
+#define VPBS_MLP_HIDDEN 64
+#define VPBS_MLP_OUT 5
+#define VPBS_MLP_NPARAMS (VPBS_MLP_HIDDEN * VPBS_MLP_IN + VPBS_MLP_HIDDEN + VPBS_MLP_HIDDEN * VPBS_MLP_HIDDEN + \
+                          VPBS_MLP_HIDDEN + VPBS_MLP_OUT * VPBS_MLP_HIDDEN + VPBS_MLP_OUT)
+typedef struct vpbs_mlp vpbs_mlp;
+int vpbs_mlp_create(int32_t device, int32_t max_batch, vpbs_mlp** out);
+int vpbs_mlp_destroy(vpbs_mlp* m);
+const char* vpbs_mlp_last_error(const vpbs_mlp* m);
+int vpbs_mlp_set_params(vpbs_mlp* m, const float* params, int64_t n);
+int vpbs_mlp_get_params(vpbs_mlp* m, float* params, int64_t n);
+int vpbs_mlp_set_loss_weights(vpbs_mlp* m, const float* w);
+int vpbs_mlp_forward(vpbs_mlp* m, const float* X, int32_t n, float* Y);
+int vpbs_mlp_gradient(vpbs_mlp* m, const float* X, const float* T, int32_t n, float* grad, float* loss);
+int vpbs_mlp_train_step(vpbs_mlp* m, const float* X, const float* T, int32_t n, float lr, float* loss);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,123 @@
+"""Learned parameter predictor: the default rule, grid rounding, the network against its CPU
+oracle (forward, gradient, training) and the configuration features against theirs."""
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import load_package
+from oracle import features_ref, mlp_ref
+
+vp = load_package()
+from vortexpasta_b200 import _lib, configs, learned, tuning  # noqa: E402
+
+L = 2 * math.pi
+
+
+def test_default_rule_matches_reference_formulas():
+    # gaussian.jl:175-186 with rtol = 1e-5 and r_cut = L/16
+    ch = tuning.default_rule(L, 1e-5, L / 16)
+    beta = math.sqrt(-math.log(1e-5 / 10 ** (-1.3)))
+    assert ch.alpha == pytest.approx(beta / (L / 16), rel=1e-14)
+    assert ch.Ns == 2 * math.ceil(2 * ch.alpha * beta * L / (2 * math.pi)) + 2
+    assert (ch.sigma, ch.m) == (1.5, 4)
+
+
+@pytest.mark.parametrize("Ns_min,sigma,m", [(90, 1.5, 4), (38, 1.25, 3), (161, 2.0, 3), (500, 1.25, 5), (9, 1.5, 2)])
+def test_grid_rounding(Ns_min, sigma, m):
+    Ns = tuning.grid_for(Ns_min, sigma, m)
+    n = tuning.fft_size(Ns, sigma)
+    assert Ns >= Ns_min
+    assert n % tuning.FFT_MULTIPLE == 0 and n >= 2 * m
+    assert tuning.fft_size(Ns + 1, sigma) > n  # no larger Ns with the same FFT
+
+
+def test_choice_of_outputs_is_valid():
+    y = learned.targets_of(tuning.choice_from(L, L / 24, 3.0, 3.1, 1.5, 3), L)
+    ch = learned.choice_of(y, L)
+    assert ch.rcut == pytest.approx(L / 24)
+    assert (ch.sigma, ch.m) == (1.5, 3)
+    ch2 = learned.choice_of(np.array([math.log(10.0), 2.0, 7.3, 1.9, 9.6]), L)
+    assert ch2.rcut <= 0.35 * L and ch2.m == 8 and ch2.sigma == 2.0
+    p = ch2.params(L)  # constructible (passes the reference's cut-off checks)
+    assert p.precision == "mixed"
+
+
+def test_mlp_oracle_gradient_finite_differences():
+    p = learned.init_params(3).astype(np.float64)
+    rng = np.random.default_rng(0)
+    X, T = rng.normal(size=(9, 16)), rng.normal(size=(9, 5))
+    _, g = mlp_ref.loss_and_grad(p, X, T)
+    eps = 1e-6
+    for i in rng.choice(p.size, 40, replace=False):
+        a, b = p.copy(), p.copy()
+        a[i] += eps
+        b[i] -= eps
+        fd = (mlp_ref.loss_and_grad(a, X, T)[0] - mlp_ref.loss_and_grad(b, X, T)[0]) / (2 * eps)
+        assert fd == pytest.approx(g[i], rel=1e-5, abs=1e-9)
+
+
+def test_predictor_roundtrip(tmp_path):
+    pr = learned.Predictor(params=learned.init_params(1), x_mean=np.zeros(16), x_std=np.ones(16),
+                           y_mean=np.zeros(5), y_std=np.ones(5), rtol=1e-5)
+    pr.save(tmp_path / "p.npz")
+    q = learned.Predictor.load(tmp_path / "p.npz")
+    assert np.array_equal(q.params, pr.params) and q.rtol == 1e-5
+
+
+# ---------------- GPU ----------------
+
+@pytest.mark.gpu
+def test_mlp_forward_and_gradient_match_oracle():
+    rng = np.random.default_rng(5)
+    p = learned.init_params(7)
+    X = rng.normal(size=(37, 16)).astype(np.float32)
+    T = rng.normal(size=(37, 5)).astype(np.float32)
+    net = learned.MLP(max_batch=64, params=p)
+    try:
+        Y = net.forward(X)
+        Yr, _ = mlp_ref.forward(p, X)
+        assert np.abs(Y - Yr).max() <= 1e-5 * np.abs(Yr).max()
+        loss, g = net.gradient(X, T)
+        lr, gr = mlp_ref.loss_and_grad(p, X, T)
+        assert loss == pytest.approx(lr, rel=1e-5)
+        assert np.linalg.norm(g - gr) <= 1e-5 * np.linalg.norm(gr)
+    finally:
+        net.close()
+
+
+@pytest.mark.gpu
+def test_mlp_training_fits_a_smooth_map():
+    rng = np.random.default_rng(2)
+    X = rng.normal(size=(256, 16)).astype(np.float32)
+    W = rng.normal(size=(16, 5)) / 4
+    T = np.tanh(X @ W).astype(np.float32)
+    net = learned.MLP(max_batch=256, seed=1)
+    try:
+        first = net.train_step(X, T, 3e-3)
+        for _ in range(600):
+            last = net.train_step(X, T, 3e-3)
+        assert last < 0.05 * first
+        # the parameters the device holds give the loss the oracle computes
+        lr, _ = mlp_ref.loss_and_grad(net.get_params(), X, T)
+        loss, _ = net.gradient(X, T)
+        assert loss == pytest.approx(lr, rel=1e-4)
+    finally:
+        net.close()
+
+
+@pytest.mark.gpu
+def test_features_match_oracle():
+    fs = configs.tangle(12, 40, seed=3)
+    c = vp.init_cache(learned.feature_params(L))
+    try:
+        c.set_filaments(fs)
+        f = c.features()
+        pd = c.pointdata()
+    finally:
+        c.close()
+    ref = features_ref.features(pd["nodes"], pd["idx_prev"], pd["points"], 3, L, L * learned.FEATURE_RCUT)
+    assert np.allclose(f[:4], ref[:4], rtol=1e-5, atol=1e-6)
+    assert np.allclose(f[4:], ref[4:], atol=1.5 / len(pd["nodes"]))  # at most one node on a bin edge
+    assert f[4:].sum() == pytest.approx(1.0, abs=1e-6)

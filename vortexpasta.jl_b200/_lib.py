@@ -19,6 +19,7 @@ PRECISION = {"fp64": 0, "mixed": 1}
 c_double_p = ct.POINTER(ct.c_double)
 c_int32_p = ct.POINTER(ct.c_int32)
 c_int64_p = ct.POINTER(ct.c_int64)
+c_float_p = ct.POINTER(ct.c_float)
 
 
 class VpbsParams(ct.Structure):
@@ -65,7 +66,21 @@ SIGNATURES = {
     "vpbs_point_data_noalloc": (ct.c_int, [ct.POINTER(VpbsParams), ct.c_int64, c_int64_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "vpbs_features": (ct.c_int, [ct.c_void_p, c_float_p, ct.c_int32]),
+    "vpbs_mlp_create": (ct.c_int, [ct.c_int32, ct.c_int32, ct.POINTER(ct.c_void_p)]),
+    "vpbs_mlp_destroy": (ct.c_int, [ct.c_void_p]),
+    "vpbs_mlp_last_error": (ct.c_char_p, [ct.c_void_p]),
+    "vpbs_mlp_set_params": (ct.c_int, [ct.c_void_p, c_float_p, ct.c_int64]),
+    "vpbs_mlp_get_params": (ct.c_int, [ct.c_void_p, c_float_p, ct.c_int64]),
+    "vpbs_mlp_set_loss_weights": (ct.c_int, [ct.c_void_p, c_float_p]),
+    "vpbs_mlp_forward": (ct.c_int, [ct.c_void_p, c_float_p, ct.c_int32, c_float_p]),
+    "vpbs_mlp_gradient": (ct.c_int, [ct.c_void_p, c_float_p, c_float_p, ct.c_int32, c_float_p, c_float_p]),
+    "vpbs_mlp_train_step": (ct.c_int, [ct.c_void_p, c_float_p, c_float_p, ct.c_int32, ct.c_float, c_float_p]),
 }
+
+NUM_FEATURES = 16
+MLP_IN, MLP_HIDDEN, MLP_OUT = 16, 64, 5
+MLP_NPARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_OUT * MLP_HIDDEN + MLP_OUT
 
 NUM_STAGES = 9
 
@@ -104,3 +119,8 @@ def check(rc: int, handle=None, what: str = ""):
 def dptr(a):
     """ctypes double* of a contiguous float64 numpy array."""
     return a.ctypes.data_as(c_double_p)
+
+
+def fptr(a):
+    """ctypes float* of a contiguous float32 numpy array."""
+    return a.ctypes.data_as(c_float_p)

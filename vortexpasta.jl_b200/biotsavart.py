@@ -135,6 +135,13 @@ class BiotSavartCache:
                    self._h, "device_field")
         return x.value, y.value, z.value
 
+    def features(self) -> np.ndarray:
+        """Configuration features of the loaded filaments (vpbs_features): the inputs of the
+        learned parameter predictor."""
+        out = np.zeros(_lib.NUM_FEATURES, dtype=np.float32)
+        _lib.check(self._lib.vpbs_features(self._h, _lib.fptr(out), _lib.NUM_FEATURES), self._h, "features")
+        return out
+
     def pair_counts(self):
         a, b = ct.c_int64(), ct.c_int64()
         _lib.check(self._lib.vpbs_pair_counts(self._h, ct.byref(a), ct.byref(b)), self._h, "pair_counts")

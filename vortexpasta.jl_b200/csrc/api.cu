@@ -258,7 +258,7 @@ int vpbs_destroy(vpbs_handle* h) {
                       &h->src_seg, &h->dst_cell, &h->dst_start, &h->dst_fill, &h->dst_order, &h->counters,
                       &h->grid_r, &h->grid_c, &h->grid_c2, &h->uhat, &h->decx, &h->decy, &h->decz, &h->nodes_lr,
                       &h->vel, &h->psi, &h->spread_bin, &h->spread_counts, &h->spread_start, &h->binned,
-                      &h->spread_foot, &h->ewald_tab};
+                      &h->spread_foot, &h->ewald_tab, &h->scan_tmp, &h->scan_tmp_lr};
     for (DevBuf* b : bufs) free_buf(*b);
     if (h->pin_in) cudaFreeHost(h->pin_in);
     if (h->pin_out) cudaFreeHost(h->pin_out);

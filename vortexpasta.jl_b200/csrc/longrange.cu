@@ -640,7 +640,7 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
         spread_bin_count_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(S, B, nb0, nb1, nb2, Nq, src, sx[0], sx[1],
                                                                            sx[2], bin, rank, counts);
         h->launches++;
-        if ((rc = exclusive_scan(h, counts, start, nbins))) return rc;
+        if ((rc = exclusive_scan(h, counts, start, nbins, h->scan_tmp_lr))) return rc;
         spread_bin_scatter_kernel<T><<<grid_for(Nq, 128), 128, 0, h->stream>>>(S, Nq, src, sx[0], sx[1], sx[2], bin,
                                                                                 rank, start, (T*)h->binned.p, foot);
         h->launches++;

@@ -72,6 +72,66 @@ __global__ void __launch_bounds__(1024) scan_kernel(const int32_t* __restrict__ 
     if (tid == 1023) start[n] = part[1023];
 }
 
+// Multi-CTA exclusive scan for long count arrays: per-chunk sums, a scan of the sums (with
+// scan_kernel), then every chunk scanned in shared memory from its offset.
+constexpr int kScanThreads = 1024, kScanPer = 4, kScanChunk = kScanThreads * kScanPer;
+
+__device__ __forceinline__ int warp_incl_scan(int x, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    return x;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_partials_kernel(const int32_t* __restrict__ counts, int64_t n,
+                                                                    int32_t* __restrict__ part) {
+    __shared__ int wt[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t base = (int64_t)blockIdx.x * kScanChunk + (int64_t)threadIdx.x * kScanPer;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k)
+        if (base + k < n) s += counts[base + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) wt[warp] = s;
+    __syncthreads();
+    if (warp == 0) {
+        int v = wt[lane];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) part[blockIdx.x] = v;
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_chunks_kernel(const int32_t* __restrict__ counts, int64_t n,
+                                                                  const int32_t* __restrict__ part_start,
+                                                                  int32_t* __restrict__ start) {
+    __shared__ int wt[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t base = (int64_t)blockIdx.x * kScanChunk + (int64_t)threadIdx.x * kScanPer;
+    int c[kScanPer], s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        c[k] = base + k < n ? counts[base + k] : 0;
+        s += c[k];
+    }
+    const int x = warp_incl_scan(s, lane);
+    if (lane == 31) wt[warp] = x;
+    __syncthreads();
+    if (warp == 0) wt[lane] = warp_incl_scan(wt[lane], lane);
+    __syncthreads();
+    int acc = part_start[blockIdx.x] + (warp > 0 ? wt[warp - 1] : 0) + x - s;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        if (base + k < n) start[base + k] = acc;
+        acc += c[k];
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) start[n] = part_start[gridDim.x];
+}
+
 // Scatter the sources into cell order (SoA: x, y, z, qx, qy, qz) and record their segment.
 __global__ void scatter_sources_kernel(int64_t Nq, int nquad, const double* __restrict__ points,
                                        const double* __restrict__ charges, const int32_t* __restrict__ cell,
@@ -316,10 +376,11 @@ __global__ void __launch_bounds__(256) pair_kernel(
 // dependency chains overlap.  Destinations are handled in passes of up to kPassDst nodes;
 // warps take (destination, row-part) items and add each item's warp-reduced sum to the
 // destination's shared-memory accumulator.
-constexpr int kTile = 2816;
+constexpr int kTile = 2560;
 constexpr int kTilePad = kTile + 32;  // a chunk of 32 lanes may read past the tile end (masked)
 constexpr int kPassDst = 64;
-constexpr int kMaxNbCells = 729;  // neighbour slabs: (2M+1)^2 rows x (2M+1) G slabs
+constexpr int kMaxNbCells = 2048;  // neighbour slabs of a block: rows x slabs per row
+constexpr int kMaxBlockRows = 16;  // (y, z) cell rows of a block (destination ranges)
 constexpr int kMaxRows = 81;      // (2M+1)^2
 constexpr int kTileQueue = 128;   // screened pairs are evaluated 64 at a time (two per lane)
 constexpr double kScreenMargin = 2e-5;
@@ -333,6 +394,7 @@ struct TileSmem {
     double acc[kPassDst][6];  // per destination: velocity, streamfunction
     double dx[kPassDst][3];   // destination positions
     int32_t di[kPassDst], dprev[kPassDst];
+    int32_t dr_start[kMaxBlockRows], dr_base[kMaxBlockRows + 1];  // destination ranges of the block
     int32_t off[kMaxNbCells + 1];  // concatenated offsets of the neighbour slabs
     int32_t cstart[kMaxNbCells];   // first cell-sorted source of each neighbour slab
     int2 rng[kPairThreads / 32][kMaxRows];  // per warp: candidate range of every row
@@ -499,26 +561,46 @@ __global__ void __launch_bounds__(kPairThreads, 2) pair_cell_kernel(
     KParams K, CellGrid cg, int64_t Np, int64_t Ns, const int32_t* __restrict__ dst_start,
     const int32_t* __restrict__ dst_order, const double* __restrict__ nodes, const int32_t* __restrict__ idx_prev,
     const double* __restrict__ src, const int32_t* __restrict__ src_start, const int32_t* __restrict__ seg,
-    double* __restrict__ vel, double* __restrict__ psi, unsigned long long* __restrict__ counters) {
+    double* __restrict__ vel, double* __restrict__ psi, unsigned long long* __restrict__ counters, int3 bk,
+    int3 nb) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TileSmem& S = *reinterpret_cast<TileSmem*>(smem_raw);
-    const int M = cg.M, G = cg.G, W = 2 * M + 1, WX = W * G, nrow = W * W, ncb = nrow * WX;
+    const int M = cg.M, G = cg.G;
     const int nc0 = cg.nc[0], nc1 = cg.nc[1], nc2 = cg.nc[2];
     const int ncc = nc0 / G;  // cells in x (each made of G slabs)
-    const int64_t cell = blockIdx.x;
-    const int c0 = (int)(cell % ncc), c1 = (int)((cell / ncc) % nc1), c2 = (int)(cell / ((int64_t)ncc * nc1));
-    const int64_t slab0 = ((int64_t)c2 * nc1 + c1) * nc0 + (int64_t)c0 * G;
-    const int d0 = dst_start[slab0], nd = dst_start[slab0 + G] - d0;
-    if (nd == 0) return;
+    // this CTA's block of cells [cx0, cx1) x [cy0, cy1) x [cz0, cz1)
+    const int bxi = blockIdx.x % nb.x, byi = (blockIdx.x / nb.x) % nb.y, bzi = blockIdx.x / (nb.x * nb.y);
+    const int cx0 = bxi * bk.x, cx1 = min(cx0 + bk.x, ncc);
+    const int cy0 = byi * bk.y, cy1 = min(cy0 + bk.y, nc1);
+    const int cz0 = bzi * bk.z, cz1 = min(cz0 + bk.z, nc2);
+    const int ndr = (cy1 - cy0) * (cz1 - cz0);  // destination ranges: one per (y, z) cell row
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int k = 0; k < ndr; ++k) {
+            const int yy = cy0 + k % (cy1 - cy0), zz = cz0 + k / (cy1 - cy0);
+            const int64_t s0 = ((int64_t)zz * nc1 + yy) * nc0 + (int64_t)cx0 * G;
+            const int a = dst_start[s0], b = dst_start[s0 + (int64_t)(cx1 - cx0) * G];
+            S.dr_start[k] = a;
+            S.dr_base[k] = acc;
+            acc += b - a;
+        }
+        S.dr_base[ndr] = acc;
+    }
+    __syncthreads();
+    const int nd = S.dr_base[ndr];
+    if (nd == 0) return;  // uniform over the CTA
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const double hx = K.L[0] / nc0, h1 = K.L[1] / nc1, h2 = K.L[2] / nc2, inv_hx = nc0 / K.L[0];
-    const int xs0 = c0 * G - M * G;  // first neighbour slab in x (unwrapped index)
-    const double o0 = c0 * G * hx, o1 = c1 * h1, o2 = c2 * h2;  // cell corner: origin of the FP32 coordinates
+    // neighbourhood: rows (y, z) of the block widened by M cells, slabs in x widened by M G
+    const int WY = cy1 - cy0 + 2 * M, WZ = cz1 - cz0 + 2 * M, WX = (cx1 - cx0 + 2 * M) * G;
+    const int nrow = WY * WZ, ncb = nrow * WX;
+    const int ry0 = cy0 - M, rz0 = cz0 - M, xs0 = cx0 * G - M * G;  // unwrapped first row / slab
+    const double o0 = cx0 * G * hx, o1 = cy0 * h1, o2 = cz0 * h2;  // block corner: origin of the FP32 coordinates
     const float rc2s = (float)(K.rcut2 * (1.0 + kScreenMargin));
     // neighbour slabs in (row, slab) order: first cell-sorted source and count
     for (int ci = threadIdx.x; ci < ncb; ci += kPairThreads) {
         const int r = ci / WX, k = ci % WX;
-        int xx = xs0 + k, yy = c1 + r % W - M, zz = c2 + r / W - M;
+        int xx = xs0 + k, yy = ry0 + r % WY, zz = rz0 + r / WY;
         xx = xx < 0 ? xx + nc0 : (xx >= nc0 ? xx - nc0 : xx);
         yy = yy < 0 ? yy + nc1 : (yy >= nc1 ? yy - nc1 : yy);
         zz = zz < 0 ? zz + nc2 : (zz >= nc2 ? zz - nc2 : zz);
@@ -551,7 +633,10 @@ __global__ void __launch_bounds__(kPairThreads, 2) pair_cell_kernel(
         const int np = nd - p0 < kPassDst ? nd - p0 : kPassDst;
         __syncthreads();  // the previous pass has written its results
         for (int t = threadIdx.x; t < np; t += kPairThreads) {
-            const int i = dst_order[d0 + p0 + t];
+            const int tt = p0 + t;
+            int k = 0;
+            while (k + 1 < ndr && S.dr_base[k + 1] <= tt) ++k;
+            const int i = dst_order[S.dr_start[k] + tt - S.dr_base[k]];
             S.di[t] = i;
             S.dprev[t] = idx_prev[i];
 #pragma unroll
@@ -574,7 +659,7 @@ __global__ void __launch_bounds__(kPairThreads, 2) pair_cell_kernel(
                 if (a >= b) continue;
                 // periodic image of this slab next to the destination cell
                 const int r = ci / WX, k = ci % WX;
-                const int xu = xs0 + k, yu = c1 + r % W - M, zu = c2 + r / W - M;
+                const int xu = xs0 + k, yu = ry0 + r % WY, zu = rz0 + r / WY;
                 const double sx = xu < 0 ? -K.L[0] : (xu >= nc0 ? K.L[0] : 0.0);
                 const double sy = yu < 0 ? -K.L[1] : (yu >= nc1 ? K.L[1] : 0.0);
                 const double sz = zu < 0 ? -K.L[2] : (zu >= nc2 ? K.L[2] : 0.0);
@@ -595,8 +680,8 @@ __global__ void __launch_bounds__(kPairThreads, 2) pair_cell_kernel(
                 const double x[3] = {S.dx[dl][0], S.dx[dl][1], S.dx[dl][2]};
                 // candidate range of every row, trimmed to the slabs within r_cut of the node
                 for (int r = ra + lane; r < rb; r += 32) {
-                    const double gy = box_gap(x[1], (c1 + r % W - M) * h1, h1);
-                    const double gz = box_gap(x[2], (c2 + r / W - M) * h2, h2);
+                    const double gy = box_gap(x[1], (ry0 + r % WY) * h1, h1);
+                    const double gz = box_gap(x[2], (rz0 + r / WY) * h2, h2);
                     const double gyz = gy * gy + gz * gz;
                     int a = 0, b = 0;
                     if (gyz <= K.rcut2) {
@@ -773,14 +858,14 @@ int build_cell_lists(vpbs_handle* h) {
                                                                 (int32_t*)h->src_fill.p);
     cell_count_kernel<<<grid_for(Np, 256), 256, 0, h->stream>>>(h->K, h->cg, Np, (const double*)h->nodes.p, dcell, drank,
                                                                 (int32_t*)h->dst_fill.p);
-    scan_kernel<<<1, 1024, 0, h->stream>>>((const int32_t*)h->src_fill.p, (int32_t*)h->src_start.p, ncell);
-    scan_kernel<<<1, 1024, 0, h->stream>>>((const int32_t*)h->dst_fill.p, (int32_t*)h->dst_start.p, ncell);
+    if ((rc = exclusive_scan(h, (const int32_t*)h->src_fill.p, (int32_t*)h->src_start.p, ncell, h->scan_tmp))) return rc;
+    if ((rc = exclusive_scan(h, (const int32_t*)h->dst_fill.p, (int32_t*)h->dst_start.p, ncell, h->scan_tmp))) return rc;
     scatter_sources_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(
         Nq, h->K.nquad, (const double*)h->points.p, (const double*)h->charges.p, scell, srank,
         (const int32_t*)h->src_start.p, (double*)h->src_sorted.p, (int32_t*)h->src_seg.p);
     scatter_nodes_kernel<<<grid_for(Np, 256), 256, 0, h->stream>>>(Np, dcell, drank, (const int32_t*)h->dst_start.p,
                                                                    (int32_t*)h->dst_order.p);
-    h->launches += 6;
+    h->launches += 4;  // plus the scans, counted by exclusive_scan
     return check_cuda(h, cudaGetLastError(), "cell list kernels");
 }
 
@@ -815,10 +900,22 @@ void ewald_table_host(double xmax, int* ntab, double* tab) {
     }
 }
 
-int exclusive_scan(vpbs_handle* h, const int32_t* counts, int32_t* start, int64_t n) {
-    scan_kernel<<<1, 1024, 0, h->stream>>>(counts, start, n);
-    h->launches++;
-    return check_cuda(h, cudaGetLastError(), "scan kernel");
+int exclusive_scan(vpbs_handle* h, const int32_t* counts, int32_t* start, int64_t n, DevBuf& tmp) {
+    const int64_t nblk = (n + kScanChunk - 1) / kScanChunk;
+    if (nblk <= 1) {
+        scan_kernel<<<1, 1024, 0, h->stream>>>(counts, start, n);
+        h->launches++;
+        return check_cuda(h, cudaGetLastError(), "scan kernel");
+    }
+    int rc;
+    if ((rc = ensure(h, tmp, sizeof(int32_t) * (2 * nblk + 1), "scan partial sums"))) return rc;
+    int32_t* part = (int32_t*)tmp.p;
+    int32_t* part_start = part + nblk;
+    scan_partials_kernel<<<(unsigned)nblk, kScanThreads, 0, h->stream>>>(counts, n, part);
+    scan_kernel<<<1, 1024, 0, h->stream>>>(part, part_start, nblk);
+    scan_chunks_kernel<<<(unsigned)nblk, kScanThreads, 0, h->stream>>>(counts, n, part_start, start);
+    h->launches += 3;
+    return check_cuda(h, cudaGetLastError(), "scan kernels");
 }
 
 template <typename T>
@@ -849,17 +946,37 @@ int pair_interactions(vpbs_handle* h, int fields) {
     StageScope st(h, ST_PAIRS);
     const unsigned grid = grid_for(Np, 8);
     const bool v = fields & VPBS_VELOCITY, p = fields & VPBS_STREAMFUNCTION;
-    const int Wc = 2 * h->cg.M + 1;
-    if (!open && h->cg.M > 0 && Wc * Wc * Wc * h->cg.G <= kMaxNbCells) {
+    const CellGrid& cg = h->cg;
+    const int Wc = 2 * cg.M + 1;
+    if (!open && cg.M > 0 && Wc * Wc <= kMaxRows && Wc * Wc * Wc * cg.G <= kMaxNbCells) {
+        // blocks of Bc^3 cells per CTA, grown while a block holds fewer than ~24 nodes on average,
+        // at least 16 CTAs per SM remain, and the neighbourhood fits the shared-memory tables and
+        // stays inside one period
+        const int ncc = cg.nc[0] / cg.G;
+        const double ncoarse = (double)ncc * cg.nc[1] * cg.nc[2];
+        const double per_cell = (double)Np / ncoarse;
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+        int Bc = 1;
+        while (Bc * Bc * Bc * per_cell < 24.0) {
+            const int nb = Bc + 1, w = nb + 2 * cg.M;
+            const bool fits = w <= ncc && w <= cg.nc[1] && w <= cg.nc[2] && w * w <= kMaxRows &&
+                              w * w * w * cg.G <= kMaxNbCells && nb * nb <= kMaxBlockRows &&
+                              ncoarse / ((double)nb * nb * nb) >= 16.0 * nsm;
+            if (!fits) break;
+            Bc = nb;
+        }
+        const int3 bk = make_int3(Bc, Bc, Bc);
+        const int3 nb = make_int3((ncc + Bc - 1) / Bc, (cg.nc[1] + Bc - 1) / Bc, (cg.nc[2] + Bc - 1) / Bc);
         const size_t smem = sizeof(TileSmem);
-        const unsigned ncells = (unsigned)(h->cg.ncell / h->cg.G);
+        const unsigned nblocks = (unsigned)((int64_t)nb.x * nb.y * nb.z);
         auto launch_tiled = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            kern<<<ncells, kPairThreads, smem, h->stream>>>(
+            kern<<<nblocks, kPairThreads, smem, h->stream>>>(
                 h->K, h->cg, Np, Nq, (const int32_t*)h->dst_start.p, (const int32_t*)h->dst_order.p,
                 (const double*)h->nodes.p, (const int32_t*)h->idx_prev.p, (const double*)h->src_sorted.p,
                 (const int32_t*)h->src_start.p, (const int32_t*)h->src_seg.p, (double*)h->vel.p, (double*)h->psi.p,
-                (unsigned long long*)h->counters.p);
+                (unsigned long long*)h->counters.p, bk, nb);
         };
         auto by_fields = [&](auto skip, auto prec) {
             constexpr bool SK = decltype(skip)::value;

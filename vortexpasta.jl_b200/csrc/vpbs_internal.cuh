@@ -112,6 +112,7 @@ struct vpbs_handle {
     vpbs::CellGrid cg{};
     vpbs::DevBuf src_cell, src_start, src_fill, src_sorted, src_seg, dst_cell, dst_start, dst_fill, dst_order;
     vpbs::DevBuf counters;  // [0] in-range pairs, [1] candidates (unsigned long long)
+    vpbs::DevBuf scan_tmp, scan_tmp_lr;  // multi-CTA scan scratch (cell lists; spreading bins)
     vpbs::DevBuf ewald_tab;  // Taylor tables of the Ewald weights (KParams::ewald_tab)
 
     // long range
@@ -162,7 +163,8 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
 
 // shortrange.cu
 int build_cell_lists(vpbs_handle* h);
-int exclusive_scan(vpbs_handle* h, const int32_t* counts, int32_t* start, int64_t n);  // start[0..n]
+int exclusive_scan(vpbs_handle* h, const int32_t* counts, int32_t* start, int64_t n,
+                   DevBuf& tmp);  // start[0..n]; tmp: scratch of the multi-CTA scan
 int local_and_self(vpbs_handle* h, int fields, int lia_mode, int with_pairs_self, double integration_cutoff);
 int pair_interactions(vpbs_handle* h, int fields);
 int add_local_integrals(vpbs_handle* h, int fields);

@@ -1,0 +1,286 @@
+"""Learned Ewald/NUFFT parameter predictor.
+
+A 16 -> 64 -> 64 -> 5 GELU perceptron (hand-written CUDA forward, backward and Adam kernels in
+csrc/mlp.cu, reached through the C ABI) maps cheap configuration features (csrc/features.cu) to
+the parameters of the cheapest evaluation that met the accuracy target in the library's own
+sweeps (tuning.sweep against an FP64 reference):
+
+    outputs = (log alpha L, r_cut / L, log2 Ns, sigma, m)   (standardised for training)
+
+``predict_choice`` turns the outputs into a valid ``EwaldChoice`` (sigma snapped to the
+allowed set, m rounded, the grid rounded up to a brick-friendly FFT size) and
+``choose_parameters`` checks the prediction against a plain FP64 evaluation and falls back to
+the reference's default rule (tuning.default_rule) when the target is missed.  The reference
+has no counterpart (it removed its alpha autotuner).
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+import math
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib, configs, curves, tuning
+
+DATA_DIR = Path(__file__).resolve().parent / "data"
+DEFAULT_MODEL = DATA_DIR / "predictor.npz"
+FEATURE_RCUT = 1.0 / 16  # r_cut / L of the cell lists the feature search runs on
+
+
+class MLP:
+    """The predictor network on the GPU (vpbs_mlp_*)."""
+
+    def __init__(self, max_batch: int = 1024, device: int = 0, params: np.ndarray | None = None, seed: int = 0):
+        self._lib = _lib.load()
+        h = ct.c_void_p()
+        rc = self._lib.vpbs_mlp_create(int(device), int(max_batch), ct.byref(h))
+        if rc != 0:
+            raise _lib.VpbsError(f"vpbs_mlp_create failed ({rc})")
+        self._h = h
+        self.max_batch = int(max_batch)
+        self.set_params(init_params(seed) if params is None else params)
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = self._lib.vpbs_mlp_last_error(self._h)
+            raise _lib.VpbsError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.vpbs_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(self._lib.vpbs_mlp_set_params(self._h, _lib.fptr(p), p.size), "mlp set_params")
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(_lib.MLP_NPARAMS, dtype=np.float32)
+        self._check(self._lib.vpbs_mlp_get_params(self._h, _lib.fptr(p), p.size), "mlp get_params")
+        return p
+
+    def set_loss_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._check(self._lib.vpbs_mlp_set_loss_weights(self._h, _lib.fptr(w)), "mlp set_loss_weights")
+
+    def forward(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.zeros((X.shape[0], _lib.MLP_OUT), dtype=np.float32)
+        for a in range(0, X.shape[0], self.max_batch):
+            Xa = np.ascontiguousarray(X[a:a + self.max_batch])
+            Ya = np.zeros((Xa.shape[0], _lib.MLP_OUT), dtype=np.float32)
+            self._check(self._lib.vpbs_mlp_forward(self._h, _lib.fptr(Xa), Xa.shape[0], _lib.fptr(Ya)), "mlp forward")
+            Y[a:a + self.max_batch] = Ya
+        return Y
+
+    def gradient(self, X, T):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        g = np.zeros(_lib.MLP_NPARAMS, dtype=np.float32)
+        loss = ct.c_float()
+        self._check(self._lib.vpbs_mlp_gradient(self._h, _lib.fptr(X), _lib.fptr(T), X.shape[0], _lib.fptr(g),
+                                                ct.byref(loss)), "mlp gradient")
+        return float(loss.value), g
+
+    def train_step(self, X, T, lr: float) -> float:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        loss = ct.c_float()
+        self._check(self._lib.vpbs_mlp_train_step(self._h, _lib.fptr(X), _lib.fptr(T), X.shape[0], float(lr),
+                                                  ct.byref(loss)), "mlp train_step")
+        return float(loss.value)
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-normal weights, zero biases, in the flat layout of csrc/mlp.cu."""
+    rng = np.random.default_rng(seed)
+    I, H, O = _lib.MLP_IN, _lib.MLP_HIDDEN, _lib.MLP_OUT
+    parts = [rng.normal(0, math.sqrt(2.0 / I), (H, I)), np.zeros(H), rng.normal(0, math.sqrt(2.0 / H), (H, H)),
+             np.zeros(H), rng.normal(0, math.sqrt(1.0 / H), (O, H)), np.zeros(O)]
+    return np.concatenate([p.ravel() for p in parts]).astype(np.float32)
+
+
+def targets_of(choice: tuning.EwaldChoice, L: float) -> np.ndarray:
+    """Network outputs of a parameter choice: (log alpha L, r_cut / L, log2 Ns, sigma, m)."""
+    return np.array([math.log(choice.alpha * L), choice.rcut / L, math.log2(choice.Ns), choice.sigma, choice.m],
+                    dtype=np.float64)
+
+
+def choice_of(y, L: float) -> tuning.EwaldChoice:
+    """Valid parameters from (de-standardised) network outputs."""
+    alpha = math.exp(float(y[0])) / L
+    rcut = min(max(float(y[1]), 1 / 64), 0.35) * L
+    sigma = min(tuning.SIGMAS, key=lambda s: abs(s - float(y[3])))
+    m = int(min(max(round(float(y[4])), 2), 8))
+    Ns_min = max(8, int(round(2.0 ** float(y[2]))))
+    return tuning.EwaldChoice(alpha=alpha, rcut=rcut, Ns=tuning.grid_for(Ns_min, sigma, m), sigma=sigma, m=m)
+
+
+@dataclass
+class Predictor:
+    """Trained network weights with the feature and output standardisation."""
+    params: np.ndarray
+    x_mean: np.ndarray
+    x_std: np.ndarray
+    y_mean: np.ndarray
+    y_std: np.ndarray
+    rtol: float
+
+    def save(self, path):
+        np.savez(path, params=self.params, x_mean=self.x_mean, x_std=self.x_std, y_mean=self.y_mean,
+                 y_std=self.y_std, rtol=np.array(self.rtol))
+
+    @classmethod
+    def load(cls, path=DEFAULT_MODEL) -> "Predictor":
+        z = np.load(path)
+        return cls(params=z["params"].astype(np.float32), x_mean=z["x_mean"], x_std=z["x_std"], y_mean=z["y_mean"],
+                   y_std=z["y_std"], rtol=float(z["rtol"]))
+
+    def outputs(self, features, net: MLP | None = None) -> np.ndarray:
+        X = ((np.atleast_2d(features) - self.x_mean) / self.x_std).astype(np.float32)
+        own = net is None
+        net = net or MLP(max_batch=max(1, X.shape[0]), params=self.params)
+        try:
+            if not own:
+                net.set_params(self.params)
+            Y = net.forward(X)
+        finally:
+            if own:
+                net.close()
+        return Y * self.y_std + self.y_mean
+
+    def predict_choice(self, features, L: float) -> tuning.EwaldChoice:
+        return choice_of(self.outputs(features)[0], L)
+
+
+def feature_params(L: float):
+    """Parameters of the cache the features are computed on (its cell lists bound the nearest-
+    distance search; its Fourier grid is never used)."""
+    return configs.params_for(FEATURE_RCUT * L, 3.0, 16, 2)
+
+
+def features_of(fs, L: float) -> np.ndarray:
+    from .biotsavart import init_cache
+    c = init_cache(feature_params(L))
+    try:
+        c.set_filaments(fs)
+        return c.features()
+    finally:
+        c.close()
+
+
+def reference_choice(L: float) -> tuning.EwaldChoice:
+    """Parameters of the FP64 reference the sweeps and the check compare against (beta = 4 in both
+    ranges, r_cut = L/16, NUFFT m = 6): about 1e-8 relative error, far below the targets."""
+    alpha = 4.0 / (L / 16)
+    return tuning.EwaldChoice(alpha=alpha, rcut=L / 16, Ns=tuning.grid_for(
+        tuning.kmax_to_gridsize(2 * alpha * 4.0, L), 1.5, 6), sigma=1.5, m=6)
+
+
+def reference_velocity(fs, L: float) -> np.ndarray:
+    return tuning.measure(fs, reference_choice(L), L, precision="fp64", reps=1)[1]
+
+
+def random_configuration(rng: np.random.Generator, L: float = 2 * math.pi, min_nodes: int = 5_000,
+                         max_nodes: int = 1_200_000):
+    """A random tangle of the benchmark's ring family: node count log-uniform in
+    [min_nodes, max_nodes], random ring resolution (32-400 nodes per ring, at most 8000 rings) and
+    radii (the training and held-out configurations)."""
+    target = 10 ** rng.uniform(math.log10(min_nodes), math.log10(max_nodes))
+    npr = int(rng.choice([32, 48, 64, 96, 128, 200, 256, 400]))
+    nrings = int(min(max(1, round(target / npr)), 8000))
+    rmin = L * rng.uniform(0.04, 0.14)
+    rmax = min(rmin * rng.uniform(1.2, 2.5), L / 4)
+    return curves.random_tangle(nrings, npr, L=L, rmin=rmin, rmax=rmax, seed=int(rng.integers(1 << 31)))
+
+
+LABEL_MARGIN = 0.6  # labels are the cheapest sweep point with error <= LABEL_MARGIN * rtol
+
+
+def sweep_configuration(fs, L: float, choices, rtol: float = 1e-5):
+    """Features, sweep records and label (cheapest choice within LABEL_MARGIN * rtol) of one
+    configuration, plus the cost of the default rule at rtol."""
+    feats = features_of(fs, L)
+    vref = reference_velocity(fs, L)
+    recs = tuning.sweep(fs, L, vref, choices, "mixed")
+    best = tuning.cheapest(recs, LABEL_MARGIN * rtol)
+    d = tuning.sweep(fs, L, vref, [tuning.default_rule(L, rtol, FEATURE_RCUT * L)], "mixed")[0]
+    return feats, recs, best, d
+
+
+def training_choices(L: float):
+    return tuning.candidate_grid(L, rcut_fracs=(1 / 12, 1 / 16, 1 / 20, 1 / 24, 1 / 32, 1 / 40, 1 / 48),
+                                 betas=(2.9, 3.1, 3.3), sigma_m=((1.25, 4), (1.5, 3), (2.0, 3)))
+
+
+def generate_dataset(n: int, seed: int, L: float = 2 * math.pi, rtol: float = 1e-5, min_nodes: int = 5_000,
+                     max_nodes: int = 1_200_000, log=None) -> dict:
+    """(features, label) pairs of `n` random configurations from parameter sweeps against the
+    FP64 reference, with the default rule's cost and error for comparison."""
+    rng = np.random.default_rng(seed)
+    choices = training_choices(L)
+    X, Y, nodes, best_ms, default_ms, default_err = [], [], [], [], [], []
+    for k in range(n):
+        fs = random_configuration(rng, L, min_nodes, max_nodes)
+        feats, recs, best, d = sweep_configuration(fs, L, choices, rtol)
+        if best is None:
+            continue
+        ch = tuning.EwaldChoice(alpha=best["alpha"], rcut=best["rcut"], Ns=best["Ns"], sigma=best["sigma"], m=best["m"])
+        X.append(feats)
+        Y.append(targets_of(ch, L))
+        nodes.append(sum(len(f) for f in fs))
+        best_ms.append(best["ms"])
+        default_ms.append(d["ms"])
+        default_err.append(d["rel_l2"])
+        if log:
+            log(f"{k}: N={nodes[-1]} best {best['ms']:.2f} ms (rcut L/{L / best['rcut']:.0f}, fft {best['fft']}, "
+                f"m {best['m']}) default {d['ms']:.2f} ms err {d['rel_l2']:.1e}")
+    return {"X": np.array(X, dtype=np.float32), "Y": np.array(Y), "nodes": np.array(nodes),
+            "best_ms": np.array(best_ms), "default_ms": np.array(default_ms), "default_err": np.array(default_err),
+            "rtol": rtol, "L": L}
+
+
+def train(X, Y, rtol: float, steps: int = 4000, lr: float = 3e-3, seed: int = 0, device: int = 0) -> Predictor:
+    """Full-batch Adam on the GPU (the library's MLP kernels) on standardised inputs/outputs."""
+    X = np.asarray(X, dtype=np.float64)
+    Y = np.asarray(Y, dtype=np.float64)
+    x_mean, x_std = X.mean(0), X.std(0) + 1e-6
+    y_mean, y_std = Y.mean(0), Y.std(0) + 1e-6
+    Xs = ((X - x_mean) / x_std).astype(np.float32)
+    Ys = ((Y - y_mean) / y_std).astype(np.float32)
+    net = MLP(max_batch=len(Xs), device=device, seed=seed)
+    try:
+        for s in range(steps):
+            net.train_step(Xs, Ys, lr if s < steps // 2 else lr / 4)
+        params = net.get_params()
+    finally:
+        net.close()
+    return Predictor(params=params, x_mean=x_mean, x_std=x_std, y_mean=y_mean, y_std=y_std, rtol=rtol)
+
+
+def choose_parameters(fs, L: float, rtol: float = 1e-5, predictor: Predictor | None = None, check: bool = True):
+    """Predicted parameters for `fs` at tolerance `rtol`; with `check`, a plain FP64 evaluation
+    judges the prediction (mixed form) and the default rule replaces it when it misses rtol.
+    Returns (choice, info)."""
+    pred = predictor or Predictor.load()
+    feats = features_of(fs, L)
+    ch = pred.predict_choice(feats, L)
+    info = {"features": feats, "predicted": ch, "fallback": False}
+    if check:
+        vref = reference_velocity(fs, L)
+        _, v = tuning.measure(fs, ch, L, "mixed", reps=1)
+        err = tuning.rel_errors(v, vref)[0]
+        info["rel_l2"] = err
+        if not err <= rtol:
+            info["fallback"] = True
+            ch = tuning.default_rule(L, rtol, FEATURE_RCUT * L)
+    return ch, info
