@@ -1,13 +1,17 @@
-"""Benchmark: Biot-Savart node velocities per second (velocity_on_nodes! on a 20k-node tangle).
+"""Benchmark: Biot-Savart node velocities per second at a 1e-5 relative-error target, tuned FP32
+(learned parameters) against plain FP64, on the 1M-node tangle.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
 One step = one velocity evaluation on all nodes of the workload: device-side point data
 (quintic splines, quadrature points), cell lists, pair kernel, local term, NUFFT long range.
-`value` is measured with the filament nodes already resident in HBM; `e2e` goes through the
-public API (velocity_on_nodes_ with host arrays): host->device copy of the nodes and
-device->host copy of the velocities inside the timed region.  Multi-GPU (torchrun): every rank
-evaluates its own independent tangle (weak scaling, no collective on the data path).
+The headline `value` is the tuned form: mixed precision at the Ewald/NUFFT parameters the
+learned predictor chooses for the target (checked against a plain FP64 evaluation); the plain
+FP64 and mixed forms at the workload's own parameters are reported under `forms`.  `value` is
+measured with the filament nodes already resident in HBM; `e2e` goes through the public API
+(velocity_on_nodes_ with host arrays): host->device copy of the nodes and device->host copy of
+the velocities inside the timed region.  Multi-GPU (torchrun): every rank evaluates its own
+independent tangle (weak scaling, no collective on the data path).
 """
 
 from __future__ import annotations
@@ -134,7 +138,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     vp = load_package()
-    fs, p = vp.configs.WORKLOADS[args.workload]()
+    fs, p, desc = cpu_sample(vp, args.workload)
     Np = sum(len(f) for f in fs)
     cores = host_cores()
     for _ in range(min(args.warmup, 1)):
@@ -148,8 +152,7 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD_DESC[args.workload], "fields": "velocity"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"one full velocity evaluation of {args.workload} per step "
-                                   "(CPU FP64 restatement of the reference path, OpenMP)"},
+                         "sample": f"one evaluation per step; {desc}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -157,18 +160,19 @@ def run_reference(args):
 
 
 def stage_model(stage, S):
-    """Algorithmic work per launch of each stage: (bound, amount, unit)."""
-    Np, Nq, n3, nc3 = S["Np"], S["Nq"], S["n3"], S["nc3"]
+    """Algorithmic work per launch of each stage: (bound, amount, unit).  S["gsz"] is the grid
+    element size (8 bytes in the plain form, 4 in the FP32 forms)."""
+    Np, Nq, n3, nc3, g = S["Np"], S["Nq"], S["n3"], S["nc3"], S["gsz"]
     if stage == "pairs":
-        return "fp64", S["pairs"] * F_PAIR_VEL, "flop"
+        return S["pair_bound"], S["pairs"] * F_PAIR_VEL, "flop"
     if stage == "spread":
-        return "hbm", Nq * 6 * 8 + 3 * n3 * 8, "byte"
+        return "hbm", Nq * 6 * 8 + 3 * n3 * g, "byte"
     if stage == "interp":
-        return "hbm", 3 * n3 * 8 + Np * 3 * 8 + Np * 3 * 8, "byte"
+        return "hbm", 3 * n3 * g + Np * 3 * 8 + Np * 3 * 8, "byte"
     if stage == "fourier":
-        return "hbm", 2 * 3 * nc3 * 16, "byte"
+        return "hbm", 2 * 3 * nc3 * 2 * g, "byte"
     if stage in ("fft_forward", "fft_inverse"):
-        return "hbm", 2 * 2 * 3 * n3 * 8, "byte"
+        return "hbm", 2 * 2 * 3 * n3 * g, "byte"
     if stage == "local_self":
         return "hbm", Np * (11 * 8 + 6 * S["nq"] * 6 * 8) + Np * 3 * 8, "byte"
     if stage == "geometry":
@@ -290,6 +294,52 @@ def measure_form(vp, p, fs, args, dev, world, local_rank):
             "pairs_in_range": pairs_in_range, "v": v_dev.copy(), "v_api": v_api, "clk": clk}
 
 
+def form_summary(p, m, Np, Nq, world, args, peaks):
+    """Throughputs and the per-stage roofline of one measured form (rank 0)."""
+    from vortexpasta_b200 import _lib
+    n = [_lib.load().vpbs_fft_size(N, p.backend_long.sigma) for N in p.splitting.Ns]
+    fp32 = p.precision == "mixed"
+    S = {"Np": Np, "Nq": Nq, "n3": n[0] * n[1] * n[2], "nc3": (n[0] // 2 + 1) * n[1] * n[2],
+         "pairs": m["pairs_in_range"], "nq": len(p.quadrature), "gsz": 4 if fp32 else 8,
+         "pair_bound": "fp32" if fp32 else "fp64"}
+    avg = {k: statistics.mean(v) for k, v in m["stage_ms"].items()}
+    stages = {}
+    for name, ms in avg.items():
+        bound, amount, unit = stage_model(name, S)
+        if ms <= 0:
+            continue
+        if bound in ("fp64", "fp32"):
+            ach = amount / (ms * 1e-3) / 1e12
+            pk = peaks[bound]
+            stages[name] = {"ms": ms, "bound": bound, "achieved": ach, "unit": "TFLOP/s", "peak": pk,
+                            "frac": ach / pk if pk else None}
+        else:
+            ach = amount / (ms * 1e-3) / 1e9
+            stages[name] = {"ms": ms, "bound": "hbm", "achieved": ach, "unit": "GB/s", "peak": peaks["hbm"],
+                            "frac": ach / peaks["hbm"]}
+    dom = max(avg, key=avg.get)
+    return {"value": world * Np * args.steps / (m["total_ms"] * 1e-3), "ms_per_step": m["total_ms"] / args.steps,
+            "e2e_value": world * Np * args.steps / (m["e2e_ms"] * 1e-3), "stages": stages, "dominant": dom,
+            "fft": n[0], "pairs_in_range": int(m["pairs_in_range"])}
+
+
+def device_peaks(local_rank):
+    import ctypes as ct
+    from vortexpasta_b200 import _lib
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    out = {"hbm": peaks.get("hbm_gbs") or 6650.0,
+           "hbm_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks.get("hbm_gbs") else "fallback 6650 GB/s"}
+    for key, fp64 in (("fp64", 1), ("fp32", 0)):
+        v = ct.c_double()
+        out[key] = v.value if _lib.load().vpbs_fma_throughput(local_rank, fp64, ct.byref(v)) == 0 else None
+    return out
+
+
+def errors_vs(v, vref):
+    return {"rel_l2_vs_fp64": float(np.linalg.norm(v - vref) / np.linalg.norm(vref)),
+            "max_err_vs_fp64": float(np.abs(v - vref).max() / np.abs(vref).max())}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -302,101 +352,106 @@ def run_ours(args):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     vp = load_package()
-    from vortexpasta_b200 import _lib
+    from vortexpasta_b200 import learned
     fs, p = rank_workload(vp, args.workload, rank)
     p = p.with_(device=local_rank)
+    L = p.splitting.Ls[0]
     Np = sum(len(f) for f in fs)
     Nq = Np * len(p.quadrature)
     nodes, offsets = vp.curves.concat(fs)
 
+    # plain FP64 and mixed forms at the workload's parameters
     m64 = measure_form(vp, p, fs, args, dev, world, local_rank)
     mixed = measure_form(vp, p.with_(precision="mixed"), fs, args, dev, world, local_rank) if args.mixed else None
-    total_ms, e2e_ms, stage_ms, clk = m64["total_ms"], m64["e2e_ms"], m64["stage_ms"], m64["clk"]
-    launches, pairs_in_range, v_dev = m64["launches"], m64["pairs_in_range"], m64["v"]
-    ms_per_step = total_ms / args.steps
-    value = world * Np * args.steps / (total_ms * 1e-3)
-    e2e_value = world * Np * args.steps / (e2e_ms * 1e-3)
+    # tuned form: parameters from the learned predictor (checked against a plain FP64 evaluation,
+    # default rule on a miss), FP32 bulk arithmetic
+    tuned = None
+    if args.tuned:
+        t0 = time.perf_counter()
+        choice, info = learned.choose_parameters(fs, L, rtol=args.rtol, device=local_rank)
+        t_choose = time.perf_counter() - t0
+        pt = choice.params(L, "mixed", device=local_rank)
+        tuned = measure_form(vp, pt, fs, args, dev, world, local_rank)
+    head = tuned if tuned is not None else m64
+    head_p = pt if tuned is not None else p
 
     if rank == 0:
-        lr = p.splitting
-        n = [_lib.load().vpbs_fft_size(N, p.backend_long.sigma) for N in lr.Ns]
-        S = {"Np": Np, "Nq": Nq, "n3": n[0] * n[1] * n[2], "nc3": (n[0] // 2 + 1) * n[1] * n[2], "pairs": pairs_in_range,
-             "nq": len(p.quadrature)}
-        avg = {k: statistics.mean(v) for k, v in stage_ms.items()}
-        dom = max(avg, key=avg.get)
-        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-        hbm = peaks.get("hbm_gbs")
-        hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if hbm else "fallback 6650 GB/s"
-        hbm = hbm or 6650.0
-        fp64_peak = ct_double = None
-        import ctypes as ct
-        ct_double = ct.c_double()
-        if _lib.load().vpbs_fma_throughput(local_rank, 1, ct.byref(ct_double)) == 0:
-            fp64_peak = ct_double.value
-        stages = {}
-        for name, ms in avg.items():
-            bound, amount, unit = stage_model(name, S)
-            if ms <= 0:
-                continue
-            if bound == "fp64":
-                ach = amount / (ms * 1e-3) / 1e12
-                stages[name] = {"ms": ms, "bound": "fp64", "achieved": ach, "unit": "TFLOP/s",
-                                "frac": ach / fp64_peak if fp64_peak else None}
-            else:
-                ach = amount / (ms * 1e-3) / 1e9
-                stages[name] = {"ms": ms, "bound": "hbm", "achieved": ach, "unit": "GB/s", "frac": ach / hbm}
-        d = stages[dom]
-        roof = {"kernel": dom, "bound": d["bound"], "achieved": d["achieved"],
-                "peak": fp64_peak if d["bound"] == "fp64" else hbm, "unit": d["unit"], "frac": d["frac"],
-                "traffic": read_traffic(dom),
-                "peak_source": ("measured FP64 FMA throughput (vpbs_fma_throughput)" if d["bound"] == "fp64"
-                                else hbm_src)}
+        peaks = device_peaks(local_rank)
+        f64 = form_summary(p, m64, Np, Nq, world, args, peaks)
+        fh = form_summary(head_p, head, Np, Nq, world, args, peaks)
+        d = fh["stages"][fh["dominant"]]
+        roof = {"kernel": fh["dominant"], "bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"],
+                "unit": d["unit"], "frac": d["frac"], "traffic": read_traffic(fh["dominant"]),
+                "peak_source": {"fp64": "measured FP64 FMA throughput (vpbs_fma_throughput)",
+                                "fp32": "measured FP32 FMA throughput (vpbs_fma_throughput)"}.get(d["bound"],
+                                                                                                   peaks["hbm_source"])}
+        forms = {"fp64": {**{k: f64[k] for k in ("value", "ms_per_step", "e2e_value")},
+                          "stages_ms": {k: v["ms"] for k, v in f64["stages"].items()},
+                          "description": "plain FP64 at the workload's parameters"}}
+        if mixed is not None:
+            fm = form_summary(p.with_(precision="mixed"), mixed, Np, Nq, world, args, peaks)
+            forms["mixed"] = {**{k: fm[k] for k in ("value", "ms_per_step", "e2e_value")},
+                              "speedup_vs_fp64": fm["value"] / f64["value"], **errors_vs(mixed["v"], m64["v"]),
+                              "stages_ms": {k: v["ms"] for k, v in fm["stages"].items()},
+                              "description": "FP32 pair sum / spreading / FFT / interpolation at the workload's "
+                                             "parameters; FP64 positions, separations, local and self terms, "
+                                             "accumulation"}
+        if tuned is not None:
+            forms["tuned"] = {**{k: fh[k] for k in ("value", "ms_per_step", "e2e_value")},
+                              "speedup_vs_fp64": fh["value"] / f64["value"],
+                              "e2e_speedup_vs_fp64": fh["e2e_value"] / f64["e2e_value"],
+                              **errors_vs(tuned["v"], m64["v"]),
+                              "parameters": {**choice.as_dict(), "fft": fh["fft"], "rcut_over_L": choice.rcut / L,
+                                             "beta": choice.beta_short},
+                              "predictor": {"fallback_to_default_rule": bool(info["fallback"]),
+                                            "checked_rel_l2": info.get("rel_l2"), "rtol": args.rtol,
+                                            "seconds": t_choose},
+                              "stages_ms": {k: v["ms"] for k, v in fh["stages"].items()},
+                              "description": "mixed precision at parameters predicted by the learned MLP"}
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_DESC[args.workload], "form": "plain FP64", "fields": "velocity",
+            "metric": METRIC, "value": fh["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": fh["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if tuned is not None else "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_DESC[args.workload],
+                       "form": ("tuned FP32 (learned parameters; FP64 positions, separations, local term and "
+                                "accumulation), compared with plain FP64 at the workload's parameters under 'forms'"
+                                if tuned is not None else "plain FP64"),
+                       "fields": "velocity", "target_rel_l2": args.rtol,
                        "parallelism": f"replicas x{world} (independent tangles, no collective)",
                        "l2": "flushed between timed steps (256 MiB write, outside the timed events)"},
             "roofline": roof,
-            "stages": stages,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(nodes.nbytes + offsets.nbytes),
+            "stages": fh["stages"],
+            "forms": forms,
+            "e2e": {"value": fh["e2e_value"], "unit": UNIT, "h2d_bytes_per_step": int(nodes.nbytes + offsets.nbytes),
                     "d2h_bytes_per_step": int(Np * 3 * 8)},
-            "gpu_launches": int(launches),
-            "clocks": clk.summary(),
-            "pairs_in_range": int(pairs_in_range),
+            "gpu_launches": int(head["launches"]),
+            "clocks": head["clk"].summary(),
+            "pairs_in_range": fh["pairs_in_range"],
         }
-        if mixed is not None:
-            vm = mixed["v"]
-            line["forms"] = {
-                "fp64": {"value": value, "ms_per_step": ms_per_step, "e2e_value": e2e_value},
-                "mixed": {
-                    "value": world * Np * args.steps / (mixed["total_ms"] * 1e-3),
-                    "ms_per_step": mixed["total_ms"] / args.steps,
-                    "e2e_value": world * Np * args.steps / (mixed["e2e_ms"] * 1e-3),
-                    "speedup_vs_fp64": total_ms / mixed["total_ms"],
-                    "rel_l2_vs_fp64": float(np.linalg.norm(vm - v_dev) / np.linalg.norm(v_dev)),
-                    "max_err_vs_fp64": float(np.abs(vm - v_dev).max() / np.abs(v_dev).max()),
-                    "rel_l2_e2e_vs_fp64": float(np.linalg.norm(mixed["v_api"] - m64["v_api"]) /
-                                                np.linalg.norm(m64["v_api"])),
-                    "stages_ms": {k: statistics.mean(x) for k, x in mixed["stage_ms"].items()},
-                    "description": "FP32 pair sum / spreading / FFT / interpolation; FP64 positions, separations, "
-                                   "local and self terms, final accumulation",
-                },
-            }
-        if args.workload == "tangle1m":
-            args.no_cpu_baseline = True  # one oracle evaluation of 1M nodes takes minutes: not a bounded sample
         if world == 1 and not args.no_cpu_baseline:
             cores = host_cores()
-            t_cpu, v_cpu = cpu_oracle_time(fs, p, cores, args.cpu_reps)
-            line["cpu_baseline"] = {"value": Np / t_cpu, "unit": UNIT, "cores": cores, "kind": "port",
-                                    "sample": f"{args.cpu_reps} full velocity evaluations of {args.workload} "
-                                              "(CPU FP64 restatement, OpenMP), best taken"}
-            line["accuracy"] = {"rel_l2_vs_oracle": float(np.linalg.norm(v_dev - v_cpu) / np.linalg.norm(v_cpu))}
+            sfs, sp, desc = cpu_sample(vp, args.workload)
+            t_cpu, v_cpu = cpu_oracle_time(sfs, sp, cores, args.cpu_reps)
+            line["cpu_baseline"] = {"value": sum(len(f) for f in sfs) / t_cpu, "unit": UNIT, "cores": cores,
+                                    "kind": "port", "sample": desc}
+            if args.workload != "tangle1m":
+                line["accuracy"] = {"fp64_rel_l2_vs_oracle": float(np.linalg.norm(m64["v"] - v_cpu) /
+                                                                   np.linalg.norm(v_cpu))}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def cpu_sample(vp, workload):
+    """The bounded CPU sample of a workload: (filaments, parameters, description)."""
+    if workload == "tangle1m":
+        fs, p = vp.configs.tangle1m_cpu_sample()
+        return fs, p, ("tangle1m_cpu_sample: 1/64-volume replica of tangle1m (cube L/4, 78 rings x 200 nodes = "
+                       "15,600 nodes, same node density, same absolute r_cut, alpha and grid spacing), "
+                       "best of the timed full velocity evaluations (CPU FP64 restatement, OpenMP)")
+    fs, p = vp.configs.WORKLOADS[workload]()
+    return fs, p, (f"full velocity evaluations of {workload}, best taken (CPU FP64 restatement, OpenMP)")
 
 
 def main():
@@ -405,11 +460,14 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tangle20k", choices=sorted(WORKLOAD_DESC))
+    ap.add_argument("--workload", default="tangle1m", choices=sorted(WORKLOAD_DESC))
     ap.add_argument("--cpu-reps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", dest="mixed", action="store_false",
                     help="skip the mixed-precision (FP32 bulk) form reported under 'forms'")
+    ap.add_argument("--no-tuned", dest="tuned", action="store_false",
+                    help="skip the tuned form (learned parameters); the headline is then the plain FP64 form")
+    ap.add_argument("--rtol", type=float, default=1e-5, help="accuracy target of the tuned form")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

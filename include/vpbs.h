@@ -209,6 +209,38 @@ int vpbs_ewald_table_eval(double xmax, const double* x, int64_t n, double* erfc_
  * reference. */
 int vpbs_fma_throughput(int32_t device, int32_t fp64, double* tflops);
 
+/* ---- Time stepping and ensembles (the batching form) ---- */
+
+/* One classic RK4 step (src/Timestepping/timesteppers/explicit/RK4.jl:14-44, advection of
+ * advect.jl:40-76) of the filaments last loaded with vpbs_set_filaments: `nodes` is a device AoS
+ * array [Np][3] with that filament layout, advanced in place by dt.  Each stage re-solves the
+ * splines on the stage nodes with the knots of the first stage (update_coefficients! with
+ * knots = ts_base) and evaluates the velocity as vpbs_compute(VELOCITY, LIA_TRUE, both ranges).
+ * The velocity of the last stage stays in the handle.  After the first call on a handle it
+ * neither allocates nor synchronises with the host (capturable).  Asynchronous on the handle's
+ * stream. */
+int vpbs_rk4_step(vpbs_handle* h, double* nodes, double dt);
+
+/* An ensemble of independent systems (handles on one device, each holding filaments and its own
+ * device node array and time step) advanced together: one RK4 step of every system, each on its
+ * own stream, is captured into one CUDA graph at creation (after a dt = 0 warm-up step that
+ * leaves the nodes unchanged) and vpbs_ensemble_step replays it `nsteps` times (one graph launch
+ * per step, asynchronous on the ensemble's stream).  Errors: vpbs_ensemble_last_error. */
+typedef struct vpbs_ensemble vpbs_ensemble;
+int vpbs_ensemble_create(vpbs_handle* const* systems, double* const* nodes, const double* dts, int32_t n,
+                         vpbs_ensemble** out);
+int vpbs_ensemble_step(vpbs_ensemble* e, int32_t nsteps);
+int vpbs_ensemble_synchronize(vpbs_ensemble* e);
+void* vpbs_ensemble_stream(vpbs_ensemble* e);
+int vpbs_ensemble_destroy(vpbs_ensemble* e);
+const char* vpbs_ensemble_last_error(void);
+
+/* Autotuner: times the pair kernel on the handle's current point data for each candidate
+ * number of cells per CTA edge (1-4, and the built-in rule) and keeps the fastest for later
+ * evaluations (`chosen`: 0 = the rule, else the edge).  Overwrites the handle's output fields.
+ * Synchronous. */
+int vpbs_autotune(vpbs_handle* h, int32_t* chosen);
+
 /* ---- Learned parameter predictor (no counterpart in the reference, which removed its alpha
  * autotuner; the fallback is the default rule of splitting/gaussian.jl:133-200). ---- */
 
@@ -224,7 +256,8 @@ int vpbs_features(vpbs_handle* h, float* out, int32_t n);
  * b2, W3 (OUT x H), b3].  Inputs X are row-major [n][IN], targets and outputs [n][OUT].  The loss
  * is sum_o w_o (y_o - t_o)^2 averaged over the batch (w: vpbs_mlp_set_loss_weights, default 1).
  * vpbs_mlp_train_step runs forward, backward and one Adam step (beta1 0.9, beta2 0.999, eps 1e-8)
- * on the device; vpbs_mlp_gradient returns the loss and its gradient without updating.  n must not
+ * on the device (with the L2 term of vpbs_mlp_set_weight_decay, default 0); vpbs_mlp_gradient returns
+ * the data loss and its gradient without updating.  n must not
  * exceed the max_batch given at creation.  Errors: vpbs_mlp_last_error. */
 #define VPBS_MLP_IN 16
 #define VPBS_MLP_HIDDEN 64
@@ -238,6 +271,7 @@ const char* vpbs_mlp_last_error(const vpbs_mlp* m);
 int vpbs_mlp_set_params(vpbs_mlp* m, const float* params, int64_t n);
 int vpbs_mlp_get_params(vpbs_mlp* m, float* params, int64_t n);
 int vpbs_mlp_set_loss_weights(vpbs_mlp* m, const float* w);
+int vpbs_mlp_set_weight_decay(vpbs_mlp* m, float wd);  /* L2 term (wd/2)|p|^2 in the training loss */
 int vpbs_mlp_forward(vpbs_mlp* m, const float* X, int32_t n, float* Y);
 int vpbs_mlp_gradient(vpbs_mlp* m, const float* X, const float* T, int32_t n, float* grad, float* loss);
 int vpbs_mlp_train_step(vpbs_mlp* m, const float* X, const float* T, int32_t n, float lr, float* loss);

@@ -192,3 +192,19 @@ def test_errors_surface(vp, built_lib):
         cache.set_filaments([vp.curves.ring(4, 0.5, center=(3, 3, 3))])
     with pytest.raises(ValueError, match="not recognised"):
         vp.compute_on_nodes_({"vorticity": [np.zeros_like(fs[0])]}, cache, fs)
+
+
+@pytest.mark.gpu
+def test_spline_solve_at_exactly_48k_shared_memory(vp):
+    """Filaments of 128 nodes make the spline solve ask for exactly 48 KB of shared memory;
+    this must work in a fresh process-wide state (no earlier larger launch)."""
+    fs = vp.configs.tangle(5, 128, seed=11)
+    p = vp.configs.params_for(2 * np.pi / 8, 3.5, 32, 4)
+    c = vp.init_cache(p)
+    try:
+        c.set_filaments(fs)
+        c.compute(1)
+        v = c.get(1)
+    finally:
+        c.close()
+    assert np.isfinite(v).all() and np.abs(v).max() > 0

@@ -121,3 +121,24 @@ def test_features_match_oracle():
     assert np.allclose(f[:4], ref[:4], rtol=1e-5, atol=1e-6)
     assert np.allclose(f[4:], ref[4:], atol=1.5 / len(pd["nodes"]))  # at most one node on a bin edge
     assert f[4:].sum() == pytest.approx(1.0, abs=1e-6)
+
+
+@pytest.mark.gpu
+def test_predictor_beats_default_rule_on_heldout_tangles():
+    """The committed network (data/predictor.npz) against the reference's default rule at 1e-5
+    on held-out tangles from a seed the training never used: every final choice meets the
+    target (or is the default rule after a rejected prediction) and together the predicted
+    parameters take less device time."""
+    pred = learned.Predictor.load()
+    rng = np.random.default_rng(2024)
+    tot_p = tot_d = 0.0
+    for _ in range(3):
+        fs = learned.random_configuration(rng, L, min_nodes=150_000, max_nodes=400_000)
+        vref = learned.reference_velocity(fs, L)
+        ch, info = learned.choose_parameters(fs, L, 1e-5, pred)
+        ms_p, v_p = tuning.measure(fs, ch, L, "mixed")
+        ms_d, _ = tuning.measure(fs, tuning.default_rule(L, 1e-5, L * learned.FEATURE_RCUT), L, "mixed")
+        assert info["fallback"] or tuning.rel_errors(v_p, vref)[0] <= 1e-5
+        tot_p += ms_p
+        tot_d += ms_d
+    assert tot_p < tot_d

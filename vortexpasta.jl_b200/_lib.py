@@ -67,12 +67,22 @@ SIGNATURES = {
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "vpbs_features": (ct.c_int, [ct.c_void_p, c_float_p, ct.c_int32]),
+    "vpbs_rk4_step": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_double]),
+    "vpbs_ensemble_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_void_p), c_double_p, ct.c_int32,
+                                        ct.POINTER(ct.c_void_p)]),
+    "vpbs_ensemble_step": (ct.c_int, [ct.c_void_p, ct.c_int32]),
+    "vpbs_ensemble_synchronize": (ct.c_int, [ct.c_void_p]),
+    "vpbs_ensemble_stream": (ct.c_void_p, [ct.c_void_p]),
+    "vpbs_ensemble_destroy": (ct.c_int, [ct.c_void_p]),
+    "vpbs_ensemble_last_error": (ct.c_char_p, []),
+    "vpbs_autotune": (ct.c_int, [ct.c_void_p, c_int32_p]),
     "vpbs_mlp_create": (ct.c_int, [ct.c_int32, ct.c_int32, ct.POINTER(ct.c_void_p)]),
     "vpbs_mlp_destroy": (ct.c_int, [ct.c_void_p]),
     "vpbs_mlp_last_error": (ct.c_char_p, [ct.c_void_p]),
     "vpbs_mlp_set_params": (ct.c_int, [ct.c_void_p, c_float_p, ct.c_int64]),
     "vpbs_mlp_get_params": (ct.c_int, [ct.c_void_p, c_float_p, ct.c_int64]),
     "vpbs_mlp_set_loss_weights": (ct.c_int, [ct.c_void_p, c_float_p]),
+    "vpbs_mlp_set_weight_decay": (ct.c_int, [ct.c_void_p, ct.c_float]),
     "vpbs_mlp_forward": (ct.c_int, [ct.c_void_p, c_float_p, ct.c_int32, c_float_p]),
     "vpbs_mlp_gradient": (ct.c_int, [ct.c_void_p, c_float_p, c_float_p, ct.c_int32, c_float_p, c_float_p]),
     "vpbs_mlp_train_step": (ct.c_int, [ct.c_void_p, c_float_p, c_float_p, ct.c_int32, ct.c_float, c_float_p]),

@@ -49,3 +49,17 @@ def tangle1m(seed: int = 42, **kw):
 
 
 WORKLOADS = {"ring64": ring64, "tangle20k": tangle20k, "tangle1m": tangle1m}
+
+
+def tangle1m_cpu_sample(seed: int = 42, **kw):
+    """Bounded CPU sample of ``tangle1m``: a cube of side L/4 (1/64 of the volume) holding 78 rings
+    x 200 nodes (15,600 nodes: the same node density) with radii scaled by 1/4, and the same
+    absolute parameters -- r_cut = L/16 (= L'/4), alpha = 4 / r_cut, the same grid spacing
+    (Ns = 128, FFT 192^3), m = 5 -- so every node sees the same work as in the full workload."""
+    Ls = L / 4
+    fs = curves.random_tangle(78, 200, L=Ls, rmin=Ls / 8, rmax=Ls / 4, seed=seed)
+    rcut = Ls / 4
+    p = ParamsBiotSavart(Gamma=1.0, a=1e-8, Delta=0.25,
+                         splitting=GaussianSplitting(Ls=Ls, alpha=4.0 / rcut, rcut=rcut, Ns=128),
+                         quadrature=GaussLegendre(3), backend_long=NonuniformFFTsBackend(1.5, 5), **kw)
+    return fs, p

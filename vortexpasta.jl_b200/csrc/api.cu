@@ -86,7 +86,7 @@ static int alloc_points(vpbs_handle* h, int64_t Np) {
     return 0;
 }
 
-static int process_point_charges(vpbs_handle* h) {
+int process_point_charges(vpbs_handle* h) {
     // process_point_charges! of both backends: cell lists (cell_lists.jl:117-127); the long-range
     // rescaling to [0, 2 pi) (longrange.jl:409-471) is folded into the NUFFT kernels.
     int rc = build_cell_lists(h);
@@ -258,7 +258,7 @@ int vpbs_destroy(vpbs_handle* h) {
                       &h->src_seg, &h->dst_cell, &h->dst_start, &h->dst_fill, &h->dst_order, &h->counters,
                       &h->grid_r, &h->grid_c, &h->grid_c2, &h->uhat, &h->decx, &h->decy, &h->decz, &h->nodes_lr,
                       &h->vel, &h->psi, &h->spread_bin, &h->spread_counts, &h->spread_start, &h->binned,
-                      &h->spread_foot, &h->ewald_tab, &h->scan_tmp, &h->scan_tmp_lr};
+                      &h->spread_foot, &h->ewald_tab, &h->scan_tmp, &h->scan_tmp_lr, &h->rk_vs, &h->rk_tmp};
     for (DevBuf* b : bufs) free_buf(*b);
     if (h->pin_in) cudaFreeHost(h->pin_in);
     if (h->pin_out) cudaFreeHost(h->pin_out);
@@ -316,6 +316,8 @@ int vpbs_set_filaments(vpbs_handle* h, int64_t nfil, const int64_t* offsets, con
     h->nfil = nfil;
     int64_t nmax = 0;
     for (int64_t f = 0; f < nfil; ++f) nmax = std::max<int64_t>(nmax, offsets[f + 1] - offsets[f]);
+    h->nmax = nmax;
+    h->have_filaments = true;
     if ((rc = geometry_from_filaments(h, nfil, (const int64_t*)h->offsets.p, d_nodes, nmax))) return rc;
     h->li_valid = h->K.lia_fraction > 0;
     return process_point_charges(h);
@@ -361,6 +363,7 @@ int vpbs_set_points(vpbs_handle* h, int64_t Np, vpbs_cvec3 nodes, const int32_t*
             return rc;
     if ((rc = check_cuda(h, cudaEventRecord(h->h2d_done, h->stream), "event record"))) return rc;
     h->li_valid = false;  // add_local_integrals! stays with the caller in the point-data contract
+    h->have_filaments = false;  // point data without a filament layout: no time stepping
     return process_point_charges(h);
 }
 

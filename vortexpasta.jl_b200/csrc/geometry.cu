@@ -108,11 +108,13 @@ __device__ void solve4(double H[4][4], double r[4][3]) {
 
 // One warp per filament.  Work space: 12 doubles per node (5 band + 7 right-hand sides), in
 // dynamic shared memory (smem_n doubles x 12 per warp) when smem_n > 0, else in `scratch`.
+// keep_knots: reuse the knots and periods already in `knots` / `periods` (the knots frozen
+// inside a time step, RK4.jl with update_coefficients!(f; knots = ts_base)).
 __global__ void __launch_bounds__(128) spline_solve_kernel(
     int64_t nfil, const int64_t* __restrict__ offsets, const double* __restrict__ X,
     double* __restrict__ knots, double* __restrict__ periods, int32_t* __restrict__ fil_of_node,
     double* __restrict__ coef, double* __restrict__ dcoef1, double* __restrict__ dcoef2,
-    double* __restrict__ scratch, int32_t* __restrict__ status, int smem_n) {
+    double* __restrict__ scratch, int32_t* __restrict__ status, int smem_n, int keep_knots) {
     extern __shared__ double sm_work[];
     const int lane = threadIdx.x & 31;
     const int64_t fidx = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -132,8 +134,8 @@ __global__ void __launch_bounds__(128) spline_solve_kernel(
     double* c2 = dcoef2 + 3 * off;
 
     // 1. chordal knots: warp-wide inclusive scan of segment lengths (parametrisations.jl:43-44)
-    double carry = 0.0;
-    for (int base = 0; base < n; base += 32) {
+    double carry = keep_knots ? periods[fidx] : 0.0;
+    for (int base = 0; base < n && !keep_knots; base += 32) {
         int i = base + lane;
         double len = 0.0;
         if (i < n) {
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(128) spline_solve_kernel(
         carry += __shfl_sync(0xffffffffu, incl, 31);
     }
     const double T = carry;
-    if (lane == 0) periods[fidx] = T;
+    if (lane == 0 && !keep_knots) periods[fidx] = T;
     __syncwarp();
     FilView f{t, T, n};
 
@@ -409,13 +411,17 @@ static int solve_smem_n(int64_t nmax, size_t* bytes) {
 }
 
 int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offsets, const double* d_nodes,
-                            int64_t nmax) {
+                            int64_t nmax, bool keep_knots) {
     const int64_t Np = h->Np;
     int rc;
     size_t smem_bytes = 0;
     const int smem_n = solve_smem_n(nmax, &smem_bytes);
-    if (smem_bytes > 48 * 1024)
-        cudaFuncSetAttribute(spline_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    // opt in to the exact size every time (a launch at exactly 48 KB also needs it, and the
+    // attribute is per function, not per handle)
+    if (smem_bytes > 0 &&
+        (rc = check_cuda(h, cudaFuncSetAttribute(spline_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem_bytes), "spline kernel shared memory")))
+        return rc;
     if ((rc = ensure(h, h->knots, sizeof(double) * (Np + nfil), "knots"))) return rc;
     if ((rc = ensure(h, h->fil_of_node, sizeof(int32_t) * Np, "fil_of_node"))) return rc;
     if ((rc = ensure(h, h->coefs, sizeof(double) * 3 * Np, "coefs"))) return rc;
@@ -429,7 +435,7 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
     if ((rc = check_cuda(h, cudaMemsetAsync(status, 0, sizeof(int32_t), h->stream), "memset"))) return rc;
     spline_solve_kernel<<<grid_for(nfil, 4), 128, smem_bytes, h->stream>>>(
         nfil, d_offsets, d_nodes, knots, periods, (int32_t*)h->fil_of_node.p, (double*)h->coefs.p,
-        (double*)h->dcoef1.p, (double*)h->dcoef2.p, (double*)h->spline_scratch.p, status, smem_n);
+        (double*)h->dcoef1.p, (double*)h->dcoef2.p, (double*)h->spline_scratch.p, status, smem_n, keep_knots ? 1 : 0);
     h->launches++;
     const bool want_li = h->K.lia_fraction > 0;
     point_data_kernel<<<grid_for(Np, 128), 128, 0, h->stream>>>(
@@ -550,7 +556,7 @@ extern "C" int vpbs_point_data_noalloc(const vpbs_params* params, int64_t nfil, 
     if (e != cudaSuccess)
         return set_error(nullptr, VPBS_ERR_CUDA, std::string("vpbs_point_data_noalloc: ") + cudaGetErrorString(e));
     spline_solve_kernel<<<grid_for(nfil, 4), 128, 0, s>>>(nfil, d_offsets, nodes_xyz, knots, periods, fil_of_node, coefs,
-                                                          dcoef1, dcoef2, scratch, status, 0);
+                                                          dcoef1, dcoef2, scratch, status, 0, 0);
     point_data_kernel<<<grid_for(Np, 128), 128, 0, s>>>(K, Np, d_offsets, fil_of_node, nodes_xyz, knots, periods, coefs,
                                                         dcoef1, dcoef2, nodes, node_idx_prev, deriv1, deriv2,
                                                         delta_minus, delta_plus, points, charges, nullptr, nullptr, 0);

@@ -75,12 +75,13 @@ __global__ void dense_input_grad_kernel(int n, int nin, int nout, const float* _
     dZprev[idx] = s * gelu_grad(Zprev[idx]);
 }
 
-// Adam (Kingma & Ba 2015) with bias correction; step t >= 1.
+// Adam (Kingma & Ba 2015) with bias correction on the loss plus (wd/2)|p|^2; step t >= 1.
 __global__ void adam_kernel(int np, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m1,
-                            float* __restrict__ m2, float lr, float b1, float b2, float eps, float c1, float c2) {
+                            float* __restrict__ m2, float lr, float b1, float b2, float eps, float c1, float c2,
+                            float wd) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
-    const float gi = g[i];
+    const float gi = g[i] + wd * p[i];
     const float a = b1 * m1[i] + (1.0f - b1) * gi;
     const float v = b2 * m2[i] + (1.0f - b2) * gi * gi;
     m1[i] = a;
@@ -96,6 +97,7 @@ struct vpbs_mlp {
     int device = 0;
     int max_batch = 0;
     int64_t steps = 0;
+    float weight_decay = 0.0f;
     std::string err;
     cudaStream_t stream = nullptr;
     float* params = nullptr;  // kNParams
@@ -238,6 +240,12 @@ int vpbs_mlp_set_loss_weights(vpbs_mlp* m, const float* w) {
     return rc;
 }
 
+int vpbs_mlp_set_weight_decay(vpbs_mlp* m, float wd) {
+    if (!m || !(wd >= 0.0f)) return mlp_err(m, VPBS_ERR_ARG, "weight decay must be >= 0");
+    m->weight_decay = wd;
+    return 0;
+}
+
 int vpbs_mlp_forward(vpbs_mlp* m, const float* X, int32_t n, float* Y) {
     if (!m || !X || !Y) return VPBS_ERR_ARG;
     int rc = mlp_cuda(m, cudaSetDevice(m->device), "cudaSetDevice");
@@ -270,7 +278,7 @@ int vpbs_mlp_train_step(vpbs_mlp* m, const float* X, const float* T, int32_t n, 
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.0f - std::pow(b1, (float)m->steps), c2 = 1.0f - std::pow(b2, (float)m->steps);
     adam_kernel<<<nblk(kNParams), 256, 0, m->stream>>>(kNParams, m->params, m->grad, m->m1, m->m2, lr, b1, b2, 1e-8f,
-                                                       c1, c2);
+                                                       c1, c2, m->weight_decay);
     rc = mlp_cuda(m, cudaGetLastError(), "Adam kernel");
     if (!rc && loss) {
         rc = mlp_cuda(m, cudaMemcpyAsync(loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream), "copy loss");

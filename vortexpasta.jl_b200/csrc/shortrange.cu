@@ -957,14 +957,18 @@ int pair_interactions(vpbs_handle* h, int fields) {
         const double per_cell = (double)Np / ncoarse;
         int nsm = 148;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+        auto fits = [&](int nb) {
+            const int w = nb + 2 * cg.M;
+            return w <= ncc && w <= cg.nc[1] && w <= cg.nc[2] && w * w <= kMaxRows && w * w * w * cg.G <= kMaxNbCells &&
+                   nb * nb <= kMaxBlockRows;
+        };
         int Bc = 1;
-        while (Bc * Bc * Bc * per_cell < 24.0) {
-            const int nb = Bc + 1, w = nb + 2 * cg.M;
-            const bool fits = w <= ncc && w <= cg.nc[1] && w <= cg.nc[2] && w * w <= kMaxRows &&
-                              w * w * w * cg.G <= kMaxNbCells && nb * nb <= kMaxBlockRows &&
-                              ncoarse / ((double)nb * nb * nb) >= 16.0 * nsm;
-            if (!fits) break;
-            Bc = nb;
+        if (h->pair_block > 0 && fits(h->pair_block)) {
+            Bc = h->pair_block;  // chosen by vpbs_autotune
+        } else {
+            while (Bc * Bc * Bc * per_cell < 24.0 && fits(Bc + 1) &&
+                   ncoarse / ((double)(Bc + 1) * (Bc + 1) * (Bc + 1)) >= 16.0 * nsm)
+                ++Bc;
         }
         const int3 bk = make_int3(Bc, Bc, Bc);
         const int3 nb = make_int3((ncc + Bc - 1) / Bc, (cg.nc[1] + Bc - 1) / Bc, (cg.nc[2] + Bc - 1) / Bc);

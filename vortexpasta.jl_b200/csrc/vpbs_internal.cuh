@@ -142,6 +142,13 @@ struct vpbs_handle {
     cudaEvent_t ev_fork = nullptr, ev_short = nullptr, ev_long = nullptr;
     cudaEvent_t interp_wait = nullptr;  // event the interpolation waits for (outputs are shared)
 
+    // time stepping (vpbs_rk4_step): filament layout of the last vpbs_set_filaments, RK buffers
+    int64_t nmax = 0;
+    bool have_filaments = false;
+    vpbs::DevBuf rk_vs, rk_tmp;
+    // pair-kernel cells per CTA edge chosen by vpbs_autotune (0: the built-in rule)
+    int pair_block = 0;
+
     // optional per-stage CUDA-event timing (vpbs_stage_timing)
     bool timing = false;
     cudaEvent_t tev[16][4][2] = {};  // [stage][occurrence][start/stop]
@@ -159,7 +166,10 @@ inline unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 
 
 // geometry.cu
 int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offsets, const double* d_nodes,
-                            int64_t nmax);  // nmax: largest node count of a filament
+                            int64_t nmax, bool keep_knots = false);  // nmax: largest node count of a filament
+
+// api.cu
+int process_point_charges(vpbs_handle* h);  // cell lists of the current point data
 
 // shortrange.cu
 int build_cell_lists(vpbs_handle* h);

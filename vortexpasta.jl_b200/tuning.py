@@ -124,11 +124,12 @@ def candidate_grid(L: float, rcut_fracs=(1 / 8, 1 / 12, 1 / 16, 1 / 20, 1 / 24, 
     return out
 
 
-def measure(fs, choice: EwaldChoice, L: float, precision: str = "mixed", reps: int = 2, fields: int = _lib.VELOCITY):
+def measure(fs, choice: EwaldChoice, L: float, precision: str = "mixed", reps: int = 2, fields: int = _lib.VELOCITY,
+            device: int = 0):
     """Device time (ms, best of `reps`, every stage from the geometry to the interpolation, run
     one after another) of one evaluation with `choice`, and the node velocities."""
     from .biotsavart import init_cache
-    cache = init_cache(choice.params(L, precision))
+    cache = init_cache(choice.params(L, precision, device=device))
     try:
         cache.set_filaments(fs)
         cache.compute(fields)
@@ -146,11 +147,12 @@ def measure(fs, choice: EwaldChoice, L: float, precision: str = "mixed", reps: i
     return best, v
 
 
-def sweep(fs, L: float, vref: np.ndarray, choices, precision: str = "mixed", reps: int = 2) -> list[dict]:
+def sweep(fs, L: float, vref: np.ndarray, choices, precision: str = "mixed", reps: int = 2,
+          device: int = 0) -> list[dict]:
     """(parameters, cost, error) records of `choices` on the configuration `fs`."""
     recs = []
     for ch in choices:
-        ms, v = measure(fs, ch, L, precision, reps)
+        ms, v = measure(fs, ch, L, precision, reps, device=device)
         l2, mx = rel_errors(v, vref)
         recs.append({**ch.as_dict(), "fft": ch.fft_size(), "beta_short": ch.beta_short, "beta_long": ch.beta_long(L),
                      "ms": ms, "rel_l2": l2, "max_err": mx})
