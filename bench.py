@@ -454,6 +454,42 @@ def cpu_sample(vp, workload):
     return fs, p, (f"full velocity evaluations of {workload}, best taken (CPU FP64 restatement, OpenMP)")
 
 
+KERNEL_CASES = {
+    "pairs1m": "pair kernel of tangle1m (r_cut = L/16, beta = 4) with a 64^3 Fourier grid, FP64 then mixed",
+    "tuned500k": "2500 rings x 200 nodes (500k nodes) at the tuned 1M parameters (alpha = 22.03, r_cut = 0.1561, "
+                 "Ns = 341, sigma = 1.5, m = 3), mixed precision",
+}
+
+
+def run_kernel_case(args):
+    """Small fixed workloads for kernel profiling (three evaluations each, stage times printed)."""
+    vp = load_package()
+    from vortexpasta_b200 import _lib, tuning
+    L = 2 * math.pi
+    cases = []
+    if args.kernel_case == "pairs1m":
+        fs = vp.configs.tangle(5000, 200, 42)
+        cases = [("fp64", vp.configs.params_for(L / 16, 4.0, 64, 5)),
+                 ("mixed", vp.configs.params_for(L / 16, 4.0, 64, 5, precision="mixed"))]
+    else:
+        fs = vp.configs.tangle(2500, 200, 42)
+        ch = tuning.EwaldChoice(alpha=22.0286100737363, rcut=0.15608485585182466, Ns=341, sigma=1.5, m=3)
+        cases = [("mixed", ch.params(L, "mixed"))]
+    for name, p in cases:
+        c = vp.init_cache(p)
+        try:
+            c.set_filaments(fs)
+            c.stage_timing(True)
+            for _ in range(3):
+                c.compute(_lib.VELOCITY)
+                st = c.stage_times()
+            print(json.dumps({"case": args.kernel_case, "form": name, "stages_ms": st,
+                              "pairs": list(c.pair_counts())}), flush=True)
+        finally:
+            c.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -468,9 +504,13 @@ def main():
     ap.add_argument("--no-tuned", dest="tuned", action="store_false",
                     help="skip the tuned form (learned parameters); the headline is then the plain FP64 form")
     ap.add_argument("--rtol", type=float, default=1e-5, help="accuracy target of the tuned form")
+    ap.add_argument("--kernel-case", choices=sorted(KERNEL_CASES), default=None,
+                    help="run a small fixed workload for kernel profiling instead of the benchmark")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.kernel_case:
+        return run_kernel_case(args)
     return run_reference(args) if args.impl == "reference" else run_ours(args)
 
 
