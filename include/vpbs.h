@@ -132,6 +132,25 @@ int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t short
  * handle's stream. */
 int vpbs_get(vpbs_handle* h, int32_t field, double* out_xyz, int32_t accumulate);
 
+/* Per-filament variants for hosts that keep one array per filament (the reference's
+ * Vector of filaments): vpbs_set_filament_list takes nfil host pointers to AoS [counts[f]][3]
+ * node arrays (same semantics as vpbs_set_filaments with on_device = 0); vpbs_get_filament_list
+ * writes a computed field into nfil host AoS arrays laid out like the filaments of the last
+ * vpbs_set_filaments / vpbs_set_filament_list.  Both copy through pinned staging with up to 8
+ * host threads. */
+int vpbs_set_filament_list(vpbs_handle* h, int64_t nfil, const double* const* nodes, const int64_t* counts);
+int vpbs_get_filament_list(vpbs_handle* h, int32_t field, double* const* out, int64_t nfil);
+
+/* Staging without an intermediate copy, for hosts that assemble the inputs themselves:
+ * vpbs_stage_filaments returns pinned host buffers for nfil+1 offsets and 3 Np AoS node
+ * coordinates (valid until the next staging call on h) that the caller fills; then
+ * vpbs_set_staged_filaments(h, nfil) proceeds as vpbs_set_filaments with host nodes.
+ * vpbs_get_staged returns a pinned AoS [Np][3] copy of a computed field (node order), valid until
+ * the next call on h.  Both synchronise the handle's stream as needed. */
+int vpbs_stage_filaments(vpbs_handle* h, int64_t nfil, int64_t Np, int64_t** offsets, double** nodes);
+int vpbs_set_staged_filaments(vpbs_handle* h, int64_t nfil);
+int vpbs_get_staged(vpbs_handle* h, int32_t field, const double** aos);
+
 /* Same as vpbs_get but into SoA host arrays. */
 int vpbs_get_soa(vpbs_handle* h, int32_t field, vpbs_vec3 out, int32_t accumulate);
 

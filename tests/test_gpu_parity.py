@@ -208,3 +208,36 @@ def test_spline_solve_at_exactly_48k_shared_memory(vp):
     finally:
         c.close()
     assert np.isfinite(v).all() and np.abs(v).max() > 0
+
+
+@pytest.mark.gpu
+def test_host_entry_points_agree(vp):
+    """Staged list input (velocity_on_nodes), the flat host-buffer call and the per-filament
+    pointer-list C entry points give the same velocities."""
+    import ctypes as ct
+    from vortexpasta_b200 import _lib
+    fs, p = vp.configs.tangle20k()
+    fs = fs[:40]
+    c = vp.init_cache(p)
+    try:
+        v_list = np.concatenate(vp.velocity_on_nodes(c, fs))
+        nodes, offsets = vp.curves.concat(fs)
+        c.set_filaments_flat(nodes, offsets)
+        c.compute(_lib.VELOCITY)
+        v_flat = c.get(_lib.VELOCITY)
+        lib = _lib.load()
+        fsc = [np.ascontiguousarray(f, dtype=np.float64) for f in fs]
+        ptrs = (ct.c_void_p * len(fsc))(*[f.ctypes.data for f in fsc])
+        counts = np.array([len(f) for f in fsc], dtype=np.int64)
+        _lib.check(lib.vpbs_set_filament_list(c.handle, len(fsc), ptrs, counts.ctypes.data_as(_lib.c_int64_p)),
+                   c.handle, "set_filament_list")
+        c.compute(_lib.VELOCITY)
+        outs = [np.zeros_like(f) for f in fsc]
+        optr = (ct.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
+        _lib.check(lib.vpbs_get_filament_list(c.handle, _lib.VELOCITY, optr, len(outs)), c.handle,
+                   "get_filament_list")
+        v_ptr = np.concatenate(outs)
+    finally:
+        c.close()
+    assert np.abs(v_flat - v_list).max() <= 1e-13 * np.abs(v_list).max()
+    assert np.abs(v_ptr - v_list).max() <= 1e-13 * np.abs(v_list).max()

@@ -67,6 +67,12 @@ SIGNATURES = {
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "vpbs_features": (ct.c_int, [ct.c_void_p, c_float_p, ct.c_int32]),
+    "vpbs_set_filament_list": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_void_p, c_int64_p]),
+    "vpbs_stage_filaments": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int64, ct.POINTER(c_int64_p),
+                                        ct.POINTER(c_double_p)]),
+    "vpbs_set_staged_filaments": (ct.c_int, [ct.c_void_p, ct.c_int64]),
+    "vpbs_get_staged": (ct.c_int, [ct.c_void_p, ct.c_int32, ct.POINTER(c_double_p)]),
+    "vpbs_get_filament_list": (ct.c_int, [ct.c_void_p, ct.c_int32, ct.c_void_p, ct.c_int64]),
     "vpbs_rk4_step": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_double]),
     "vpbs_ensemble_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_void_p), c_double_p, ct.c_int32,
                                         ct.POINTER(ct.c_void_p)]),

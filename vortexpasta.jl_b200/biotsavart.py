@@ -100,12 +100,22 @@ class BiotSavartCache:
         _lib.check(self._lib.vpbs_set_stream(self._h, ct.c_void_p(stream_ptr or 0)), self._h, "set_stream")
 
     def set_filaments(self, fs, on_device_ptr: int | None = None, offsets=None):
-        """add_point_charges! on the device. `fs`: list of (N, 3) arrays, or None with a device
-        pointer to AoS nodes plus host `offsets`."""
+        """add_point_charges! on the device. `fs`: list of (N, 3) arrays (assembled straight into
+        the handle's pinned staging buffer), or None with a device pointer to AoS nodes plus host
+        `offsets`."""
         if on_device_ptr is None:
-            nodes, offsets = concat(fs)
-            rc = self._lib.vpbs_set_filaments(self._h, len(offsets) - 1, offsets.ctypes.data_as(_lib.c_int64_p),
-                                              nodes.ctypes.data_as(ct.c_void_p), 0)
+            n = len(fs)
+            counts = np.fromiter(map(len, fs), dtype=np.int64, count=n)
+            Np = int(counts.sum())
+            po, pn = _lib.c_int64_p(), _lib.c_double_p()
+            _lib.check(self._lib.vpbs_stage_filaments(self._h, n, Np, ct.byref(po), ct.byref(pn)), self._h,
+                       "add_point_charges!")
+            off = np.ctypeslib.as_array(po, shape=(n + 1,))
+            off[0] = 0
+            np.cumsum(counts, out=off[1:])
+            np.concatenate(fs, axis=0, out=np.ctypeslib.as_array(pn, shape=(Np, 3)))
+            offsets = off.copy()
+            rc = self._lib.vpbs_set_staged_filaments(self._h, n)
         else:
             offsets = np.ascontiguousarray(offsets, dtype=np.int64)
             rc = self._lib.vpbs_set_filaments(self._h, len(offsets) - 1, offsets.ctypes.data_as(_lib.c_int64_p),
@@ -113,6 +123,27 @@ class BiotSavartCache:
         _lib.check(rc, self._h, "add_point_charges!")
         self.Np = int(offsets[-1])
         self._offsets = np.asarray(offsets)
+
+    def set_filaments_flat(self, nodes: np.ndarray, offsets: np.ndarray):
+        """add_point_charges! from one host AoS array [Np][3] and filament offsets (the flat C-ABI
+        call vpbs_set_filaments with host nodes)."""
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        rc = self._lib.vpbs_set_filaments(self._h, len(offsets) - 1, offsets.ctypes.data_as(_lib.c_int64_p),
+                                          nodes.ctypes.data_as(ct.c_void_p), 0)
+        _lib.check(rc, self._h, "add_point_charges!")
+        self.Np = int(offsets[-1])
+        self._offsets = offsets
+
+    def get_list(self, field_mask: int, outs) -> None:
+        """Copy a computed field into per-filament host arrays laid out like the last filaments."""
+        p = _lib.c_double_p()
+        _lib.check(self._lib.vpbs_get_staged(self._h, field_mask, ct.byref(p)), self._h,
+                   "copy_output_values_on_nodes!")
+        flat = np.ctypeslib.as_array(p, shape=(self.Np, 3))
+        off = self._offsets.tolist()
+        for k, u in enumerate(outs):
+            u[...] = flat[off[k]:off[k + 1]]
 
     def compute(self, fields_mask: int, lia_mode: int = _lib.LIA_TRUE, shortrange=True, longrange=True,
                 integration_cutoff=None):
@@ -234,10 +265,7 @@ def compute_on_nodes_(fields: dict, cache: BiotSavartCache, fs, *, LIA=True, sho
         callback_vorticity(cache)
     for name, bit in (("velocity", _lib.VELOCITY), ("streamfunction", _lib.STREAMFUNCTION)):
         if name in names:
-            flat = cache.get(bit)
-            off = cache._offsets
-            for k, u in enumerate(fields[name]):
-                u[...] = flat[off[k]:off[k + 1]]
+            cache.get_list(bit, fields[name])
     return fields
 
 

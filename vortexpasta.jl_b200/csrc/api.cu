@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "vpbs_internal.cuh"
@@ -282,9 +283,69 @@ int vpbs_set_stream(vpbs_handle* h, void* stream) {
     return 0;
 }
 
-int vpbs_set_filaments(vpbs_handle* h, int64_t nfil, const int64_t* offsets, const double* nodes_xyz, int32_t on_device) {
-    if (!h) return VPBS_ERR_ARG;
-    if (nfil < 1 || !offsets || !nodes_xyz) return set_error(h, VPBS_ERR_ARG, "vpbs_set_filaments: bad arguments");
+}  // extern "C"
+
+namespace vpbs {
+
+// Copies `n` blocks (dst[k] <- src[k], bytes[k]) with up to 8 host threads (large inputs only):
+// the staging of filament lists into and out of pinned memory is bound by host memory copies.
+static void parallel_copies(int64_t n, void* const* dst, const void* const* src, const size_t* bytes) {
+    size_t total = 0;
+    for (int64_t k = 0; k < n; ++k) total += bytes[k];
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int T = (int)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, total >> 21));  // >= 2 MB per thread
+    auto work = [&](int64_t a, int64_t b) {
+        for (int64_t k = a; k < b; ++k) std::memcpy(dst[k], src[k], bytes[k]);
+    };
+    if (T <= 1) {
+        work(0, n);
+        return;
+    }
+    // split the blocks into T ranges of about equal bytes
+    std::vector<int64_t> cut(T + 1, n);
+    cut[0] = 0;
+    size_t acc = 0;
+    int t = 1;
+    for (int64_t k = 0; k < n && t < T; ++k) {
+        acc += bytes[k];
+        if (acc >= total * t / T) cut[t++] = k + 1;
+    }
+    std::vector<std::thread> pool;
+    for (int i = 0; i < T; ++i)
+        if (cut[i] < cut[i + 1]) pool.emplace_back(work, cut[i], cut[i + 1]);
+    for (auto& th : pool) th.join();
+}
+
+// Shared tail of the filament entry points: offsets (host) are staged in pin_in[0..), the nodes
+// either already sit in pin_in after the offsets (host input) or in device memory (d_nodes).
+static int set_filaments_staged(vpbs_handle* h, int64_t nfil, const int64_t* offsets, const double* d_nodes) {
+    int rc;
+    const int64_t Np = offsets[nfil];
+    const size_t bytes_off = sizeof(int64_t) * (nfil + 1);
+    if ((rc = check_cuda(h, cudaMemcpyAsync(h->offsets.p, h->pin_in, bytes_off, cudaMemcpyHostToDevice, h->stream),
+                         "H2D offsets")))
+        return rc;
+    if (!d_nodes) {
+        if ((rc = check_cuda(h, cudaMemcpyAsync(h->nodes_in.p, (char*)h->pin_in + bytes_off, sizeof(double) * 3 * Np,
+                                                cudaMemcpyHostToDevice, h->stream), "H2D nodes")))
+            return rc;
+        d_nodes = (const double*)h->nodes_in.p;
+    }
+    if ((rc = check_cuda(h, cudaEventRecord(h->h2d_done, h->stream), "event record"))) return rc;
+    h->nfil = nfil;
+    h->host_offsets.assign(offsets, offsets + nfil + 1);
+    int64_t nmax = 0;
+    for (int64_t f = 0; f < nfil; ++f) nmax = std::max<int64_t>(nmax, offsets[f + 1] - offsets[f]);
+    h->nmax = nmax;
+    h->have_filaments = true;
+    if ((rc = geometry_from_filaments(h, nfil, (const int64_t*)h->offsets.p, d_nodes, nmax))) return rc;
+    h->li_valid = h->K.lia_fraction > 0;
+    return process_point_charges(h);
+}
+
+// Checks, allocation and pinned staging common to both filament entry points; on success the
+// offsets are in pin_in and room for 3 Np host doubles follows them when host_nodes.
+static int prepare_filaments(vpbs_handle* h, int64_t nfil, const int64_t* offsets, bool host_nodes) {
     if (offsets[0] != 0) return set_error(h, VPBS_ERR_ARG, "offsets[0] must be 0");
     for (int64_t f = 0; f < nfil; ++f)
         if (offsets[f + 1] - offsets[f] < 5)
@@ -295,32 +356,79 @@ int vpbs_set_filaments(vpbs_handle* h, int64_t nfil, const int64_t* offsets, con
     if ((rc = activate(h))) return rc;
     if ((rc = alloc_points(h, Np))) return rc;
     if ((rc = ensure(h, h->offsets, sizeof(int64_t) * (nfil + 1), "offsets"))) return rc;
-    // stage offsets (+ nodes from the host) through pinned memory
     const size_t bytes_off = sizeof(int64_t) * (nfil + 1);
-    const size_t bytes_nodes = on_device ? 0 : sizeof(double) * 3 * Np;
+    const size_t bytes_nodes = host_nodes ? sizeof(double) * 3 * Np : 0;
+    if (host_nodes && (rc = ensure(h, h->nodes_in, bytes_nodes, "input nodes"))) return rc;
     if ((rc = check_cuda(h, cudaEventSynchronize(h->h2d_done), "event sync"))) return rc;
     if ((rc = ensure_pinned(h, &h->pin_in, &h->pin_in_bytes, bytes_off + bytes_nodes))) return rc;
-    std::memcpy(h->pin_in, offsets, bytes_off);
-    if ((rc = check_cuda(h, cudaMemcpyAsync(h->offsets.p, h->pin_in, bytes_off, cudaMemcpyHostToDevice, h->stream), "H2D offsets")))
-        return rc;
-    const double* d_nodes = nodes_xyz;
-    if (!on_device) {
-        if ((rc = ensure(h, h->nodes_in, bytes_nodes, "input nodes"))) return rc;
-        char* dst = (char*)h->pin_in + bytes_off;
-        std::memcpy(dst, nodes_xyz, bytes_nodes);
-        if ((rc = check_cuda(h, cudaMemcpyAsync(h->nodes_in.p, dst, bytes_nodes, cudaMemcpyHostToDevice, h->stream), "H2D nodes")))
-            return rc;
-        d_nodes = (const double*)h->nodes_in.p;
+    if (offsets != (const int64_t*)h->pin_in) std::memcpy(h->pin_in, offsets, bytes_off);
+    return 0;
+}
+
+}  // namespace vpbs
+
+extern "C" {
+
+int vpbs_set_filaments(vpbs_handle* h, int64_t nfil, const int64_t* offsets, const double* nodes_xyz, int32_t on_device) {
+    if (!h) return VPBS_ERR_ARG;
+    if (nfil < 1 || !offsets || !nodes_xyz) return set_error(h, VPBS_ERR_ARG, "vpbs_set_filaments: bad arguments");
+    int rc;
+    if ((rc = prepare_filaments(h, nfil, offsets, !on_device))) return rc;
+    if (on_device) return set_filaments_staged(h, nfil, offsets, nodes_xyz);
+    const size_t bytes_off = sizeof(int64_t) * (nfil + 1);
+    const void* src[1] = {nodes_xyz};
+    void* dst[1] = {(char*)h->pin_in + bytes_off};
+    const size_t bytes[1] = {sizeof(double) * 3 * offsets[nfil]};
+    parallel_copies(1, dst, src, bytes);
+    return set_filaments_staged(h, nfil, offsets, nullptr);
+}
+
+int vpbs_stage_filaments(vpbs_handle* h, int64_t nfil, int64_t Np, int64_t** offsets, double** nodes) {
+    if (!h) return VPBS_ERR_ARG;
+    if (nfil < 1 || Np < 0 || !offsets || !nodes) return set_error(h, VPBS_ERR_ARG, "vpbs_stage_filaments: bad arguments");
+    int rc;
+    if ((rc = activate(h))) return rc;
+    if ((rc = check_cuda(h, cudaEventSynchronize(h->h2d_done), "event sync"))) return rc;
+    const size_t bytes_off = sizeof(int64_t) * (nfil + 1);
+    if ((rc = ensure_pinned(h, &h->pin_in, &h->pin_in_bytes, bytes_off + sizeof(double) * 3 * Np))) return rc;
+    *offsets = (int64_t*)h->pin_in;
+    *nodes = (double*)((char*)h->pin_in + bytes_off);
+    return 0;
+}
+
+int vpbs_set_staged_filaments(vpbs_handle* h, int64_t nfil) {
+    if (!h) return VPBS_ERR_ARG;
+    if (nfil < 1 || !h->pin_in) return set_error(h, VPBS_ERR_STATE, "vpbs_set_staged_filaments: nothing staged");
+    const int64_t* offsets = (const int64_t*)h->pin_in;
+    if ((size_t)(sizeof(int64_t) * (nfil + 1)) > h->pin_in_bytes ||
+        sizeof(int64_t) * (nfil + 1) + sizeof(double) * 3 * (size_t)std::max<int64_t>(offsets[nfil], 0) > h->pin_in_bytes)
+        return set_error(h, VPBS_ERR_ARG, "vpbs_set_staged_filaments: staged sizes exceed the staging buffer");
+    int rc;
+    if ((rc = prepare_filaments(h, nfil, offsets, true))) return rc;
+    return set_filaments_staged(h, nfil, offsets, nullptr);
+}
+
+int vpbs_set_filament_list(vpbs_handle* h, int64_t nfil, const double* const* nodes, const int64_t* counts) {
+    if (!h) return VPBS_ERR_ARG;
+    if (nfil < 1 || !nodes || !counts) return set_error(h, VPBS_ERR_ARG, "vpbs_set_filament_list: bad arguments");
+    std::vector<int64_t> offsets(nfil + 1, 0);
+    for (int64_t f = 0; f < nfil; ++f) {
+        if (!nodes[f]) return set_error(h, VPBS_ERR_ARG, "vpbs_set_filament_list: null filament");
+        offsets[f + 1] = offsets[f] + counts[f];
     }
-    if ((rc = check_cuda(h, cudaEventRecord(h->h2d_done, h->stream), "event record"))) return rc;
-    h->nfil = nfil;
-    int64_t nmax = 0;
-    for (int64_t f = 0; f < nfil; ++f) nmax = std::max<int64_t>(nmax, offsets[f + 1] - offsets[f]);
-    h->nmax = nmax;
-    h->have_filaments = true;
-    if ((rc = geometry_from_filaments(h, nfil, (const int64_t*)h->offsets.p, d_nodes, nmax))) return rc;
-    h->li_valid = h->K.lia_fraction > 0;
-    return process_point_charges(h);
+    int rc;
+    if ((rc = prepare_filaments(h, nfil, offsets.data(), true))) return rc;
+    double* base = (double*)((char*)h->pin_in + sizeof(int64_t) * (nfil + 1));
+    std::vector<void*> dst(nfil);
+    std::vector<const void*> src(nfil);
+    std::vector<size_t> bytes(nfil);
+    for (int64_t f = 0; f < nfil; ++f) {
+        dst[f] = base + 3 * offsets[f];
+        src[f] = nodes[f];
+        bytes[f] = sizeof(double) * 3 * counts[f];
+    }
+    parallel_copies(nfil, dst.data(), src.data(), bytes.data());
+    return set_filaments_staged(h, nfil, offsets.data(), nullptr);
 }
 
 int vpbs_set_points(vpbs_handle* h, int64_t Np, vpbs_cvec3 nodes, const int32_t* node_idx_prev, vpbs_cvec3 deriv1,
@@ -418,6 +526,18 @@ int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t short
     return 0;
 }
 
+}  // extern "C"
+
+namespace vpbs {
+// SoA [3][Np] -> AoS [Np][3] (the node-order layout of the host output arrays)
+__global__ void soa_to_aos_kernel(int64_t Np, const double* __restrict__ src, double* __restrict__ dst) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 3 * Np) dst[i] = src[(i % 3) * Np + i / 3];
+}
+}  // namespace vpbs
+
+extern "C" {
+
 static int fetch_soa(vpbs_handle* h, int32_t field, const double** out) {
     if (field != VPBS_VELOCITY && field != VPBS_STREAMFUNCTION) return set_error(h, VPBS_ERR_ARG, "bad field");
     if (!(h->last_fields & field)) return set_error(h, VPBS_ERR_STATE, "field was not computed");
@@ -432,20 +552,70 @@ static int fetch_soa(vpbs_handle* h, int32_t field, const double** out) {
     return 0;
 }
 
+// Device transpose of a computed field to AoS, D2H into pinned memory; returns the pinned copy.
+static int fetch_aos(vpbs_handle* h, int32_t field, const double** out) {
+    if (field != VPBS_VELOCITY && field != VPBS_STREAMFUNCTION) return set_error(h, VPBS_ERR_ARG, "bad field");
+    if (!(h->last_fields & field)) return set_error(h, VPBS_ERR_STATE, "field was not computed");
+    int rc;
+    if ((rc = activate(h))) return rc;
+    const int64_t Np = h->Np;
+    const size_t bytes = sizeof(double) * 3 * Np;
+    if ((rc = ensure(h, h->aos_out, bytes, "AoS output staging"))) return rc;
+    if ((rc = ensure_pinned(h, &h->pin_out, &h->pin_out_bytes, bytes))) return rc;
+    soa_to_aos_kernel<<<grid_for(3 * Np, 256), 256, 0, h->stream>>>(
+        Np, (const double*)(field == VPBS_VELOCITY ? h->vel.p : h->psi.p), (double*)h->aos_out.p);
+    h->launches++;
+    if ((rc = check_cuda(h, cudaGetLastError(), "AoS kernel"))) return rc;
+    if ((rc = check_cuda(h, cudaMemcpyAsync(h->pin_out, h->aos_out.p, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H")))
+        return rc;
+    if ((rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync"))) return rc;
+    *out = (const double*)h->pin_out;
+    return 0;
+}
+
 int vpbs_get(vpbs_handle* h, int32_t field, double* out_xyz, int32_t accumulate) {
     if (!h) return VPBS_ERR_ARG;
     if (!out_xyz) return set_error(h, VPBS_ERR_ARG, "null output");
     const double* s;
-    int rc = fetch_soa(h, field, &s);
+    int rc = fetch_aos(h, field, &s);
     if (rc) return rc;
-    const int64_t Np = h->Np;
+    const int64_t n = 3 * h->Np;
     if (accumulate) {
-        for (int64_t i = 0; i < Np; ++i)
-            for (int d = 0; d < 3; ++d) out_xyz[3 * i + d] += s[d * Np + i];
+        for (int64_t i = 0; i < n; ++i) out_xyz[i] += s[i];
     } else {
-        for (int64_t i = 0; i < Np; ++i)
-            for (int d = 0; d < 3; ++d) out_xyz[3 * i + d] = s[d * Np + i];
+        void* dst[1] = {out_xyz};
+        const void* src[1] = {s};
+        const size_t nb[1] = {sizeof(double) * n};
+        parallel_copies(1, dst, src, nb);
     }
+    return 0;
+}
+
+int vpbs_get_staged(vpbs_handle* h, int32_t field, const double** aos) {
+    if (!h) return VPBS_ERR_ARG;
+    if (!aos) return set_error(h, VPBS_ERR_ARG, "null output pointer");
+    return fetch_aos(h, field, aos);
+}
+
+int vpbs_get_filament_list(vpbs_handle* h, int32_t field, double* const* out, int64_t nfil) {
+    if (!h) return VPBS_ERR_ARG;
+    if (!out) return set_error(h, VPBS_ERR_ARG, "null output list");
+    if (!h->have_filaments || nfil != h->nfil || (int64_t)h->host_offsets.size() != nfil + 1)
+        return set_error(h, VPBS_ERR_STATE, "output list does not match the filaments of the last vpbs_set_filaments");
+    const double* s;
+    int rc = fetch_aos(h, field, &s);
+    if (rc) return rc;
+    std::vector<void*> dst(nfil);
+    std::vector<const void*> src(nfil);
+    std::vector<size_t> nb(nfil);
+    const int64_t* off = h->host_offsets.data();
+    for (int64_t f = 0; f < nfil; ++f) {
+        if (!out[f]) return set_error(h, VPBS_ERR_ARG, "null filament output");
+        dst[f] = out[f];
+        src[f] = s + 3 * off[f];
+        nb[f] = sizeof(double) * 3 * (off[f + 1] - off[f]);
+    }
+    parallel_copies(nfil, dst.data(), src.data(), nb.data());
     return 0;
 }
 

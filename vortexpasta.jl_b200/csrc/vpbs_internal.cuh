@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "vpbs.h"
 
@@ -141,6 +142,9 @@ struct vpbs_handle {
     cudaStream_t aux_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_short = nullptr, ev_long = nullptr;
     cudaEvent_t interp_wait = nullptr;  // event the interpolation waits for (outputs are shared)
+
+    std::vector<int64_t> host_offsets;  // filament layout of the last vpbs_set_filaments (host copy)
+    vpbs::DevBuf aos_out;                 // AoS staging of an output field (vpbs_get_filaments)
 
     // time stepping (vpbs_rk4_step): filament layout of the last vpbs_set_filaments, RK buffers
     int64_t nmax = 0;
