@@ -346,6 +346,73 @@ def errors_vs(v, vref):
             "max_err_vs_fp64": float(np.abs(v - vref).max() / np.abs(vref).max())}
 
 
+def ensemble_systems(vp, nsys=64, seed=64):
+    """The batching-form ensemble: `nsys` random tangles (200-node rings) with node counts
+    log-uniform in [2k, 200k], grid Ns = nearest power of two to N^(1/3) * 4 clamped to [64, 256],
+    beta = 3.5 (alpha and r_cut from the reference's rule), mixed precision.  Time step:
+    min(1e-3 L^2 / Gamma, Kelvin-wave period of the shortest segment) -- the fixed 1e-3 L^2/Gamma
+    alone is ~650x above that stability limit and the tangles blow up within a few steps."""
+    from vortexpasta_b200.params import (GaussianSplitting, GaussLegendre, NonuniformFFTsBackend, ParamsBiotSavart,
+                                         kelvin_wave_period)
+    L = 2 * math.pi
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(nsys):
+        N = 10 ** rng.uniform(math.log10(2000), math.log10(200000))
+        nrings = max(10, int(round(N / 200)))
+        fs = vp.curves.random_tangle(nrings, 200, L=L, seed=int(rng.integers(1 << 31)))
+        Ns = int(min(256, max(64, 2 ** round(math.log2(N ** (1 / 3) * 4)))))
+        p = ParamsBiotSavart(Gamma=1.0, a=1e-8, Delta=0.25, splitting=GaussianSplitting(Ls=L, beta=3.5, Ns=Ns),
+                             quadrature=GaussLegendre(3), backend_long=NonuniformFFTsBackend(1.5, 4), precision="mixed")
+        dmin = min(float(np.linalg.norm(np.roll(f, -1, axis=0) - f, axis=1).min()) for f in fs)
+        dt = min(1e-3 * L ** 2 / 1.0, kelvin_wave_period(dmin, a=1e-8, Delta=0.25, Gamma=1.0))
+        out.append((fs, p, dt))
+    return out
+
+
+def measure_ensemble(vp, args, local_rank):
+    """RK4 steps of the whole ensemble replayed as one CUDA graph per step, against the same
+    steps issued system by system without a graph."""
+    import torch
+    from vortexpasta_b200 import timestepping
+    systems = ensemble_systems(vp)
+    nodes = sum(sum(len(f) for f in fs) for fs, _, _ in systems)
+    t0 = time.perf_counter()
+    ens = timestepping.Ensemble([(fs, p.with_(device=local_rank), dt) for fs, p, dt in systems], device=local_rank,
+                                autotune_pairs=True)
+    t_setup = time.perf_counter() - t0
+    try:
+        stream = torch.cuda.ExternalStream(ens.stream(), device=local_rank)
+        ens.step(2)  # warm-up replays
+        ens.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ens.step(args.ensemble_steps)
+        e1.record(stream)
+        ens.synchronize()
+        ms_graph = e0.elapsed_time(e1)
+        # the same steps, system by system, no graph (host wall clock around a synchronised loop)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(args.ensemble_steps):
+            for c, x, (_, _, dt) in zip(ens.caches, ens.nodes, systems):
+                timestepping.rk4_step(c, x.data_ptr(), dt)
+        torch.cuda.synchronize()
+        ms_seq = (time.perf_counter() - t1) * 1e3
+        finite = all(bool(torch.isfinite(x).all()) for x in ens.nodes)
+    finally:
+        ens.close()
+    evals = 4 * nodes * args.ensemble_steps
+    return {"systems": len(systems), "nodes_total": nodes, "rk4_steps": args.ensemble_steps,
+            "node_velocities_per_s": evals / (ms_graph * 1e-3), "ms_per_step": ms_graph / args.ensemble_steps,
+            "sequential_node_velocities_per_s": evals / (ms_seq * 1e-3), "graph_speedup": ms_seq / ms_graph,
+            "pair_blocks_autotuned": ens.tuned, "setup_s": t_setup, "finite": finite,
+            "description": "64 random tangles, N log-uniform in [2k, 200k] (200-node rings), Ns = nearest power of "
+                           "two to N^(1/3)*4 in [64, 256], beta = 3.5, mixed precision, RK4 with dt = min(1e-3 L^2/Gamma, "
+                           "Kelvin-wave period of the shortest segment); one CUDA graph launch per RK4 step (all "
+                           "systems, one stream each), vs the same steps issued system by system"}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -434,6 +501,8 @@ def run_ours(args):
             "clocks": head["clk"].summary(),
             "pairs_in_range": fh["pairs_in_range"],
         }
+        if world == 1 and args.ensemble_steps > 0:
+            line["ensemble"] = measure_ensemble(vp, args, local_rank)
         if world == 1 and not args.no_cpu_baseline:
             cores = host_cores()
             sfs, sp, desc = cpu_sample(vp, args.workload)
@@ -510,6 +579,8 @@ def main():
     ap.add_argument("--no-tuned", dest="tuned", action="store_false",
                     help="skip the tuned form (learned parameters); the headline is then the plain FP64 form")
     ap.add_argument("--rtol", type=float, default=1e-5, help="accuracy target of the tuned form")
+    ap.add_argument("--ensemble-steps", type=int, default=20,
+                    help="RK4 steps of the batching-form ensemble reported under 'ensemble' (0: skip)")
     ap.add_argument("--kernel-case", choices=sorted(KERNEL_CASES), default=None,
                     help="run a small fixed workload for kernel profiling instead of the benchmark")
     args = ap.parse_args()

@@ -47,9 +47,16 @@ static inline void cross3(const double* u, const double* v, double* w) {
 
 static inline int is_open(const vpo_params* p) { return !(p->L[0] > 0 && p->L[1] > 0 && p->L[2] > 0); }
 
-/* Fold into [0, L).  reference: src/Filaments/min_distance.jl:5-20 */
+/* Fold into [0, L).  reference: src/Filaments/min_distance.jl:5-20 (subtraction loops within
+ * four periods; one exact fmod beyond, so a huge or non-finite coordinate cannot loop) */
 static inline double fold1(double x, double L) {
     if (!(L > 0)) return x;
+    if (!(fabs(x) <= 4.0 * L)) {
+        x = fmod(x, L);
+        if (x < 0) x += L;
+        if (x >= L) x = 0.0;
+        return x;
+    }
     while (x < 0) x += L;
     while (x >= L) x -= L;
     return x;

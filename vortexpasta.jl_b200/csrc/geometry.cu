@@ -68,8 +68,17 @@ __device__ __forceinline__ void eval_seg(const FilView& f, const double* coef, l
     }
 }
 
+// Fold into [0, L) (min_distance.jl:5-20).  Within four periods the reference's subtraction
+// loops (at most five iterations, same rounding); beyond that, or for a non-finite coordinate,
+// one exact fmod, so the cost never depends on the value (inf and NaN come out as NaN).
 __device__ __forceinline__ double fold(double x, double L, int open) {
     if (open) return x;
+    if (!(fabs(x) <= 4.0 * L)) {
+        x = fmod(x, L);  // exact, |x| < L; NaN for inf / NaN
+        if (x < 0.0) x += L;
+        if (x >= L) x = 0.0;  // -tiny + L rounded to L
+        return x;
+    }
     while (x < 0.0) x += L;
     while (x >= L) x -= L;
     return x;

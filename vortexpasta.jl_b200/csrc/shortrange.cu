@@ -28,7 +28,11 @@ __device__ __forceinline__ int cell_coord(double x, double L, int nc) {
     return c < 0 ? 0 : (c >= nc ? nc - 1 : c);
 }
 
+// Cell (slab) of a point; a point with a non-finite coordinate goes to the sentinel cell
+// `ncell`, which no neighbourhood contains (its pairs are skipped instead of piling up in
+// cell 0 and making the pair search quadratic).
 __device__ __forceinline__ int64_t cell_of(const CellGrid& cg, const KParams& K, double x, double y, double z) {
+    if (!(isfinite(x) && isfinite(y) && isfinite(z))) return cg.ncell;
     int cx = cell_coord(x, K.L[0], cg.nc[0]);
     int cy = cell_coord(y, K.L[1], cg.nc[1]);
     int cz = cell_coord(z, K.L[2], cg.nc[2]);
@@ -839,27 +843,32 @@ int build_cell_lists(vpbs_handle* h) {
     const int64_t Np = h->Np, Nq = h->Nq, ncell = h->cg.ncell;
     int rc;
     if ((rc = ensure(h, h->src_cell, sizeof(int32_t) * 2 * Nq, "src_cell"))) return rc;
-    if ((rc = ensure(h, h->src_start, sizeof(int32_t) * (ncell + 1), "src_start"))) return rc;
-    if ((rc = ensure(h, h->src_fill, sizeof(int32_t) * ncell, "src_counts"))) return rc;
+    // ncell + 1 cells: the last one is the sentinel of points with non-finite coordinates
+    if ((rc = ensure(h, h->src_start, sizeof(int32_t) * (ncell + 2), "src_start"))) return rc;
+    if ((rc = ensure(h, h->src_fill, sizeof(int32_t) * (ncell + 1), "src_counts"))) return rc;
     if ((rc = ensure(h, h->src_sorted, sizeof(double) * 6 * Nq, "src_sorted"))) return rc;
     if ((rc = ensure(h, h->src_seg, sizeof(int32_t) * Nq, "src_seg"))) return rc;
     if ((rc = ensure(h, h->dst_cell, sizeof(int32_t) * 2 * Np, "dst_cell"))) return rc;
-    if ((rc = ensure(h, h->dst_start, sizeof(int32_t) * (ncell + 1), "dst_start"))) return rc;
-    if ((rc = ensure(h, h->dst_fill, sizeof(int32_t) * ncell, "dst_counts"))) return rc;
+    if ((rc = ensure(h, h->dst_start, sizeof(int32_t) * (ncell + 2), "dst_start"))) return rc;
+    if ((rc = ensure(h, h->dst_fill, sizeof(int32_t) * (ncell + 1), "dst_counts"))) return rc;
     if ((rc = ensure(h, h->dst_order, sizeof(int32_t) * Np, "dst_order"))) return rc;
     int32_t* scell = (int32_t*)h->src_cell.p;
     int32_t* srank = scell + Nq;
     int32_t* dcell = (int32_t*)h->dst_cell.p;
     int32_t* drank = dcell + Np;
     StageScope st(h, ST_CELL_LISTS);
-    if ((rc = check_cuda(h, cudaMemsetAsync(h->src_fill.p, 0, sizeof(int32_t) * ncell, h->stream), "memset"))) return rc;
-    if ((rc = check_cuda(h, cudaMemsetAsync(h->dst_fill.p, 0, sizeof(int32_t) * ncell, h->stream), "memset"))) return rc;
+    if ((rc = check_cuda(h, cudaMemsetAsync(h->src_fill.p, 0, sizeof(int32_t) * (ncell + 1), h->stream), "memset")))
+        return rc;
+    if ((rc = check_cuda(h, cudaMemsetAsync(h->dst_fill.p, 0, sizeof(int32_t) * (ncell + 1), h->stream), "memset")))
+        return rc;
     cell_count_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(h->K, h->cg, Nq, (const double*)h->points.p, scell, srank,
                                                                 (int32_t*)h->src_fill.p);
     cell_count_kernel<<<grid_for(Np, 256), 256, 0, h->stream>>>(h->K, h->cg, Np, (const double*)h->nodes.p, dcell, drank,
                                                                 (int32_t*)h->dst_fill.p);
-    if ((rc = exclusive_scan(h, (const int32_t*)h->src_fill.p, (int32_t*)h->src_start.p, ncell, h->scan_tmp))) return rc;
-    if ((rc = exclusive_scan(h, (const int32_t*)h->dst_fill.p, (int32_t*)h->dst_start.p, ncell, h->scan_tmp))) return rc;
+    if ((rc = exclusive_scan(h, (const int32_t*)h->src_fill.p, (int32_t*)h->src_start.p, ncell + 1, h->scan_tmp)))
+        return rc;
+    if ((rc = exclusive_scan(h, (const int32_t*)h->dst_fill.p, (int32_t*)h->dst_start.p, ncell + 1, h->scan_tmp)))
+        return rc;
     scatter_sources_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(
         Nq, h->K.nquad, (const double*)h->points.p, (const double*)h->charges.p, scell, srank,
         (const int32_t*)h->src_start.p, (double*)h->src_sorted.p, (int32_t*)h->src_seg.p);

@@ -218,3 +218,9 @@ class ParamsBiotSavart:
                     precision=self.precision, device=self.device)
         base.update(kw)
         return ParamsBiotSavart(**base)
+
+
+def kelvin_wave_period(lam: float, *, a: float, Delta: float, Gamma: float) -> float:
+    """Period of a small-amplitude Kelvin wave of wavelength `lam` (params.jl:502-507); the
+    reference's AdaptBasedOnSegmentLength sets dt = gamma * kelvin_wave_period(min segment length)."""
+    return 2 * lam ** 2 / Gamma / (math.log(lam / (math.pi * a)) + 0.5 - (Delta + 0.5772156649015329))
