@@ -71,7 +71,8 @@ def test_flags(vp, oracle, built_lib, LIA, short, long):
     assert rel(v, vo) < TOL and rel(psi, po) < TOL
 
 
-@pytest.mark.parametrize("variant", ["explicit_erf", "lia_fraction", "truncate", "m5", "gl2", "nsubdiv1"])
+@pytest.mark.parametrize("variant", ["explicit_erf", "lia_fraction", "truncate", "m5", "m6", "m8", "sigma125_m3",
+                                     "gl2", "nsubdiv1"])
 def test_parameter_variants(vp, oracle, built_lib, variant):
     fs, p = vp.configs.tangle20k()
     fs = fs[:30]
@@ -80,6 +81,9 @@ def test_parameter_variants(vp, oracle, built_lib, variant):
         "lia_fraction": dict(lia_segment_fraction=0.3, quadrature_near_singularity=vp.GaussLegendre(6)),
         "truncate": dict(longrange_truncate_spherical=True),
         "m5": dict(backend_long=vp.NonuniformFFTsBackend(1.5, 5)),
+        "m6": dict(backend_long=vp.NonuniformFFTsBackend(1.5, 6)),
+        "m8": dict(backend_long=vp.NonuniformFFTsBackend(2.0, 8)),
+        "sigma125_m3": dict(backend_long=vp.NonuniformFFTsBackend(1.25, 3)),
         "gl2": dict(quadrature=vp.GaussLegendre(2)),
         "nsubdiv1": dict(backend_short=vp.CellListsBackend(1)),
     }[variant]
@@ -180,6 +184,18 @@ def test_mixed_precision_flags(vp, oracle, built_lib, LIA):
     fs = fs[:25]
     v, psi, _ = gpu_fields(vp, p, fs, LIA=LIA)
     vo, po, _ = oracle.compute_on_nodes(p, fs, streamfunction=True, LIA=LIA)
+    assert rel(v, vo) < MIXED_TOL and rel(psi, po) < MIXED_TOL
+
+
+@pytest.mark.parametrize("sigma,m", [(1.5, 6), (1.25, 3), (2.0, 8)])
+def test_mixed_precision_kernel_widths(vp, oracle, built_lib, sigma, m):
+    """Mixed form with other NUFFT widths (FP32 brick spreading and interpolation tables of
+    up to 3 x 16 entries)."""
+    fs, p = vp.configs.tangle20k(precision="mixed")
+    fs = fs[:25]
+    p = p.with_(backend_long=vp.NonuniformFFTsBackend(sigma, m))
+    v, psi, _ = gpu_fields(vp, p, fs)
+    vo, po, _ = oracle.compute_on_nodes(p, fs, streamfunction=True)
     assert rel(v, vo) < MIXED_TOL and rel(psi, po) < MIXED_TOL
 
 

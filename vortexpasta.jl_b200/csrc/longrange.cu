@@ -456,61 +456,55 @@ __global__ void __launch_bounds__(kColThreads, 2) spread_column_kernel(
     }
 }
 
-// Type-2 interpolation, one warp per node (cell order when available): lanes take (sy, sz)
-// pairs of the footprint, loop over x, and the warp reduces the three components.
-template <int W, typename T>  // kernel width 2m (compile-time: per-lane tables stay in registers)
+// Type-2 interpolation, one warp per node (cell order when available).  The node's 3 x W
+// kernel values and wrapped grid indices go to shared memory (strided over the lanes); then the lanes
+// take the W^3 footprint points in x-fastest order (consecutive lanes read consecutive x),
+// several independent gathers in flight per lane, and the warp reduces the three components.
+template <int W, typename T>  // kernel width 2m (compile-time: the footprint loop is unrolled)
 __global__ void __launch_bounds__(256) interp_warp_kernel(
     LRSizes S, int64_t Np, const int32_t* __restrict__ order, const double* __restrict__ nodes, double sx0,
     double sx1, double sx2, const T* __restrict__ grid, double* __restrict__ out) {
-    const int lane = threadIdx.x & 31;
-    const int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (t >= Np) return;
+    __shared__ T phs[8][3][W];
+    __shared__ int ixs[8][3][W];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+    if (t >= Np) return;  // warp-uniform
     const int64_t i = order ? order[t] : t;
-    constexpr int w = W;
-    const double scale[3] = {sx0, sx1, sx2};
-    double xh[3];
-    int i0[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        xh[d] = (nodes[d * Np + i] * scale[d]) / (2.0 * kPi / S.n[d]);
-        i0[d] = (int)floor(xh[d]) - S.m + 1;
+    for (int e = lane; e < 3 * W; e += 32) {  // 3 W entries (up to 48): some lanes take two
+        const int d = e / W, s = e % W;
+        const double scale = d == 0 ? sx0 : (d == 1 ? sx1 : sx2);
+        const double xh = (nodes[d * Np + i] * scale) / (2.0 * kPi / S.n[d]);
+        const int i0 = (int)floor(xh) - S.m + 1;
+        phs[warp][d][s] = (T)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge);
+        ixs[warp][d][s] = wrapi(i0 + s, S.n[d]);
     }
-    T phx[w];
-    int ixs[w];
-#pragma unroll
-    for (int s = 0; s < w; ++s) {
-        phx[s] = (T)es_kernel(xh[0] - (i0[0] + s), S.m, S.beta, S.edge);
-        ixs[s] = wrapi(i0[0] + s, S.n[0]);
-    }
-    double a0 = 0, a1 = 0, a2 = 0;
-    const int64_t ng = S.ngrid;
-    for (int l = lane; l < w * w; l += 32) {
-        const int sy = l % w, sz = l / w;
-        const double f = es_kernel(xh[1] - (i0[1] + sy), S.m, S.beta, S.edge) *
-                         es_kernel(xh[2] - (i0[2] + sz), S.m, S.beta, S.edge);
-        const int64_t rowi = ((int64_t)wrapi(i0[2] + sz, S.n[2]) * S.n[1] + wrapi(i0[1] + sy, S.n[1])) * S.n[0];
-        T b0 = 0, b1 = 0, b2 = 0;
-#pragma unroll
-        for (int sx = 0; sx < w; ++sx) {
-            const int64_t g = rowi + ixs[sx];
-            b0 += phx[sx] * grid[g];
-            b1 += phx[sx] * grid[ng + g];
-            b2 += phx[sx] * grid[2 * ng + g];
+    __syncwarp();
+    const int64_t ng = S.ngrid, n0 = S.n[0], n1 = S.n[1];
+    T a0 = 0, a1 = 0, a2 = 0;
+    constexpr int kIter = (W * W * W + 31) / 32;
+#pragma unroll 4
+    for (int k = 0; k < kIter; ++k) {
+        const int l = lane + 32 * k;
+        if (l < W * W * W) {
+            const int sx = l % W, sy = (l / W) % W, sz = l / (W * W);
+            const T f = phs[warp][0][sx] * phs[warp][1][sy] * phs[warp][2][sz];
+            const int64_t g = ((int64_t)ixs[warp][2][sz] * n1 + ixs[warp][1][sy]) * n0 + ixs[warp][0][sx];
+            a0 += f * grid[g];
+            a1 += f * grid[ng + g];
+            a2 += f * grid[2 * ng + g];
         }
-        a0 += f * (double)b0;
-        a1 += f * (double)b1;
-        a2 += f * (double)b2;
     }
+    double b0 = a0, b1 = a1, b2 = a2;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        b0 += __shfl_xor_sync(0xffffffffu, b0, o);
+        b1 += __shfl_xor_sync(0xffffffffu, b1, o);
+        b2 += __shfl_xor_sync(0xffffffffu, b2, o);
     }
     if (lane == 0) {
-        out[i] += a0;
-        out[Np + i] += a1;
-        out[2 * Np + i] += a2;
+        out[i] += b0;
+        out[Np + i] += b1;
+        out[2 * Np + i] += b2;
     }
 }
 
@@ -653,7 +647,15 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
         };
         switch (B) {
             case kColB:
-                spread_column_kernel<T><<<nblk, kColThreads, 0, h->stream>>>(S, nb0, nb1, nb2, start, bsrc, foot, grid);
+                // FP32 grids with narrow kernels (m <= 4): shared-memory atomics are native and beat
+                // the 16-deep register columns, which mostly multiply zeros there (1M tangle, m = 3:
+                // 5.2 vs 7.2 ms); wider kernels (m = 5: 13.5 vs 10.1 ms) and FP64 grids (no FP64
+                // shared atomics) use the columns
+                if (std::is_same<T, float>::value && S.m <= 4)
+                    launch(spread_brick_kernel<16, T>);
+                else
+                    spread_column_kernel<T><<<nblk, kColThreads, 0, h->stream>>>(S, nb0, nb1, nb2, start, bsrc, foot,
+                                                                                 grid);
                 break;
             case 12: launch(spread_brick_kernel<12, T>); break;
             case 10: launch(spread_brick_kernel<10, T>); break;
