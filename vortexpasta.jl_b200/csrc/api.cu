@@ -16,6 +16,24 @@ thread_local std::string g_create_error;
 
 namespace vpbs {
 
+// Cells r_cut / M wide in y and z (at least 1 per direction); M > 0 splits each cell into G
+// x-slabs, up to 4 while the (2M+1)^3-cell neighbourhood stays within 729 slabs.  M = 0 (the
+// naive backend) only orders the points (spatial locality).
+CellGrid make_cell_grid(const double L[3], double rcut, int M) {
+    CellGrid cg{};
+    cg.M = M;
+    for (int d = 0; d < 3; ++d)
+        cg.nc[d] = M > 0 ? (int)std::floor(L[d] * M / rcut) : (int)std::fmax(1.0, std::floor(L[d] / rcut));
+    cg.G = 1;
+    if (M > 0) {
+        const int W = 2 * M + 1;
+        cg.G = std::max(1, std::min(4, 729 / (W * W * W)));
+        cg.nc[0] *= cg.G;
+    }
+    cg.ncell = (int64_t)cg.nc[0] * cg.nc[1] * cg.nc[2];
+    return cg;
+}
+
 int set_error(vpbs_handle* h, int code, const std::string& msg) {
     if (h) h->err = msg;
     else g_create_error = msg;
@@ -168,21 +186,10 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
             return set_error(nullptr, VPBS_ERR_PARAMS, "cutoff distance `rcut` is too large. It must be less than half the cell unit size `L` in each direction");
         K.rcut = P.rcut;
         K.rcut2 = P.rcut * P.rcut;
-        cg.M = M;
-        for (int d = 0; d < 3; ++d) {
-            // with M = 0 the cells only order the points (spatial locality); pairs are not culled
-            cg.nc[d] = M > 0 ? (int)std::floor(P.L[d] * M / P.rcut) : (int)std::fmax(1.0, std::floor(P.L[d] / P.rcut));
-            if (M > 0 && cg.nc[d] < 2 * M + 1)
+        cg = make_cell_grid(P.L, P.rcut, M);
+        for (int d = 0; d < 3; ++d)
+            if (M > 0 && cg.nc[d] < 2 * M + 1 + (d == 0 ? (cg.G - 1) * (2 * M + 1) : 0))
                 return set_error(nullptr, VPBS_ERR_PARAMS, "cell lists: the cut-off distance r_cut is too large for periodic padding");
-        }
-        // x slabs per cell: up to 4 while the (2M+1)^3-cell neighbourhood stays within 729 slabs
-        cg.G = 1;
-        if (M > 0) {
-            const int W = 2 * M + 1;
-            cg.G = std::max(1, std::min(4, 729 / (W * W * W)));
-            cg.nc[0] *= cg.G;
-        }
-        cg.ncell = (int64_t)cg.nc[0] * cg.nc[1] * cg.nc[2];
         if (cg.ncell > (int64_t)1 << 30) return set_error(nullptr, VPBS_ERR_PARAMS, "too many cells (rcut too small)");
         if (!(P.sigma > 1.0)) return set_error(nullptr, VPBS_ERR_PARAMS, "NUFFT oversampling factor sigma must be > 1");
         if (P.m < 1 || P.m > kMaxHalfSupport) return set_error(nullptr, VPBS_ERR_PARAMS, "NUFFT half support m must be in 1:8");

@@ -174,6 +174,7 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
 
 // api.cu
 int process_point_charges(vpbs_handle* h);  // cell lists of the current point data
+CellGrid make_cell_grid(const double L[3], double rcut, int M);
 
 // shortrange.cu
 int build_cell_lists(vpbs_handle* h);
