@@ -211,6 +211,8 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
     if (!rc) rc = check_cuda(h, cudaStreamCreateWithFlags(&h->aux_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     for (cudaEvent_t* e : {&h->ev_fork, &h->ev_short, &h->ev_long})
         if (!rc) rc = check_cuda(h, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+    for (int k = 0; k < kStageEvents && !rc; ++k)
+        rc = check_cuda(h, cudaEventCreateWithFlags(&h->stage_ev[k], cudaEventDisableTiming), "cudaEventCreate");
     h->stream = h->own_stream;
     if (!rc && !open) rc = longrange_init(h);
     if (!rc && !open) {
@@ -272,6 +274,8 @@ int vpbs_destroy(vpbs_handle* h) {
     if (h->pin_out) cudaFreeHost(h->pin_out);
     if (h->h2d_done) cudaEventDestroy(h->h2d_done);
     if (h->aux_stream) cudaStreamSynchronize(h->aux_stream);
+    for (int k = 0; k < kStageEvents; ++k)
+        if (h->stage_ev[k]) cudaEventDestroy(h->stage_ev[k]);
     for (cudaEvent_t e : {h->ev_fork, h->ev_short, h->ev_long})
         if (e) cudaEventDestroy(e);
     if (h->aux_stream) cudaStreamDestroy(h->aux_stream);
@@ -382,12 +386,21 @@ int vpbs_set_filaments(vpbs_handle* h, int64_t nfil, const int64_t* offsets, con
     int rc;
     if ((rc = prepare_filaments(h, nfil, offsets, !on_device))) return rc;
     if (on_device) return set_filaments_staged(h, nfil, offsets, nodes_xyz);
+    // pinned staging in chunks: the host copy of chunk k overlaps the transfer of chunk k-1
     const size_t bytes_off = sizeof(int64_t) * (nfil + 1);
-    const void* src[1] = {nodes_xyz};
-    void* dst[1] = {(char*)h->pin_in + bytes_off};
-    const size_t bytes[1] = {sizeof(double) * 3 * offsets[nfil]};
-    parallel_copies(1, dst, src, bytes);
-    return set_filaments_staged(h, nfil, offsets, nullptr);
+    const size_t total = sizeof(double) * 3 * offsets[nfil];
+    const size_t chunk = std::max<size_t>(kStageChunk, (total / kStageEvents + 7) & ~(size_t)7);
+    char* pin = (char*)h->pin_in + bytes_off;
+    for (size_t o = 0; o < total; o += chunk) {
+        const size_t n = std::min(chunk, total - o);
+        const void* src[1] = {(const char*)nodes_xyz + o};
+        void* dst[1] = {pin + o};
+        parallel_copies(1, dst, src, &n);
+        if ((rc = check_cuda(h, cudaMemcpyAsync((char*)h->nodes_in.p + o, pin + o, n, cudaMemcpyHostToDevice, h->stream),
+                             "H2D nodes")))
+            return rc;
+    }
+    return set_filaments_staged(h, nfil, offsets, (const double*)h->nodes_in.p);
 }
 
 int vpbs_stage_filaments(vpbs_handle* h, int64_t nfil, int64_t Np, int64_t** offsets, double** nodes) {
@@ -583,17 +596,43 @@ static int fetch_aos(vpbs_handle* h, int32_t field, const double** out) {
 int vpbs_get(vpbs_handle* h, int32_t field, double* out_xyz, int32_t accumulate) {
     if (!h) return VPBS_ERR_ARG;
     if (!out_xyz) return set_error(h, VPBS_ERR_ARG, "null output");
-    const double* s;
-    int rc = fetch_aos(h, field, &s);
-    if (rc) return rc;
-    const int64_t n = 3 * h->Np;
     if (accumulate) {
+        const double* s;
+        int rc = fetch_aos(h, field, &s);
+        if (rc) return rc;
+        const int64_t n = 3 * h->Np;
         for (int64_t i = 0; i < n; ++i) out_xyz[i] += s[i];
-    } else {
-        void* dst[1] = {out_xyz};
-        const void* src[1] = {s};
-        const size_t nb[1] = {sizeof(double) * n};
-        parallel_copies(1, dst, src, nb);
+        return 0;
+    }
+    // device transpose, then the transfer in chunks: the host copy of chunk k overlaps the
+    // transfer of chunk k+1
+    if (field != VPBS_VELOCITY && field != VPBS_STREAMFUNCTION) return set_error(h, VPBS_ERR_ARG, "bad field");
+    if (!(h->last_fields & field)) return set_error(h, VPBS_ERR_STATE, "field was not computed");
+    int rc;
+    if ((rc = activate(h))) return rc;
+    const int64_t Np = h->Np;
+    const size_t total = sizeof(double) * 3 * Np;
+    if ((rc = ensure(h, h->aos_out, total, "AoS output staging"))) return rc;
+    if ((rc = ensure_pinned(h, &h->pin_out, &h->pin_out_bytes, total))) return rc;
+    soa_to_aos_kernel<<<grid_for(3 * Np, 256), 256, 0, h->stream>>>(
+        Np, (const double*)(field == VPBS_VELOCITY ? h->vel.p : h->psi.p), (double*)h->aos_out.p);
+    h->launches++;
+    if ((rc = check_cuda(h, cudaGetLastError(), "AoS kernel"))) return rc;
+    const size_t chunk = std::max<size_t>(kStageChunk, (total / kStageEvents + 7) & ~(size_t)7);
+    int nch = 0;
+    for (size_t o = 0; o < total; o += chunk, ++nch) {
+        const size_t n = std::min(chunk, total - o);
+        if ((rc = check_cuda(h, cudaMemcpyAsync((char*)h->pin_out + o, (const char*)h->aos_out.p + o, n,
+                                                cudaMemcpyDeviceToHost, h->stream), "D2H")))
+            return rc;
+        if ((rc = check_cuda(h, cudaEventRecord(h->stage_ev[nch], h->stream), "event record"))) return rc;
+    }
+    for (int k = 0; k < nch; ++k) {
+        const size_t o = (size_t)k * chunk, n = std::min(chunk, total - o);
+        if ((rc = check_cuda(h, cudaEventSynchronize(h->stage_ev[k]), "D2H sync"))) return rc;
+        const void* src[1] = {(const char*)h->pin_out + o};
+        void* dst[1] = {(char*)out_xyz + o};
+        parallel_copies(1, dst, src, &n);
     }
     return 0;
 }

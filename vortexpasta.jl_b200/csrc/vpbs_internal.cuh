@@ -82,6 +82,11 @@ struct LRSizes {
     double edge;     // e^{-beta}, subtracted so the kernel vanishes at |u| = m
 };
 
+// Host <-> device staging of flat node and output arrays goes in chunks of at least
+// kStageChunk bytes (at most kStageEvents of them), host copies overlapping the transfers.
+constexpr size_t kStageChunk = (size_t)8 << 20;
+constexpr int kStageEvents = 16;
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
@@ -144,6 +149,7 @@ struct vpbs_handle {
     cudaEvent_t interp_wait = nullptr;  // event the interpolation waits for (outputs are shared)
 
     std::vector<int64_t> host_offsets;  // filament layout of the last vpbs_set_filaments (host copy)
+    cudaEvent_t stage_ev[vpbs::kStageEvents] = {};  // chunked host <-> device staging
     vpbs::DevBuf aos_out;                 // AoS staging of an output field (vpbs_get_filaments)
 
     // time stepping (vpbs_rk4_step): filament layout of the last vpbs_set_filaments, RK buffers

@@ -229,8 +229,8 @@ def sweep_configuration(fs, L: float, choices, rtol: float = 1e-5):
 
 
 def training_choices(L: float):
-    return tuning.candidate_grid(L, rcut_fracs=(1 / 12, 1 / 16, 1 / 20, 1 / 24, 1 / 32, 1 / 40, 1 / 48),
-                                 betas=(2.9, 3.1, 3.3), sigma_m=((1.25, 4), (1.5, 3), (2.0, 3)))
+    return tuning.candidate_grid(L, rcut_fracs=(1 / 12, 1 / 16, 1 / 20, 1 / 24, 1 / 32, 1 / 40, 1 / 48, 1 / 56),
+                                 betas=(2.95, 3.15, 3.35), sigma_m=((1.25, 4), (1.5, 3), (2.0, 3)))
 
 
 def generate_dataset(n: int, seed: int, L: float = 2 * math.pi, rtol: float = 1e-5, min_nodes: int = 5_000,
