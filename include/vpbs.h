@@ -228,6 +228,15 @@ int vpbs_ewald_table_eval(double xmax, const double* x, int64_t n, double* erfc_
  * reference. */
 int vpbs_fma_throughput(int32_t device, int32_t fp64, double* tflops);
 
+/* ---- Diagnostics (src/Diagnostics/spectra.jl:84-232, spectra_helicity.jl:43-76) ---- */
+
+/* Energy (kind 0) or helicity (kind 1) spectrum of the vorticity coefficients left by the last
+ * long-range computation (the field of vpbs_get_uhat), summed over spherical shells of width dk:
+ * out[n] for k_n = n dk, n = 0..nk-1 (bin n = trunc(|k|/dk + 1/2), weight 1/2 on the kx = 0
+ * plane).  Energy: sum of |w_k|^2/k^2/dk; helicity: sum of 2 V Re[(i k x w_k)^* . w_k]/k^2/dk.
+ * Synchronous; host output. */
+int vpbs_spectrum(vpbs_handle* h, int32_t kind, double dk, double* out, int64_t nk);
+
 /* ---- Time stepping and ensembles (the batching form) ---- */
 
 /* One classic RK4 step (src/Timestepping/timesteppers/explicit/RK4.jl:14-44, advection of

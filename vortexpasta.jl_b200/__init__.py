@@ -5,7 +5,7 @@ The compute path is libvpbs.so (C ABI in include/vpbs.h); this package mirrors t
 reference's BiotSavart API on top of it.
 """
 
-from . import configs, curves
+from . import configs, curves, diagnostics, learned, timestepping, tuning
 from ._lib import LIB_PATH, VpbsError
 from .biotsavart import (BiotSavartCache, LongRangeCacheState, compute_on_nodes_, get_longrange_field_fourier,
                          init_cache, velocity_on_nodes, velocity_on_nodes_)
@@ -13,7 +13,7 @@ from .params import (CellListsBackend, GaussianSplitting, GaussLegendre, NaiveSh
                      NoSplitting, ParamsBiotSavart, kmax_to_gridsize, maximum_wavenumber)
 
 __all__ = [
-    "configs", "curves", "LIB_PATH", "VpbsError", "BiotSavartCache", "LongRangeCacheState", "compute_on_nodes_",
+    "configs", "curves", "diagnostics", "learned", "timestepping", "tuning", "LIB_PATH", "VpbsError", "BiotSavartCache", "LongRangeCacheState", "compute_on_nodes_",
     "get_longrange_field_fourier", "init_cache", "velocity_on_nodes", "velocity_on_nodes_", "CellListsBackend",
     "GaussianSplitting", "GaussLegendre", "NaiveShortRangeBackend", "NonuniformFFTsBackend", "NoSplitting",
     "ParamsBiotSavart", "kmax_to_gridsize", "maximum_wavenumber",

@@ -67,6 +67,7 @@ SIGNATURES = {
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "vpbs_features": (ct.c_int, [ct.c_void_p, c_float_p, ct.c_int32]),
+    "vpbs_spectrum": (ct.c_int, [ct.c_void_p, ct.c_int32, ct.c_double, c_double_p, ct.c_int64]),
     "vpbs_set_filament_list": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_void_p, c_int64_p]),
     "vpbs_stage_filaments": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int64, ct.POINTER(c_int64_p),
                                         ct.POINTER(c_double_p)]),
