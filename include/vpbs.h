@@ -50,12 +50,20 @@ typedef enum {
 #define VPBS_PRECISION_MIXED 1 /* FP32 bulk (pairs, spreading, FFT, interpolation); FP64
                                   positions, separations, local term, final accumulation */
 
+/* Ewald splitting kernels (src/BiotSavart/splitting/splitting.jl:1-47). */
+#define VPBS_SPLITTING_GAUSSIAN 0      /* GaussianSplitting, or NoSplitting when alpha == 0 */
+#define VPBS_SPLITTING_KAISER_BESSEL 1 /* KaiserBesselSplitting (splitting/kaiser_bessel.jl) */
+
 /* Parameters: the union of ParamsCommon, ParamsShortRange and ParamsLongRange
  * (src/BiotSavart/params.jl:8-30, 74-115, 141-152) plus the two backends
  * (CellListsBackend, shortrange/backends/cell_lists.jl:64-87; NonuniformFFTsBackend,
  * longrange/backends/nonuniformffts.jl:97-126).  GaussianSplitting is described by
  * (alpha, rcut, Ns) already derived by the caller (splitting/gaussian.jl:133-200);
- * alpha == 0 selects NoSplitting (open domain, naive pair sum, no long range). */
+ * alpha == 0 selects NoSplitting (open domain, naive pair sum, no long range).
+ * KaiserBesselSplitting is described by (kb_beta, rcut, Ns, kb_rtol) already derived by the
+ * caller (kaiser_bessel.jl:165-223); alpha is ignored for it.  kb_rtol sets the truncation
+ * of the Chebyshev series of the kernel and of its integral (kaiser_bessel.jl:139-147), as
+ * in the reference. */
 typedef struct {
     double Gamma;                 /* circulation */
     double a;                     /* vortex core size */
@@ -78,6 +86,9 @@ typedef struct {
     int32_t nsubdiv;              /* CellListsBackend subdivisions M (reference default 2) */
     int32_t precision;            /* VPBS_PRECISION_* */
     int32_t device;               /* CUDA device ordinal */
+    int32_t splitting;            /* VPBS_SPLITTING_* (0, the zero-initialised value: Gaussian) */
+    double kb_beta;               /* Kaiser-Bessel shape parameter beta */
+    double kb_rtol;               /* Kaiser-Bessel relative accuracy rtol */
 } vpbs_params;
 
 /* Structure-of-arrays view of a vector of Vec3 (the layout of a StructVector{Vec3}). */
@@ -222,6 +233,14 @@ int vpbs_point_data_noalloc(const vpbs_params* params, int64_t nfil, const int64
  * (splitting/gaussian.jl:273-279) by these degree-9 Taylor tables; this entry exists to test
  * them.  No counterpart in the reference. */
 int vpbs_ewald_table_eval(double xmax, const double* x, int64_t n, double* erfc_out, double* g_out);
+
+/* Host evaluation of the Kaiser-Bessel short-range weights a = 1 - F(r) and g = 1 - F(r) + r f(r)
+ * for r in [0, rcut]: from the pair kernel's tables (a_table, g_table) and from the truncated
+ * Chebyshev series they are fitted to (a_series, g_series), built with the reference's rules
+ * (splitting/kaiser_bessel.jl:139-147, splitting/chebyshev.jl:73-172).  Any output may be NULL.
+ * Exists to test the tables and the series; no counterpart in the reference. */
+int vpbs_kb_weights(double beta, double rcut, double rtol, const double* r, int64_t n, double* a_table,
+                    double* g_table, double* a_series, double* g_series);
 
 /* Measured CUDA-core FMA throughput of `device` in TFLOP/s (fp64 = 1: double, 0: float); the
  * denominator of the pair kernel's roofline.  Measurement support; no counterpart in the

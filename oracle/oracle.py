@@ -25,7 +25,8 @@ class OParams(ct.Structure):
         ("alpha", ct.c_double), ("rcut", ct.c_double), ("Ns", ct.c_int * 3), ("sigma", ct.c_double),
         ("m", ct.c_int), ("nquad", ct.c_int), ("nquad_near", ct.c_int), ("lia_segment_fraction", ct.c_double),
         ("avoid_explicit_erf", ct.c_int), ("truncate_spherical", ct.c_int), ("nsubdiv", ct.c_int),
-        ("longrange_exact", ct.c_int), ("nthreads", ct.c_int),
+        ("longrange_exact", ct.c_int), ("nthreads", ct.c_int), ("splitting", ct.c_int), ("kb_beta", ct.c_double),
+        ("kb_rtol", ct.c_double),
     ]
 
 
@@ -59,6 +60,8 @@ def load():
         lib.vpo_vorticity_fourier.restype = ct.c_int
         lib.vpo_vorticity_fourier.argtypes = [ct.POINTER(OParams), ct.c_int64, dp, dp, dp, ct.POINTER(OStats)]
         lib.vpo_gl_rule.argtypes = [ct.c_int, dp, dp]
+        lib.vpo_kb_weights.restype = ct.c_int
+        lib.vpo_kb_weights.argtypes = [ct.c_double, ct.c_double, ct.c_double, dp, ct.c_long, dp, dp]
         lib.vpo_fft_size.restype = ct.c_int
         lib.vpo_fft_size.argtypes = [ct.c_int, ct.c_double]
         _lib = lib
@@ -74,7 +77,13 @@ def make_params(p, *, exact=False, nthreads=0) -> OParams:
     o = OParams()
     o.Gamma, o.a, o.Delta = p.Gamma, p.a, p.Delta
     sp = p.splitting
-    if getattr(sp, "alpha", 0.0) == 0.0:
+    if hasattr(sp, "beta") and not hasattr(sp, "alpha"):  # KaiserBesselSplitting
+        o.splitting, o.kb_beta, o.kb_rtol = 1, sp.beta, sp.rtol
+        o.alpha, o.rcut = 0.0, sp.rcut
+        for d in range(3):
+            o.L[d] = sp.Ls[d]
+            o.Ns[d] = sp.Ns[d]
+    elif getattr(sp, "alpha", 0.0) == 0.0:
         o.alpha = 0.0
         o.rcut = math.inf
         for d in range(3):
@@ -161,6 +170,18 @@ def vorticity_fourier(p, points, charges, *, exact=False):
     if rc != 0:
         raise RuntimeError("oracle vorticity_fourier failed")
     return buf.view(np.complex128).reshape(3, Ns[2], Ns[1], nkx)
+
+
+def kb_weights(beta, rcut, rtol, r):
+    """Kaiser-Bessel short-range weights (1 - F(r), 1 - F(r) + r f(r)) from the oracle's series,
+    and the number of even Chebyshev coefficients kept in f."""
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    a = np.zeros_like(r)
+    g = np.zeros_like(r)
+    ne = load().vpo_kb_weights(beta, rcut, rtol, _dp(r), len(r), _dp(a), _dp(g))
+    if ne < 0:
+        raise RuntimeError("oracle Kaiser-Bessel series did not converge")
+    return a, g, ne
 
 
 def gl_rule(n):

@@ -11,7 +11,7 @@
  * the oracle is instead checked against the analytic ring answers of
  * test/ring.jl, the exact Fourier sums of ExactSumBackend (test/trefoil.jl), exact
  * pair counts (test/cell_lists.jl) and independence from the Ewald parameter
- * alpha (test/trefoil.jl:299-329).
+ * alpha and, for the Kaiser-Bessel kernel, from r_cut (test/trefoil.jl:299-329, 422-429).
  *
  * Each function names the reference file:line it restates (paths relative to the
  * VortexPasta.jl tree).  The NUFFT (spreading kernel, oversampled grid size) lives
@@ -46,6 +46,7 @@ static inline void cross3(const double* u, const double* v, double* w) {
 }
 
 static inline int is_open(const vpo_params* p) { return !(p->L[0] > 0 && p->L[1] > 0 && p->L[2] > 0); }
+static inline int ewald_on(const vpo_params* p) { return p->splitting == 1 || p->alpha > 0; }
 
 /* Fold into [0, L).  reference: src/Filaments/min_distance.jl:5-20 (subtraction loops within
  * four periods; one exact fmod beyond, so a huge or non-finite coordinate cannot loop) */
@@ -415,12 +416,156 @@ static void local_term(const vpo_params* p, int64_t Np, const double* d1, const 
     }
 }
 
+/* ------------------------------------------------------------------------- */
+/* Kaiser-Bessel splitting: src/BiotSavart/splitting/kaiser_bessel.jl,       */
+/*                          src/BiotSavart/splitting/chebyshev.jl            */
+/* ------------------------------------------------------------------------- */
+
+/* Modified Bessel function I0 by its power series sum_k (z^2/4)^k / (k!)^2 (all terms positive,
+ * so summing until the term no longer changes the sum is accurate to rounding). */
+static double bessel_i0(double z) {
+    double q = 0.25 * z * z, term = 1.0, sum = 1.0;
+    for (int k = 1; k < 500; ++k) {
+        term *= q / ((double)k * k);
+        double s2 = sum + term;
+        if (s2 == sum) break;
+        sum = s2;
+    }
+    return sum;
+}
+
+typedef struct {
+    double rcut;
+    int ne;          /* even coefficients of f: T_0, T_2, ..., T_{2(ne-1)} */
+    double* fe;
+    double* Fo;      /* odd coefficients of F: T_1, T_3, ..., T_{2 ne - 1} */
+} kb_series;
+
+/* chebyshev.jl:130-172 (approximate, symmetry = :even): values of
+ * f(r) = beta / (rcut sinh beta) I0(beta sqrt(1 - r^2/rcut^2)) on r_n = rcut cos(pi n/(N-1)),
+ * FFTW's REDFT00 (type-I DCT) written out, ends halved, / (N - 1); truncation before the first
+ * pair of consecutive coefficients below rtol * sum|c| (N doubles from 64 otherwise); the
+ * even-index coefficients before it are kept.  Then chebyshev.jl:99-122 (integrate even -> odd,
+ * times rcut). */
+static int kb_build(double beta, double rcut, double rtol, kb_series* S) {
+    S->rcut = rcut;
+    S->ne = 0;
+    S->fe = S->Fo = NULL;
+    double C = beta / (rcut * sinh(beta));
+    for (int N = 64; N <= 4096; N *= 2) {
+        double* u = (double*)malloc(sizeof(double) * N);
+        double* c = (double*)malloc(sizeof(double) * N);
+        for (int n = 0; n < N; ++n) {
+            double x = rcut * cos(VPO_PI * n / (N - 1));
+            double t = 1.0 - (x / rcut) * (x / rcut);
+            u[n] = C * bessel_i0(beta * sqrt(t > 0 ? t : 0.0));
+        }
+        double total = 0.0;
+        for (int k = 0; k < N; ++k) {
+            double y = u[0] + ((k & 1) ? -u[N - 1] : u[N - 1]);
+            for (int j = 1; j < N - 1; ++j) {
+                long ph = ((long)j * k) % (2L * (N - 1));
+                y += 2.0 * u[j] * cos(VPO_PI * (double)ph / (N - 1));
+            }
+            if (k == 0 || k == N - 1) y *= 0.5;
+            c[k] = y / (N - 1);
+            total += fabs(c[k]);
+        }
+        double atol = rtol * total;
+        int cut = -1;
+        for (int j = 0; j + 1 < N; ++j)
+            if (fabs(c[j]) < atol && fabs(c[j + 1]) < atol) { cut = j; break; }
+        free(u);
+        if (cut >= 1) {
+            int ne = (cut + 1) / 2;  /* even indices 0, 2, ..., < cut */
+            S->ne = ne;
+            S->fe = (double*)malloc(sizeof(double) * ne);
+            S->Fo = (double*)malloc(sizeof(double) * ne);
+            for (int i = 0; i < ne; ++i) S->fe[i] = c[2 * i];
+            free(c);
+            if (ne == 1) {
+                S->Fo[0] = S->fe[0];
+            } else {
+                S->Fo[0] = (2.0 * S->fe[0] - S->fe[1]) / 2.0;
+                for (int i = 1; i < ne - 1; ++i) S->Fo[i] = (S->fe[i] - S->fe[i + 1]) / (2.0 * (2 * i + 1));
+                S->Fo[ne - 1] = S->fe[ne - 1] / (2.0 * (2 * ne - 1));
+            }
+            for (int i = 0; i < ne; ++i) S->Fo[i] *= rcut;
+            return 0;
+        }
+        free(c);
+    }
+    return -1;
+}
+
+static void kb_free(kb_series* S) {
+    free(S->fe);
+    free(S->Fo);
+    S->fe = S->Fo = NULL;
+    S->ne = 0;
+}
+
+/* chebyshev.jl:50-71: Clenshaw recurrences of the even and odd series (x = r / rcut). */
+static double cheb_even(const double* cs, int N, double x) {
+    double bpp = 0.0, bp = 0.0, twox = 2.0 * x;
+    for (int n = N - 1; n >= 1; --n) {
+        double b = twox * bp + cs[n] - bpp;
+        bpp = bp; bp = b;
+        b = twox * bp - bpp;
+        bpp = bp; bp = b;
+    }
+    return cs[0] + x * bp - bpp;
+}
+
+static double cheb_odd(const double* cs, int N, double x) {
+    double bpp = 0.0, bp = cs[N - 1], twox = 2.0 * x;
+    for (int n = N - 2; n >= 0; --n) {
+        double b = twox * bp - bpp;
+        bpp = bp; bp = b;
+        b = twox * bp + cs[n] - bpp;
+        bpp = bp; bp = b;
+    }
+    return x * bp - bpp;
+}
+
+/* weights_shortrange (kaiser_bessel.jl:282-292): a = 1 - F(r), b = r f(r) */
+static inline void kb_short_weights(const kb_series* S, double r, double* a, double* b) {
+    double x = r / S->rcut;
+    *a = 1.0 - cheb_odd(S->Fo, S->ne, x);
+    *b = r * cheb_even(S->fe, S->ne, x);
+}
+
+/* splitting_kernel_fourier (kaiser_bessel.jl:266-278) */
+static inline double kb_fourier(double beta, double rcut, double k2) {
+    double s = beta * beta - k2 * rcut * rcut;
+    if (!(s > 0)) return 0.0;
+    double q = sqrt(s);
+    return beta / sinh(beta) * sinh(q) / q;
+}
+
+/* The series of the current call (built once per vpo_compute_on_nodes). */
+static kb_series g_kb;
+
+int vpo_kb_weights(double beta, double rcut, double rtol, const double* r, long n, double* a, double* g) {
+    kb_series S;
+    if (kb_build(beta, rcut, rtol, &S)) return -1;
+    for (long i = 0; i < n; ++i) {
+        double wa, wb;
+        kb_short_weights(&S, r[i], &wa, &wb);
+        a[i] = wa;
+        g[i] = wa + wb;
+    }
+    int ne = S.ne;
+    kb_free(&S);
+    return ne;
+}
+
 static void remove_self(const vpo_params* p, int64_t Np, const double* nodes_f, const int32_t* idx_prev,
                         const double* points, const double* charges, double* vel, double* psi) {
     double pref = p->Gamma / (4.0 * VPO_PI);
     int nq = p->nquad;
     double alpha = p->alpha;
-    int explicit_erf = !p->avoid_explicit_erf && alpha > 0;
+    int explicit_erf = !p->avoid_explicit_erf && ewald_on(p);
 #pragma omp parallel for
     for (int64_t i = 0; i < Np; ++i) {
         const double* x = nodes_f + 3 * i;
@@ -436,7 +581,15 @@ static void remove_self(const vpo_params* p, int64_t Np, const double* nodes_f, 
                 double rinv = 1.0 / rr;
                 const double* qc = charges + 3 * j;
                 double fa = 1.0, fb = 0.0;
-                if (explicit_erf) {
+                if (explicit_erf && p->splitting == 1) {
+                    /* weights_longrange (kaiser_bessel.jl:296-301): (F, r f) inside rcut, (1, 0) beyond */
+                    if (rr < p->rcut) {
+                        double sa, sb;
+                        kb_short_weights(&g_kb, rr, &sa, &sb);
+                        fa = 1.0 - sa;
+                        fb = sb;
+                    }
+                } else if (explicit_erf) {
                     double ar = alpha * rr;
                     fa = erf(ar);
                     fb = 2.0 / sqrt(VPO_PI) * ar * exp(-(ar * ar));
@@ -521,7 +674,9 @@ static inline void pair_one(const vpo_params* p, const double* x, const double* 
     double rr = sqrt(r2);
     double rinv = 1.0 / rr;
     double a = 1.0, b = 0.0;
-    if (p->alpha > 0) {
+    if (p->splitting == 1) {
+        kb_short_weights(&g_kb, rr, &a, &b);
+    } else if (p->alpha > 0) {
         double ar = p->alpha * rr;
         a = erfc(ar);
         b = 2.0 / sqrt(VPO_PI) * ar * exp(-(ar * ar));
@@ -545,13 +700,13 @@ static inline int is_local_pair(int64_t i, int64_t ip, int64_t j, int nq) {
 static void pairs(const vpo_params* p, int64_t Np, int64_t Nq, const double* nodes_f, const int32_t* idx_prev,
                   const double* points, const double* charges, double* vel, double* psi, vpo_stats* st) {
     double pref = p->Gamma / (4.0 * VPO_PI);
-    double rcut2 = (p->alpha > 0) ? p->rcut * p->rcut : INFINITY;
+    double rcut2 = ewald_on(p) ? p->rcut * p->rcut : INFINITY;
     int want_v = vel != NULL, want_psi = psi != NULL;
-    int skip_local = !p->avoid_explicit_erf && p->alpha > 0;
+    int skip_local = !p->avoid_explicit_erf && ewald_on(p);
     int nq = p->nquad;
     int64_t tot_in = 0, tot_cand = 0;
     int M = p->nsubdiv;
-    if (M <= 0 || is_open(p) || !(p->alpha > 0)) {
+    if (M <= 0 || is_open(p) || !ewald_on(p)) {
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : tot_in, tot_cand)
         for (int64_t i = 0; i < Np; ++i) {
             pair_acc acc;
@@ -931,7 +1086,8 @@ static void lr_interpolate(const vpo_params* p, const lr_field* W, int field, in
                            const double* nodes_f, double* out) {
     int Ns0 = W->Ns[0], Ns1 = W->Ns[1], Ns2 = W->Ns[2], nkx = W->nkx;
     size_t nu = (size_t)Ns2 * Ns1 * nkx;
-    /* û of the requested field, smoothed by exp(-k^2/4 alpha^2) */
+    /* û of the requested field, smoothed by exp(-k^2/4 alpha^2) (Gaussian) or by the
+     * Kaiser-Bessel filter */
     cplx* u = (cplx*)malloc(sizeof(cplx) * 3 * nu);
     double beta_g = -1.0 / (4.0 * p->alpha * p->alpha);
     for (int iz = 0; iz < Ns2; ++iz)
@@ -940,7 +1096,7 @@ static void lr_interpolate(const vpo_params* p, const lr_field* W, int field, in
                 double k[3] = {W->k0[0] * ix, W->k0[1] * mode_of(iy, Ns1), W->k0[2] * mode_of(iz, Ns2)};
                 double k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
                 double k2inv = (k2 == 0.0) ? 0.0 : 1.0 / k2;
-                double E = exp(beta_g * k2);
+                double E = p->splitting == 1 ? kb_fourier(p->kb_beta, p->rcut, k2) : exp(beta_g * k2);
                 cplx w[3];
                 for (int c = 0; c < 3; ++c) {
                     size_t q = uidx(W, c, ix, iy, iz);
@@ -1064,7 +1220,7 @@ int vpo_vorticity_fourier(const vpo_params* p, int64_t Nq, const double* points,
 #ifdef _OPENMP
     if (p->nthreads > 0) omp_set_num_threads(p->nthreads);
 #endif
-    if (is_open(p) || !(p->alpha > 0)) return -1;
+    if (is_open(p) || !ewald_on(p)) return -1;
     lr_field F;
     lr_field_init(p, &F);
     lr_vorticity(p, Nq, points, charges, &F, st);
@@ -1089,7 +1245,11 @@ int vpo_compute_on_nodes(const vpo_params* p, int nfil, const int64_t* offsets, 
     int nq = p->nquad;
     int64_t Nq = Np * nq;
     if (st) memset(st, 0, sizeof *st);
-    if (p->alpha > 0) {
+    if (p->splitting == 1) {
+        kb_free(&g_kb);
+        if (!(p->kb_beta > 0) || !(p->rcut > 0) || kb_build(p->kb_beta, p->rcut, p->kb_rtol, &g_kb)) return -3;
+    }
+    if (ewald_on(p)) {
         for (int d = 0; d < 3; ++d)
             if (!(p->L[d] > 0) || 2.0 * p->rcut > p->L[d]) return -3;
         if (p->nsubdiv > 0)
@@ -1109,7 +1269,7 @@ int vpo_compute_on_nodes(const vpo_params* p, int nfil, const int64_t* offsets, 
     if (vel_out) memset(vel_out, 0, sizeof(double) * 3 * Np);
     if (psi_out) memset(psi_out, 0, sizeof(double) * 3 * Np);
 
-    int with_long = longrange && lia_mode != 2 && p->alpha > 0;
+    int with_long = longrange && lia_mode != 2 && ewald_on(p);
     if (with_long) {
         lr_field F;
         lr_field_init(p, &F);

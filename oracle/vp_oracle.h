@@ -37,7 +37,15 @@ typedef struct {
     int    nsubdiv;                  /* cell-list subdivisions M; 0 => naive pair loop */
     int    longrange_exact;          /* 1 => ExactSumBackend instead of NUFFT */
     int    nthreads;                 /* OpenMP threads (<= 0: default) */
+    int    splitting;                /* 0: Gaussian (alpha) / none; 1: Kaiser-Bessel */
+    double kb_beta;                  /* Kaiser-Bessel shape parameter */
+    double kb_rtol;                  /* Kaiser-Bessel rtol (Chebyshev truncation) */
 } vpo_params;
+
+/* Kaiser-Bessel short-range weights 1 - F(r) and 1 - F(r) + r f(r) from the truncated
+ * Chebyshev series (reference: src/BiotSavart/splitting/kaiser_bessel.jl:139-147, 282-292;
+ * splitting/chebyshev.jl:33-172).  Returns the number of even coefficients kept in f, or -1. */
+int vpo_kb_weights(double beta, double rcut, double rtol, const double* r, long n, double* a, double* g);
 
 typedef struct {
     int64_t pairs_in_range;          /* pairs with r^2 <= rcut^2 (short range) */

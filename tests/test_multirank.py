@@ -37,7 +37,7 @@ def _worker(rank, world, port, out):
 def test_two_ranks_gloo():
     import torch.multiprocessing as mp
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
         r0, r1 = out[0], out[1]

@@ -15,6 +15,8 @@ VELOCITY = 1
 STREAMFUNCTION = 2
 LIA_FALSE, LIA_TRUE, LIA_ONLY = 0, 1, 2
 PRECISION = {"fp64": 0, "mixed": 1}
+SPLITTING_GAUSSIAN = 0
+SPLITTING_KAISER_BESSEL = 1
 
 c_double_p = ct.POINTER(ct.c_double)
 c_int32_p = ct.POINTER(ct.c_int32)
@@ -31,7 +33,7 @@ class VpbsParams(ct.Structure):
         ("nquad_near", ct.c_int32), ("quad_near_zeta", ct.c_double * 16), ("quad_near_w", ct.c_double * 16),
         ("lia_segment_fraction", ct.c_double), ("avoid_explicit_erf", ct.c_int32),
         ("truncate_spherical", ct.c_int32), ("nsubdiv", ct.c_int32), ("precision", ct.c_int32),
-        ("device", ct.c_int32),
+        ("device", ct.c_int32), ("splitting", ct.c_int32), ("kb_beta", ct.c_double), ("kb_rtol", ct.c_double),
     ]
 
 
@@ -63,6 +65,8 @@ SIGNATURES = {
     "vpbs_stage_name": (ct.c_char_p, [ct.c_int32]),
     "vpbs_fma_throughput": (ct.c_int, [ct.c_int32, ct.c_int32, c_double_p]),
     "vpbs_ewald_table_eval": (ct.c_int, [ct.c_double, c_double_p, ct.c_int64, c_double_p, c_double_p]),
+    "vpbs_kb_weights": (ct.c_int, [ct.c_double, ct.c_double, ct.c_double, c_double_p, ct.c_int64, c_double_p,
+                                   c_double_p, c_double_p, c_double_p]),
     "vpbs_point_data_noalloc": (ct.c_int, [ct.POINTER(VpbsParams), ct.c_int64, c_int64_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p]),

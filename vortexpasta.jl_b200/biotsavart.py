@@ -18,7 +18,7 @@ import numpy as np
 
 from . import _lib
 from .curves import concat
-from .params import NoSplitting, ParamsBiotSavart
+from .params import KaiserBesselSplitting, NoSplitting, ParamsBiotSavart
 
 
 def _c_params(p: ParamsBiotSavart) -> _lib.VpbsParams:
@@ -31,6 +31,12 @@ def _c_params(p: ParamsBiotSavart) -> _lib.VpbsParams:
         for d in range(3):
             c.L[d] = 0.0
             c.Ns[d] = 0
+    elif isinstance(sp, KaiserBesselSplitting):
+        c.splitting = _lib.SPLITTING_KAISER_BESSEL
+        c.alpha, c.rcut, c.kb_beta, c.kb_rtol = 0.0, sp.rcut, sp.beta, sp.rtol
+        for d in range(3):
+            c.L[d] = sp.Ls[d]
+            c.Ns[d] = sp.Ns[d]
     else:
         c.alpha, c.rcut = sp.alpha, sp.rcut
         for d in range(3):

@@ -17,7 +17,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT_DIR = PKG / "lib"
 LIB = OUT_DIR / "libvpbs.so"
-SOURCES = ["api.cu", "geometry.cu", "shortrange.cu", "longrange.cu", "features.cu", "mlp.cu", "timestep.cu", "diagnostics.cu"]
+SOURCES = ["api.cu", "geometry.cu", "shortrange.cu", "longrange.cu", "features.cu", "mlp.cu", "timestep.cu", "diagnostics.cu", "splitting.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -137,14 +137,24 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
         return set_error(nullptr, VPBS_ERR_PARAMS, "lia_segment_fraction must be in (0, 1]");
     if (P.precision != VPBS_PRECISION_FP64 && P.precision != VPBS_PRECISION_MIXED)
         return set_error(nullptr, VPBS_ERR_PARAMS, "precision must be VPBS_PRECISION_FP64 or VPBS_PRECISION_MIXED");
-    if (P.precision == VPBS_PRECISION_MIXED && !(P.alpha > 0))
+    if (P.splitting != VPBS_SPLITTING_GAUSSIAN && P.splitting != VPBS_SPLITTING_KAISER_BESSEL)
+        return set_error(nullptr, VPBS_ERR_PARAMS, "splitting must be VPBS_SPLITTING_GAUSSIAN or VPBS_SPLITTING_KAISER_BESSEL");
+    const bool kb = P.splitting == VPBS_SPLITTING_KAISER_BESSEL;
+    if (kb && !(P.kb_beta > 0 && std::isfinite(P.kb_beta)))
+        return set_error(nullptr, VPBS_ERR_PARAMS, "KaiserBesselSplitting: beta must be positive and finite");
+    if (kb && !(P.kb_rtol > 0 && P.kb_rtol < 1))
+        return set_error(nullptr, VPBS_ERR_PARAMS, "KaiserBesselSplitting: rtol must be in (0, 1)");
+    const bool open = !kb && !(P.alpha > 0);
+    if (P.precision == VPBS_PRECISION_MIXED && open)
         return set_error(nullptr, VPBS_ERR_PARAMS, "the mixed-precision form needs Ewald splitting (alpha > 0)");
-    const bool open = !(P.alpha > 0);
     KParams K{};
     K.Gamma = P.Gamma;
     K.a = P.a;
     K.Delta = P.Delta;
-    K.alpha = open ? 0.0 : P.alpha;
+    K.kb = kb ? 1 : 0;
+    // scale of the weight-table variable x = alpha r (the Gaussian alpha, or the table scale of
+    // the Kaiser-Bessel weights)
+    K.alpha = open ? 0.0 : (kb ? (P.rcut > 0 ? kb_table_xmax(P.kb_beta) / P.rcut : 0.0) : P.alpha);
     K.open_domain = open ? 1 : 0;
     K.nquad = P.nquad;
     K.nquad_near = P.nquad_near > 0 ? P.nquad_near : P.nquad;
@@ -216,12 +226,22 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
     h->stream = h->own_stream;
     if (!rc && !open) rc = longrange_init(h);
     if (!rc && !open) {
-        // Ewald weight tables over x = alpha r in [0, alpha rcut]
+        // Ewald weight tables over x = alpha r in [0, alpha rcut]: erfc-based for the Gaussian,
+        // fitted to the truncated Chebyshev series for the Kaiser-Bessel kernel
         int ntab = 0;
-        const double xmax = P.alpha * P.rcut;
-        ewald_table_host(xmax, &ntab, nullptr);
-        std::vector<double> tab((size_t)2 * ntab * kEwaldNC);
-        ewald_table_host(xmax, &ntab, tab.data());
+        std::vector<double> tab;
+        if (kb) {
+            const KBSeries S = kb_series(P.kb_beta, P.rcut, P.kb_rtol);
+            if (S.f.empty()) rc = set_error(h, VPBS_ERR_PARAMS, "KaiserBesselSplitting: Chebyshev series did not converge");
+            kb_table_host(S, &ntab, nullptr);
+            tab.resize((size_t)2 * ntab * kEwaldNC);
+            if (!rc) kb_table_host(S, &ntab, tab.data());
+        } else {
+            const double xmax = P.alpha * P.rcut;
+            ewald_table_host(xmax, &ntab, nullptr);
+            tab.resize((size_t)2 * ntab * kEwaldNC);
+            ewald_table_host(xmax, &ntab, tab.data());
+        }
         // FP32 copy: the leading kEwaldNCf coefficients of each interval, stored after the FP64 table
         std::vector<float> tabf((size_t)2 * ntab * kEwaldNCf);
         for (size_t k = 0; k < (size_t)2 * ntab; ++k)
@@ -234,7 +254,7 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
                 tab2[2 * (k * kEwaldNC + n) + 1] = tab[(ntab + k) * kEwaldNC + n];
             }
         const size_t bytes_d = sizeof(double) * tab.size(), bytes_f = sizeof(float) * tabf.size();
-        rc = ensure(h, h->ewald_tab, 2 * bytes_d + bytes_f, "Ewald tables");
+        if (!rc) rc = ensure(h, h->ewald_tab, 2 * bytes_d + bytes_f, "Ewald tables");
         if (!rc)
             rc = check_cuda(h, cudaMemcpy((char*)h->ewald_tab.p + bytes_d + bytes_f, tab2.data(), bytes_d,
                                           cudaMemcpyHostToDevice), "copy Ewald tables");

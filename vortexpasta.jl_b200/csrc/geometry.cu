@@ -535,7 +535,7 @@ extern "C" int vpbs_point_data_noalloc(const vpbs_params* params, int64_t nfil, 
     if (P.lia_segment_fraction > 1.0) return set_error(nullptr, VPBS_ERR_PARAMS, "lia_segment_fraction must be in (0, 1]");
     KParams K{};
     K.Gamma = P.Gamma;
-    K.open_domain = P.alpha > 0 ? 0 : 1;
+    K.open_domain = (P.splitting == VPBS_SPLITTING_KAISER_BESSEL || P.alpha > 0) ? 0 : 1;
     for (int d = 0; d < 3; ++d) {
         K.L[d] = K.open_domain ? 0.0 : P.L[d];
         K.Lh[d] = K.L[d] / 2;

@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(256) spread_kernel_atomic(
 template <typename C>
 __global__ void __launch_bounds__(256) fourier_kernel(
     LRSizes S, double pref, double k0x, double k0y, double k0z, int truncate, double kmax2, int fields,
+    double kb_beta2, double kb_rc2, double kb_c,
     const double* __restrict__ dec0, const double* __restrict__ dec1, const double* __restrict__ dec2,
     const double* __restrict__ decE0, const double* __restrict__ decE1, const double* __restrict__ decE2,
     C* __restrict__ gc, C* __restrict__ gc2, double2* __restrict__ uhat, int store_uhat) {
@@ -181,7 +182,18 @@ __global__ void __launch_bounds__(256) fourier_kernel(
         }
         if (live) {
             const double k2inv = (k2 == 0.0) ? 0.0 : 1.0 / k2;
-            const double g = decE0[ix] * decE1[ry] * decE2[rz];
+            double g = decE0[ix] * decE1[ry] * decE2[rz];
+            if (kb_beta2 > 0.0) {
+                // Kaiser-Bessel filter (kaiser_bessel.jl:266-278): beta / sinh(beta) sinh(q) / q,
+                // q = sqrt(beta^2 - k^2 rcut^2), zero beyond k = beta / rcut
+                const double sq = kb_beta2 - k2 * kb_rc2;
+                if (sq > 0.0) {
+                    const double q = sqrt(sq);
+                    g *= kb_c * sinh(q) / q;
+                } else {
+                    g = 0.0;
+                }
+            }
             if (fields & VPBS_VELOCITY) {
                 // i k x w / k^2 ; (i w).x = -w.y, (i w).y = w.x
                 const double2 iw0 = make_double2(-w[0].y, w[0].x), iw1 = make_double2(-w[1].y, w[1].x),
@@ -548,9 +560,11 @@ int longrange_init(vpbs_handle* h) {
     if ((rc = ensure(h, h->grid_c, 2 * rsz * 3 * S.ncgrid, "complex grid"))) return rc;
     if ((rc = ensure(h, h->grid_c2, 2 * rsz * 3 * S.ncgrid, "complex grid (streamfunction)"))) return rc;
     if ((rc = ensure(h, h->uhat, sizeof(double2) * 3 * S.nmodes, "uhat"))) return rc;
-    // separable deconvolution factors 1/psi_hat and 1/psi_hat * exp(-k^2 / 4 alpha^2)
+    // separable deconvolution factors 1/psi_hat and 1/psi_hat * exp(-k^2 / 4 alpha^2) (the
+    // Kaiser-Bessel filter is not separable: the Fourier kernel applies it per mode)
     std::vector<double> tab[6];
-    const double beta_g = -1.0 / (4.0 * P.alpha * P.alpha);
+    const bool kb = P.splitting == VPBS_SPLITTING_KAISER_BESSEL;
+    const double beta_g = kb ? 0.0 : -1.0 / (4.0 * P.alpha * P.alpha);
     for (int d = 0; d < 3; ++d) {
         const int len = d == 0 ? S.nkx : S.Ns[d];
         tab[d].resize(len);
@@ -680,6 +694,7 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
     double kmax = INFINITY;
     for (int d = 0; d < 3; ++d) kmax = fmin(kmax, 2.0 * kPi * ((P.Ns[d] - 1) / 2) / P.L[d]);
     const double pref = P.Gamma / (P.L[0] * P.L[1] * P.L[2]);
+    const bool kb = P.splitting == VPBS_SPLITTING_KAISER_BESSEL;
     const double* t = (const double*)h->decx.p;
     const double* dec0 = t;
     const double* dec1 = dec0 + S.nkx;
@@ -690,7 +705,8 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
     {
         StageScope st(h, ST_FOURIER);
         fourier_kernel<C><<<grid_for(S.ncgrid, 256), 256, 0, h->stream>>>(
-            S, pref, sx[0], sx[1], sx[2], P.truncate_spherical, kmax * kmax, fields, dec0, dec1, dec2, decE0, decE1,
+            S, pref, sx[0], sx[1], sx[2], P.truncate_spherical, kmax * kmax, fields, kb ? P.kb_beta * P.kb_beta : 0.0,
+            P.rcut * P.rcut, kb ? P.kb_beta / std::sinh(P.kb_beta) : 0.0, dec0, dec1, dec2, decE0, decE1,
             decE2, gc, gc2, (double2*)h->uhat.p, 1);
         h->launches++;
         h->have_uhat = true;

@@ -802,7 +802,16 @@ __global__ void __launch_bounds__(128) local_self_kernel(
                 const double rinv = 1.0 / rr;
                 const double qc[3] = {charges[j], charges[Nq + j], charges[2 * Nq + j]};
                 double fa = 1.0, fb = 0.0;
-                if (explicit_erf) {
+                if (explicit_erf && K.kb) {
+                    // weights_longrange of the Kaiser-Bessel kernel (kaiser_bessel.jl:296-301):
+                    // (F(r), r f(r)) = (1 - a, g - a) inside rcut, (1, 0) beyond
+                    if (rr < K.rcut) {
+                        double wa, wg;
+                        ewald_weights2(K, K.alpha * rr, wa, wg);
+                        fa = 1.0 - wa;
+                        fb = wg - wa;
+                    }
+                } else if (explicit_erf) {
                     const double ar = K.alpha * rr;
                     fa = erf(ar);
                     fb = 1.1283791670955126 * ar * exp(-(ar * ar));

@@ -27,6 +27,7 @@ struct KParams {
     double lia_fraction;  // <= 0: nothing
     int avoid_explicit_erf;
     int open_domain;      // NoSplitting
+    int kb;               // KaiserBesselSplitting: the long-range weights vanish beyond rcut
     // piecewise Taylor tables of erfc(x) and erfc(x) + 2/sqrt(pi) x exp(-x^2), x = alpha r
     const double* ewald_tab;
     const float* ewald_tab_f;  // FP32 copy (first kEwaldNCf coefficients) for the mixed form
@@ -42,6 +43,18 @@ constexpr double kEwaldInvH = 16.0;
 constexpr double kEwaldH = 1.0 / 16.0;
 void ewald_table_host(double xmax, int* ntab, double* tab);  // tab: 2 * ntab * kEwaldNC doubles
 int ewald_table_size(double xmax);
+
+// Kaiser-Bessel splitting (splitting.cu): the reference's truncated Chebyshev series of the kernel
+// f and of its integral F (full coefficient vectors in u = r / rcut), and their weight tables in
+// the layout of ewald_table_host over x = (kb_table_xmax(beta) / rcut) r.
+struct KBSeries {
+    double beta = 0.0, rcut = 0.0;
+    std::vector<double> f, F;
+};
+KBSeries kb_series(double beta, double rcut, double rtol);
+void kb_weights_series(const KBSeries& S, double r, double* a, double* g);
+double kb_table_xmax(double beta);
+void kb_table_host(const KBSeries& S, int* ntab, double* tab);
 
 __device__ __forceinline__ void ewald_weights(const KParams& K, double x, double& a, double& g) {
     int k = (int)(x * kEwaldInvH);

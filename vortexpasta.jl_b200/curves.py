@@ -37,6 +37,15 @@ def ring(n: int, radius: float, center=(0.0, 0.0, 0.0), rotation: np.ndarray | N
     return x + np.asarray(center, dtype=np.float64)
 
 
+def trefoil(n: int, R: float = np.pi / 3) -> np.ndarray:
+    """Trefoil knot of the reference's tests (PredefinedCurves/trefoil.jl:22-35, test/trefoil.jl:16-19):
+    R (1 + (sin 2 pi t + 2 sin 4 pi t, cos 2 pi t - 2 cos 4 pi t, -sin 6 pi t)) at t = (i - 1) / n."""
+    u = 2 * np.arange(n) / n
+    X = np.stack([np.sin(np.pi * u) + 2 * np.sin(2 * np.pi * u), np.cos(np.pi * u) - 2 * np.cos(2 * np.pi * u),
+                  -np.sin(3 * np.pi * u)], axis=1)
+    return R + R * X
+
+
 def random_rotation(rng: np.random.Generator) -> np.ndarray:
     """Uniformly distributed rotation matrix (Shoemake 1992, uniform unit quaternion)."""
     u1, u2, u3 = rng.random(3)

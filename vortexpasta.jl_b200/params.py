@@ -1,5 +1,5 @@
 """Parameter types mirroring VortexPasta.BiotSavart's (src/BiotSavart/params.jl,
-src/BiotSavart/splitting/gaussian.jl, the two backends and src/Quadratures).
+src/BiotSavart/splitting/gaussian.jl and kaiser_bessel.jl, the two backends and src/Quadratures).
 
 Names, keyword arguments, defaults and the errors raised at construction follow the
 reference; the backends name the CUDA implementations that replace the reference's
@@ -106,6 +106,62 @@ class GaussianSplitting:
     @property
     def beta_longrange(self):
         return maximum_wavenumber(self.Ns, self.Ls) / (2 * self.alpha)
+
+
+C_RTOL_KB = 10 ** (-0.2)  # empirical constant of rtol(beta) ~ C exp(-beta) (kaiser_bessel.jl:104-109)
+
+
+class KaiserBesselSplitting:
+    """KaiserBesselSplitting (splitting/kaiser_bessel.jl:130-223).
+
+    Pass ``Ls`` and either ``beta`` or ``rtol`` plus one of ``rcut``, ``Ns``:
+    ``beta`` and ``rcut`` give ``Ns`` from k_max = beta / rcut; ``beta`` and ``Ns`` give
+    ``rcut = beta / k_max``; ``rtol`` sets ``beta = -log(rtol / C)``; ``rcut`` and ``Ns`` give
+    ``beta = rcut k_max``.  When ``rtol`` is not given it is ``C exp(-beta)`` with C = 10^-0.2.
+    The short-range weights 1 - F(r) and r F'(r) vanish beyond ``rcut`` (compact support); the
+    long-range filter is beta / sinh(beta) sinh(q) / q with q = sqrt(beta^2 - (k rcut)^2).
+    """
+    beta: float
+    rcut: float
+    Ns: tuple
+    rtol: float
+
+    def __init__(self, *, Ls, beta=None, rcut=None, Ns=None, rtol=None):
+        Ls = tuple(float(L) for L in (Ls if np.ndim(Ls) else (Ls,) * 3))
+        given = (beta is not None, rcut is not None, Ns is not None, rtol is not None)
+        if Ns is not None:
+            Ns = tuple(int(n) for n in (Ns if np.ndim(Ns) else (Ns,) * 3))
+        if given == (True, True, False, False):
+            Ns = tuple(kmax_to_gridsize(beta / rcut, L) for L in Ls)
+            rtol = C_RTOL_KB * math.exp(-beta)
+        elif given == (False, True, True, False):
+            beta = rcut * maximum_wavenumber(Ns, Ls)
+            rtol = C_RTOL_KB * math.exp(-beta)
+        elif given == (True, False, True, False):
+            rcut = beta / maximum_wavenumber(Ns, Ls)
+            rtol = C_RTOL_KB * math.exp(-beta)
+        elif given == (False, True, False, True):
+            beta = -math.log(rtol / C_RTOL_KB)
+            Ns = tuple(kmax_to_gridsize(beta / rcut, L) for L in Ls)
+        elif given == (False, False, True, True):
+            beta = -math.log(rtol / C_RTOL_KB)
+            rcut = beta / maximum_wavenumber(Ns, Ls)
+        else:
+            raise TypeError("KaiserBesselSplitting: pass `beta` or `rtol` and one of `rcut`, `Ns`; or `rcut` and `Ns`")
+        self.Ls, self.beta, self.rcut, self.Ns, self.rtol = Ls, float(beta), float(rcut), Ns, float(rtol)
+
+    def __repr__(self):
+        return (f"KaiserBesselSplitting(Ls={self.Ls}, beta={self.beta}, rcut={self.rcut}, Ns={self.Ns}, "
+                f"rtol={self.rtol})")
+
+    def fourier_kernel(self, k2):
+        """Long-range filter as a function of k^2 (kaiser_bessel.jl:266-278)."""
+        k2 = np.asarray(k2, dtype=float)
+        s = self.beta ** 2 - k2 * self.rcut ** 2
+        q = np.sqrt(np.maximum(s, 0.0))
+        with np.errstate(invalid="ignore", divide="ignore"):
+            v = self.beta / math.sinh(self.beta) * np.where(q > 0, np.sinh(q) / np.where(q > 0, q, 1.0), 1.0)
+        return np.where(s > 0, v, 0.0)
 
 
 @dataclass(frozen=True)
