@@ -187,10 +187,10 @@ def test_mixed_precision_flags(vp, oracle, built_lib, LIA):
     assert rel(v, vo) < MIXED_TOL and rel(psi, po) < MIXED_TOL
 
 
-@pytest.mark.parametrize("sigma,m", [(1.5, 6), (1.25, 3), (2.0, 8)])
+@pytest.mark.parametrize("sigma,m", [(1.5, 6), (1.25, 3), (2.0, 8), (2.0, 2), (1.5, 1)])
 def test_mixed_precision_kernel_widths(vp, oracle, built_lib, sigma, m):
-    """Mixed form with other NUFFT widths (FP32 brick spreading and interpolation tables of
-    up to 3 x 16 entries)."""
+    """Mixed form with other NUFFT widths: plane-owner spreading with 8- and 4-wide patches
+    (m = 3, 2, 1), register columns (m = 6, 8), interpolation tables of up to 3 x 16 entries."""
     fs, p = vp.configs.tangle20k(precision="mixed")
     fs = fs[:25]
     p = p.with_(backend_long=vp.NonuniformFFTsBackend(sigma, m))

@@ -348,6 +348,181 @@ __global__ void __launch_bounds__(kBrickThreads) spread_brick_kernel(
     }
 }
 
+// Plane-owner brick spreading for FP32 grids and narrow kernels (w = 2m <= 8), 16^3 bricks, no
+// atomics: one CTA of 16 warps per brick, warp z owning the brick's z-plane z in shared memory.
+// The candidate points (those of the 8 bins whose footprints can reach the brick) are tested one
+// per thread and only the overlapping ones are staged, in batches, as brick-aligned, zero-padded
+// kernel rows (px, py, pz of 16 values; 8 threads per point) together with one slot list per
+// plane.  Each warp then walks the list of its plane and adds, for every listed point, a P x P
+// patch of (x, y) cells starting at the footprint corner (P = 4 for w <= 4, 8 for w <= 8; cells
+// past the footprint multiply a zero kernel value) with plain read-modify-writes: the plane has
+// one writer and the lanes of one instruction hold distinct cells.  The x-row stride RX puts the 32 / P rows of one instruction
+// in disjoint banks (RX = 24 for P = 8: row offsets 0, 24, 16, 8; RX = 20 for P = 4).
+// Measured on the B200: FP32 shared atomicAdd sustains 2.0 T updates/s conflict-free against
+// 4.2 T for plain read-modify-writes, and the per-point work (footprint tests, kernel rows) is
+// done once per point and batch instead of by every lane of a warp.
+constexpr int kPlaneB = 16;
+constexpr int kPlaneThreads = 512;
+constexpr int kPlaneBatch = 128;
+
+template <int P>
+struct PlaneLayout {
+    static constexpr int RX = P == 8 ? 24 : 20;  // x-row stride
+    static constexpr int PL = kPlaneB * RX;      // z-plane stride
+    static constexpr int TC = kPlaneB * PL;      // floats per component
+};
+
+// One staged point: charges, the w kernel values per dimension zero-padded to P entries, and the
+// footprint corner in brick coordinates (may be negative).
+template <int P>
+struct __align__(16) PlaneSlot {
+    float q[4];
+    float px[P], py[P], pz[P];
+    int xs, ys, zs, pad;
+};
+
+template <int P>
+__global__ void __launch_bounds__(kPlaneThreads, 2) spread_plane_kernel(
+    LRSizes S, int nb0, int nb1, int nb2, const int32_t* __restrict__ bin_start, const float* __restrict__ binned,
+    const int32_t* __restrict__ foot, float* __restrict__ grid) {
+    using Lay = PlaneLayout<P>;
+    extern __shared__ __align__(16) float ptile[];  // [3][16 planes][16 rows][RX]
+    __shared__ PlaneSlot<P> slot[kPlaneBatch];
+    __shared__ int32_t pend_j[kPlaneThreads];        // overlapping candidates of the current chunk
+    __shared__ int16_t pend_o[kPlaneThreads][3];     // their footprint corners (brick coordinates)
+    __shared__ uint8_t plist[kPlaneB][kPlaneBatch];  // slots covering each plane
+    __shared__ int pcount[kPlaneB];
+    __shared__ int npend;
+    __shared__ int nbin_start[8], nbin_base[9];
+    const int w = 2 * S.m;
+    const int stride = 3 + 3 * w;
+    const int bx = blockIdx.x % nb0;
+    const int by = (blockIdx.x / nb0) % nb1;
+    const int bz = blockIdx.x / (nb0 * nb1);
+    const int bs[3] = {bx * kPlaneB, by * kPlaneB, bz * kPlaneB};
+    const int lane = threadIdx.x & 31, z = threadIdx.x >> 5;  // warp z owns plane z
+    for (int i = threadIdx.x; i < 3 * Lay::TC; i += kPlaneThreads) ptile[i] = 0.0f;
+    if (threadIdx.x < 8) {
+        const int nbr = threadIdx.x;
+        const int cx = (bx - (nbr & 1) + nb0) % nb0;
+        const int cy = (by - ((nbr >> 1) & 1) + nb1) % nb1;
+        const int cz = (bz - ((nbr >> 2) & 1) + nb2) % nb2;
+        const int b = (cz * nb1 + cy) * nb0 + cx;
+        nbin_start[nbr] = bin_start[b];
+        nbin_base[nbr + 1] = bin_start[b + 1] - bin_start[b];
+    }
+    if (threadIdx.x < kPlaneB) pcount[threadIdx.x] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        nbin_base[0] = 0;
+        for (int k = 1; k <= 8; ++k) nbin_base[k] += nbin_base[k - 1];
+    }
+    __syncthreads();
+    const int ntot = nbin_base[8];
+    // this lane's cells of the P x P patch: (cell % P, cell / P) for cell = lane + 32 it
+    constexpr int kIter = (P * P + 31) / 32;
+    int cxo[kIter], cyo[kIter];
+#pragma unroll
+    for (int it = 0; it < kIter; ++it) {
+        const int cell = lane + 32 * it;
+        cxo[it] = cell % P;
+        cyo[it] = cell < P * P ? cell / P : 0;
+    }
+    const bool live0 = lane < P * P;  // lanes past the patch (P = 4: 16 cells) stay idle
+    float* plane = ptile + z * Lay::PL;
+    for (int c0 = 0; c0 < ntot; c0 += kPlaneThreads) {
+        // ---- 1: keep the candidates of this chunk whose footprint meets the brick ----
+        if (threadIdx.x == 0) npend = 0;
+        __syncthreads();
+        {
+            const int k = c0 + threadIdx.x;
+            if (k < ntot) {
+                int nb = 0;
+#pragma unroll
+                for (int i = 1; i < 8; ++i) nb += k >= nbin_base[i];
+                const int32_t j = nbin_start[nb] + (k - nbin_base[nb]);
+                int o[3];
+                bool empty = false;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    o[d] = foot[3 * (int64_t)j + d] - bs[d];
+                    if (o[d] >= kPlaneB) o[d] -= S.n[d];
+                    empty = empty || o[d] + w <= 0 || o[d] >= kPlaneB;
+                }
+                if (!empty) {
+                    const int q = atomicAdd(&npend, 1);
+                    pend_j[q] = j;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) pend_o[q][d] = (int16_t)o[d];
+                }
+            }
+        }
+        __syncthreads();
+        const int np = npend;
+        for (int p0 = 0; p0 < np; p0 += kPlaneBatch) {
+            const int nbatch = np - p0 < kPlaneBatch ? np - p0 : kPlaneBatch;
+            // ---- 2: stage the points (4 threads per slot) and the per-plane slot lists ----
+            {
+                const int sidx = threadIdx.x >> 2, part = threadIdx.x & 3;
+                if (sidx < nbatch) {
+                    PlaneSlot<P>& sl = slot[sidx];
+                    const int q = p0 + sidx;
+                    const float* src = binned + (int64_t)pend_j[q] * stride;
+                    // part d < 3: kernel row d (w values, zero-padded to P); part 3: charges, corner
+                    if (part < 3) {
+                        float* row = part == 0 ? sl.px : part == 1 ? sl.py : sl.pz;
+#pragma unroll
+                        for (int r = 0; r < P; ++r) row[r] = r < w ? src[3 + part * w + r] : 0.0f;
+                    } else {
+                        sl.q[0] = src[0];
+                        sl.q[1] = src[1];
+                        sl.q[2] = src[2];
+                        sl.xs = pend_o[q][0];
+                        sl.ys = pend_o[q][1];
+                        sl.zs = pend_o[q][2];
+                    }
+                    // planes [max(o2, 0), min(o2 + w, 16)), split over the slot's 4 threads
+                    const int o2 = pend_o[q][2];
+                    const int zlo = o2 < 0 ? 0 : o2, zhi = o2 + w < kPlaneB ? o2 + w : kPlaneB;
+                    for (int zz = zlo + part; zz < zhi; zz += 4) {
+                        const int pos = atomicAdd(&pcount[zz], 1);
+                        plist[zz][pos] = (uint8_t)sidx;
+                    }
+                }
+            }
+            __syncthreads();
+            // ---- 3: warp z adds the patches of the slots covering plane z ----
+            const int nz = pcount[z];
+            for (int t = 0; t < nz; ++t) {
+                const PlaneSlot<P>& sl = slot[plist[z][t]];
+                const float fz = sl.pz[z - sl.zs];
+                const float a0 = sl.q[0] * fz, a1 = sl.q[1] * fz, a2 = sl.q[2] * fz;
+                const int xs = sl.xs, ys = sl.ys;
+#pragma unroll
+                for (int it = 0; it < kIter; ++it) {
+                    const int cx = xs + cxo[it], cy = ys + cyo[it];
+                    if (live0 && (unsigned)cx < (unsigned)kPlaneB && (unsigned)cy < (unsigned)kPlaneB) {
+                        const float g = sl.px[cxo[it]] * sl.py[cyo[it]];
+                        float* cell = plane + cy * Lay::RX + cx;
+                        cell[0] = fmaf(a0, g, cell[0]);
+                        cell[Lay::TC] = fmaf(a1, g, cell[Lay::TC]);
+                        cell[2 * Lay::TC] = fmaf(a2, g, cell[2 * Lay::TC]);
+                    }
+                }
+            }
+            if (lane == 0) pcount[z] = 0;  // read above by this warp only; refilled after the barrier
+            __syncthreads();
+        }
+    }
+    const int64_t ng = S.ngrid;
+    for (int i = threadIdx.x; i < 3 * kPlaneB * kPlaneB * kPlaneB; i += kPlaneThreads) {
+        const int c = i / (kPlaneB * kPlaneB * kPlaneB), r = i % (kPlaneB * kPlaneB * kPlaneB);
+        const int x = r % kPlaneB, y = (r / kPlaneB) % kPlaneB, zz = r / (kPlaneB * kPlaneB);
+        grid[c * ng + ((int64_t)(bs[2] + zz) * S.n[1] + (bs[1] + y)) * S.n[0] + bs[0] + x] =
+            ptile[c * Lay::TC + zz * Lay::PL + y * Lay::RX + x];
+    }
+}
+
 // Register-column brick spreading for 16^3 bricks (no atomics at all): the 256 threads of a CTA
 // are the 16 x 16 (x, y) columns of the brick and each keeps its column's 16 z values of the
 // three components in registers.  The points whose footprint meets the brick are staged in
@@ -659,14 +834,21 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             kern<<<nblk, kBrickThreads, smem, h->stream>>>(S, nb0, nb1, nb2, start, bsrc, foot, grid);
         };
+        // plane-owner kernel (FP32 grids only; the branch that calls it is never taken for T = double)
+        auto launch_plane = [&](void (*kern)(LRSizes, int, int, int, const int32_t*, const float*, const int32_t*,
+                                             float*), int P) {
+            const size_t psmem = sizeof(float) * 3 * kPlaneB * kPlaneB * (P == 8 ? PlaneLayout<8>::RX : PlaneLayout<4>::RX);
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
+            kern<<<nblk, kPlaneThreads, psmem, h->stream>>>(S, nb0, nb1, nb2, start, (const float*)bsrc, foot,
+                                                           (float*)grid);
+        };
         switch (B) {
             case kColB:
-                // FP32 grids with narrow kernels (m <= 4): shared-memory atomics are native and beat
-                // the 16-deep register columns, which mostly multiply zeros there (1M tangle, m = 3:
-                // 5.2 vs 7.2 ms); wider kernels (m = 5: 13.5 vs 10.1 ms) and FP64 grids (no FP64
-                // shared atomics) use the columns
+                // FP32 grids with narrow kernels (m <= 4): the plane-owner kernel (the 16-deep
+                // register columns mostly multiply zeros there); wider kernels and FP64 grids use
+                // the columns
                 if (std::is_same<T, float>::value && S.m <= 4)
-                    launch(spread_brick_kernel<16, T>);
+                    launch_plane(S.m <= 2 ? spread_plane_kernel<4> : spread_plane_kernel<8>, S.m <= 2 ? 4 : 8);
                 else
                     spread_column_kernel<T><<<nblk, kColThreads, 0, h->stream>>>(S, nb0, nb1, nb2, start, bsrc, foot,
                                                                                  grid);

@@ -90,6 +90,53 @@ class EwaldChoice:
         return asdict(self)
 
 
+@dataclass(frozen=True)
+class KBChoice:
+    """One parameter set of a Kaiser-Bessel split (kaiser_bessel.jl) and its NUFFT: shape
+    parameter beta (short-range weights and long-range filter alike), r_cut, the Fourier grid
+    and the Chebyshev truncation rtol (C exp(-beta) unless given)."""
+    beta: float
+    rcut: float
+    Ns: int
+    sigma: float
+    m: int
+    rtol: float = 0.0
+
+    @property
+    def beta_short(self) -> float:
+        return self.beta
+
+    def beta_long(self, L: float) -> float:
+        return 2 * math.pi * ((self.Ns - 1) // 2) / L * self.rcut
+
+    def fft_size(self) -> int:
+        return fft_size(self.Ns, self.sigma)
+
+    def splitting(self, L: float):
+        from .params import C_RTOL_KB, KaiserBesselSplitting
+        sp = KaiserBesselSplitting(Ls=L, beta=self.beta, rcut=self.rcut)
+        sp.Ns = (self.Ns,) * 3
+        sp.rtol = self.rtol if self.rtol > 0 else C_RTOL_KB * math.exp(-self.beta)
+        return sp
+
+    def params(self, L: float, precision: str = "mixed", Gamma=1.0, a=1e-8, Delta=0.25, nquad=3,
+               **kw) -> ParamsBiotSavart:
+        return ParamsBiotSavart(Gamma=Gamma, a=a, Delta=Delta, splitting=self.splitting(L),
+                                quadrature=GaussLegendre(nquad), backend_long=NonuniformFFTsBackend(self.sigma, self.m),
+                                precision=precision, **kw)
+
+    def as_dict(self) -> dict:
+        return {**asdict(self), "splitting": "kaiser_bessel"}
+
+
+def kb_choice_from(L: float, rcut: float, beta: float, sigma: float, m: int, beta_long: float | None = None) -> KBChoice:
+    """Kaiser-Bessel parameters at cut-off `rcut`: the grid resolves k_max = beta_long / rcut
+    (beta_long = beta by default, the reference's rule), rounded like ``choice_from``."""
+    bl = beta if beta_long is None else beta_long
+    Ns = grid_for(kmax_to_gridsize(bl / rcut, L), sigma, m)
+    return KBChoice(beta=beta, rcut=rcut, Ns=Ns, sigma=sigma, m=m)
+
+
 def choice_from(L: float, rcut: float, beta_short: float, beta_long: float, sigma: float, m: int) -> EwaldChoice:
     alpha = beta_short / rcut
     Ns = grid_for(kmax_to_gridsize(2 * alpha * beta_long, L), sigma, m)
