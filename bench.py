@@ -478,9 +478,14 @@ def run_ours(args):
                                              "beta": choice.beta_short},
                               "predictor": {"fallback_to_default_rule": bool(info["fallback"]),
                                             "checked_rel_l2": info.get("rel_l2"), "rtol": args.rtol,
-                                            "seconds": t_choose},
+                                            "seconds": t_choose,
+                                            "candidates": [{k: a[k] for k in ("rel_l2", "ms") if k in a} |
+                                                           {"splitting": a.get("splitting", "gaussian")}
+                                                           for a in info["attempts"]]},
                               "stages_ms": {k: v["ms"] for k, v in fh["stages"].items()},
-                              "description": "mixed precision at parameters predicted by the learned MLP"}
+                              "description": ("mixed precision at the cut-off and NUFFT predicted by the learned MLP; "
+                                              "Gaussian or Kaiser-Bessel split, whichever met the tolerance in less "
+                                              "time in the FP64-checked trial")}
         line = {
             "metric": METRIC, "value": fh["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": fh["ms_per_step"], "higher_is_better": True, "scaling": "weak",

@@ -69,7 +69,7 @@ def evaluate(model, n, seed, out):
         fs = learned.random_configuration(rng, L)
         N = sum(len(f) for f in fs)
         vref = learned.reference_velocity(fs, L)
-        ch, info = learned.choose_parameters(fs, L, pred.rtol, pred)
+        ch, info = learned.choose_parameters(fs, L, pred.rtol, pred, kaiser_bessel=False)
         ms_p, v_p = tuning.measure(fs, ch, L, "mixed")
         d = tuning.default_rule(L, pred.rtol, learned.FEATURE_RCUT * L)
         ms_d, v_d = tuning.measure(fs, d, L, "mixed")
