@@ -479,7 +479,7 @@ def run_ours(args):
                               "predictor": {"fallback_to_default_rule": bool(info["fallback"]),
                                             "checked_rel_l2": info.get("rel_l2"), "rtol": args.rtol,
                                             "seconds": t_choose,
-                                            "candidates": [{k: a[k] for k in ("rel_l2", "ms") if k in a} |
+                                            "candidates": [{k: a[k] for k in ("rel_l2", "ms", "sigma", "m", "fft") if k in a} |
                                                            {"splitting": a.get("splitting", "gaussian")}
                                                            for a in info["attempts"]]},
                               "stages_ms": {k: v["ms"] for k, v in fh["stages"].items()},
