@@ -249,12 +249,33 @@ int vpbs_fma_throughput(int32_t device, int32_t fp64, double* tflops);
 
 /* ---- Diagnostics (src/Diagnostics/spectra.jl:84-232, spectra_helicity.jl:43-76) ---- */
 
-/* Energy (kind 0) or helicity (kind 1) spectrum of the vorticity coefficients left by the last
- * long-range computation (the field of vpbs_get_uhat), summed over spherical shells of width dk:
- * out[n] for k_n = n dk, n = 0..nk-1 (bin n = trunc(|k|/dk + 1/2), weight 1/2 on the kx = 0
- * plane).  Energy: sum of |w_k|^2/k^2/dk; helicity: sum of 2 V Re[(i k x w_k)^* . w_k]/k^2/dk.
- * Synchronous; host output. */
+/* Energy or helicity spectrum of the vorticity coefficients w_k held by the handle (the field of
+ * vpbs_get_uhat), summed over spherical shells of width dk: out[n] for k_n = n dk,
+ * n = 0..nk-1 (bin n = trunc(|k|/dk + 1/2), weight 1/2 on the kx = 0 plane).  kind 0: energy as
+ * the reference computes it from a vorticity-state cache, sum of |w_k|^2/k^2/dk; kind 2: energy
+ * as from a velocity-state cache (the state after a velocity evaluation), sum of |v_k|^2/dk with
+ * v_k = i k x w_k / k^2; kind 1: helicity, sum of 2 V Re[(i k x w_k)^* . w_k]/k^2/dk (the same
+ * from either state).  Synchronous; host output. */
 int vpbs_spectrum(vpbs_handle* h, int32_t kind, double dk, double* out, int64_t nk);
+
+/* get_longrange_field_fourier for a given cache state: the held coefficients as quantity
+ * 1 = vorticity (as vpbs_get_uhat), 2 = streamfunction w_k / k^2 (after
+ * compute_streamfunction_fourier!, longrange.jl:102-125), 3 = velocity i k x w_k / k^2 (after
+ * compute_velocity_fourier!, longrange.jl:128-156); 0 at k = 0 for 2 and 3.  Layout and size as
+ * vpbs_get_uhat.  Synchronous. */
+int vpbs_get_field_fourier(vpbs_handle* h, int32_t quantity, double* out, int64_t n_doubles);
+
+/* to_coarse_grained_vorticity! (src/BiotSavart/longrange/longrange.jl:160-186, 273-293): multiply
+ * the held coefficients in place by exp(-k^2 * factor), factor = (l^2 - l_old^2) / 2.  With
+ * `project` (the reference's cache holds the velocity, whose curl i k x v_k is filtered) the
+ * solenoidal part w_k - k (k . w_k) / k^2 is filtered instead (0 at k = 0).  Synchronous. */
+int vpbs_coarse_grain(vpbs_handle* h, double factor, int32_t project);
+
+/* interpolate_to_physical! with the default callback (longrange.jl:360-378) followed by
+ * copy_long_range_output!: the type-2 NUFFT at the current nodes, with no Ewald filter, of
+ * quantity 1 = the held (possibly coarse-grained) vorticity, 2 = the streamfunction w_k / k^2,
+ * 3 = the velocity i k x w_k / k^2.  out_xyz: host AoS [Np][3].  Synchronous. */
+int vpbs_interpolate_field(vpbs_handle* h, int32_t quantity, double* out_xyz);
 
 /* ---- Time stepping and ensembles (the batching form) ---- */
 

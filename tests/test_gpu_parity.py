@@ -94,17 +94,40 @@ def test_parameter_variants(vp, oracle, built_lib, variant):
 
 
 def test_vorticity_fourier_coefficients(vp, oracle, built_lib):
+    """The vorticity coefficients (what callback_vorticity sees, BiotSavart.jl:436-438) and the
+    velocity coefficients the cache holds after the evaluation (compute_velocity_fourier!,
+    longrange.jl:128-156) against the oracle's vorticity and its Biot-Savart transform."""
+    from oracle import spectra_ref
     fs, p = vp.configs.tangle20k()
     fs = fs[:20]
-    _, _, cache = gpu_fields(vp, p, fs)
-    lr = vp.get_longrange_field_fourier(cache)
-    assert lr["state"].quantity == "vorticity"
+    seen = {}
+
+    def grab(c):
+        seen["lr"] = vp.get_longrange_field_fourier(c)
+
+    cache = vp.init_cache(p)
+    vs = [np.zeros_like(f) for f in fs]
+    vp.compute_on_nodes_({"velocity": vs}, cache, fs, callback_vorticity=grab)
+    lr = seen["lr"]
+    assert lr["state"].quantity == "vorticity" and lr["state"].smoothing_scale == 0
     o = oracle.point_data(p, fs)
     uo = oracle.vorticity_fourier(p, o["points"], o["charges"])  # [3, Ns2, Ns1, nkx]
     ug = np.stack([c.transpose(2, 1, 0) for c in lr["field"]])
     assert np.linalg.norm(ug - uo) / np.linalg.norm(uo) < TOL
     kx, ky, kz = lr["wavenumbers"]
     assert kx[-1] > 0 and len(ky) == p.splitting.Ns[1]
+    after = vp.get_longrange_field_fourier(cache)
+    assert after["state"].quantity == "velocity"
+    vo = spectra_ref.velocity_from_vorticity(tuple(uo[c].transpose(2, 1, 0) for c in range(3)), lr["wavenumbers"])
+    vg = np.stack(after["field"])
+    assert np.linalg.norm(vg - np.stack(vo)) / np.linalg.norm(np.stack(vo)) < TOL
+    vp.compute_on_nodes_({"streamfunction": [np.zeros_like(f) for f in fs]}, cache, fs)
+    psi = vp.get_longrange_field_fourier(cache)
+    assert psi["state"].quantity == "streamfunction"
+    po = spectra_ref.streamfunction_from_vorticity(tuple(uo[c].transpose(2, 1, 0) for c in range(3)),
+                                                    lr["wavenumbers"])
+    assert np.linalg.norm(np.stack(psi["field"]) - np.stack(po)) / np.linalg.norm(np.stack(po)) < TOL
+    cache.close()
 
 
 def test_open_domain_ring_analytic(vp, oracle, built_lib):

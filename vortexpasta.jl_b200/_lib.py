@@ -15,6 +15,7 @@ VELOCITY = 1
 STREAMFUNCTION = 2
 LIA_FALSE, LIA_TRUE, LIA_ONLY = 0, 1, 2
 PRECISION = {"fp64": 0, "mixed": 1}
+QUANTITY = {"vorticity": 1, "streamfunction": 2, "velocity": 3}  # held long-range field
 SPLITTING_GAUSSIAN = 0
 SPLITTING_KAISER_BESSEL = 1
 
@@ -72,6 +73,9 @@ SIGNATURES = {
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "vpbs_features": (ct.c_int, [ct.c_void_p, c_float_p, ct.c_int32]),
     "vpbs_spectrum": (ct.c_int, [ct.c_void_p, ct.c_int32, ct.c_double, c_double_p, ct.c_int64]),
+    "vpbs_coarse_grain": (ct.c_int, [ct.c_void_p, ct.c_double, ct.c_int32]),
+    "vpbs_get_field_fourier": (ct.c_int, [ct.c_void_p, ct.c_int32, c_double_p, ct.c_int64]),
+    "vpbs_interpolate_field": (ct.c_int, [ct.c_void_p, ct.c_int32, c_double_p]),
     "vpbs_set_filament_list": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_void_p, c_int64_p]),
     "vpbs_stage_filaments": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int64, ct.POINTER(c_int64_p),
                                         ct.POINTER(c_double_p)]),

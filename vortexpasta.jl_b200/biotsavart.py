@@ -157,7 +157,11 @@ class BiotSavartCache:
                                     0.0 if integration_cutoff is None else float(integration_cutoff))
         _lib.check(rc, self._h, "compute_on_nodes!")
         if longrange and lia_mode != _lib.LIA_ONLY and self.params.is_periodic:
-            self.state = LongRangeCacheState("vorticity", 0.0)
+            # the field the reference's cache holds afterwards (BiotSavart.jl:540-580): the velocity
+            # when it was requested, else the streamfunction; the device keeps the vorticity
+            # coefficients and converts on request
+            q = "velocity" if fields_mask & _lib.VELOCITY else "streamfunction"
+            self.state = LongRangeCacheState(q, 0.0)
 
     def get(self, field_mask: int, out: np.ndarray | None = None) -> np.ndarray:
         if out is None:
@@ -268,7 +272,14 @@ def compute_on_nodes_(fields: dict, cache: BiotSavartCache, fs, *, LIA=True, sho
     cache.set_filaments(fs)
     cache.compute(mask, _lia_mode(LIA), shortrange, longrange, integration_cutoff)
     if callback_vorticity is not None and longrange and LIA != "only" and cache.params.is_periodic:
+        # the reference fires the callback while the cache holds the unsmoothed vorticity
+        # (BiotSavart.jl:436-438); here the evaluation is already complete, so the state is set to
+        # the vorticity for the callback and put back afterwards unless the callback changed it
+        after = cache.state
+        cache.state = LongRangeCacheState("vorticity", 0.0)
         callback_vorticity(cache)
+        if cache.state.quantity == "vorticity" and cache.state.smoothing_scale == 0.0:
+            cache.state = after
     for name, bit in (("velocity", _lib.VELOCITY), ("streamfunction", _lib.STREAMFUNCTION)):
         if name in names:
             cache.get_list(bit, fields[name])
@@ -287,18 +298,59 @@ def velocity_on_nodes(cache: BiotSavartCache, fs, **kws):
     return velocity_on_nodes_(vs, cache, fs, **kws)
 
 
+def _wavenumbers(sp):
+    Ns = sp.Ns
+    return (np.fft.rfftfreq(Ns[0], 1 / Ns[0]) * 2 * np.pi / sp.Ls[0],
+            np.fft.fftfreq(Ns[1], 1 / Ns[1]) * 2 * np.pi / sp.Ls[1],
+            np.fft.fftfreq(Ns[2], 1 / Ns[2]) * 2 * np.pi / sp.Ls[2])
+
+
 def get_longrange_field_fourier(cache: BiotSavartCache):
     """get_longrange_field_fourier (src/BiotSavart/cache.jl:72-83): returns
     ``{"field": (ux, uy, uz), "wavenumbers": (kx, ky, kz), "state": LongRangeCacheState}``
-    with each component a complex array of shape (Ns0/2+1, Ns1, Ns2) (x first, as in Julia)."""
+    with each component a complex array of shape (Ns0/2+1, Ns1, Ns2) (x first, as in Julia).
+    The field is the cache state's quantity: the velocity after a velocity evaluation, the
+    streamfunction after a streamfunction-only one, the vorticity inside ``callback_vorticity``
+    and after ``to_coarse_grained_vorticity_``."""
+    q = cache.state.quantity
+    if q not in _lib.QUANTITY:
+        raise RuntimeError(f"no long-range field in the cache ({cache.state})")
     sp = cache.params.splitting
     Ns = sp.Ns
     nkx = Ns[0] // 2 + 1
     buf = np.empty(2 * 3 * nkx * Ns[1] * Ns[2])
-    _lib.check(cache._lib.vpbs_get_uhat(cache.handle, _lib.dptr(buf), buf.size), cache.handle, "get_uhat")
+    _lib.check(cache._lib.vpbs_get_field_fourier(cache.handle, _lib.QUANTITY[q], _lib.dptr(buf), buf.size),
+               cache.handle, "get_longrange_field_fourier")
     u = buf.view(np.complex128).reshape(3, Ns[2], Ns[1], nkx)
     field = tuple(np.ascontiguousarray(u[c].transpose(2, 1, 0)) for c in range(3))
-    ks = (np.fft.rfftfreq(Ns[0], 1 / Ns[0]) * 2 * np.pi / sp.Ls[0],
-          np.fft.fftfreq(Ns[1], 1 / Ns[1]) * 2 * np.pi / sp.Ls[1],
-          np.fft.fftfreq(Ns[2], 1 / Ns[2]) * 2 * np.pi / sp.Ls[2])
-    return {"field": field, "wavenumbers": ks, "state": LongRangeCacheState(cache.state.quantity, 0.0)}
+    return {"field": field, "wavenumbers": _wavenumbers(sp),
+            "state": LongRangeCacheState(q, cache.state.smoothing_scale)}
+
+
+def to_coarse_grained_vorticity_(cache: BiotSavartCache, ell: float):
+    """to_coarse_grained_vorticity! (src/BiotSavart/longrange/longrange.jl:273-293): Gaussian
+    filter exp(-k^2 (ell^2 - ell_old^2) / 2) of the vorticity -- the curl of the held velocity,
+    or the held vorticity -- on the device; the state becomes (vorticity, ell).  Returns
+    ``get_longrange_field_fourier(cache)``."""
+    q = cache.state.quantity
+    if q not in ("velocity", "vorticity"):
+        raise RuntimeError(f"expected either the velocity or vorticity to be in the cache (got state.quantity = {q})")
+    ell_old = cache.state.smoothing_scale
+    factor = (float(ell) ** 2 - ell_old ** 2) / 2
+    _lib.check(cache._lib.vpbs_coarse_grain(cache.handle, factor, int(q == "velocity")), cache.handle,
+               "to_coarse_grained_vorticity!")
+    cache.state = LongRangeCacheState("vorticity", float(ell))
+    return get_longrange_field_fourier(cache)
+
+
+def interpolate_to_physical(cache: BiotSavartCache) -> np.ndarray:
+    """interpolate_to_physical! with the default callback + copy_long_range_output!
+    (longrange.jl:360-378): the held field of the cache state (no Ewald filter) at the nodes of
+    the last evaluation, as an (N_p, 3) array in filament order."""
+    q = cache.state.quantity
+    if q not in _lib.QUANTITY:
+        raise RuntimeError(f"no long-range field in the cache ({cache.state})")
+    out = np.empty((cache.Np, 3))
+    _lib.check(cache._lib.vpbs_interpolate_field(cache.handle, _lib.QUANTITY[q], _lib.dptr(out)), cache.handle,
+               "interpolate_to_physical!")
+    return out

@@ -935,12 +935,130 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
     return 0;
 }
 
+// interpolate_to_physical! with the default callback (longrange.jl:360-378): the field the
+// reference's cache holds -- quantity 1: the (possibly coarse-grained) vorticity w_k as stored,
+// 2: the streamfunction w_k / k^2, 3: the velocity i k x w_k / k^2 (both 0 at k = 0) -- times the
+// type-2 deconvolution, written into the padded complex grid (no Ewald filter).
+template <typename C>
+__global__ void __launch_bounds__(256) field_grid_kernel(LRSizes S, double k0x, double k0y, double k0z, int quantity,
+                                                        const double* __restrict__ dec0, const double* __restrict__ dec1,
+                                                        const double* __restrict__ dec2,
+                                                        const double2* __restrict__ uhat, C* __restrict__ gc) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= S.ncgrid) return;
+    const int ix = (int)(idx % S.nxc);
+    const int64_t rest = idx / S.nxc;
+    const int iy = (int)(rest % S.n[1]);
+    const int iz = (int)(rest / S.n[1]);
+    const int ky = iy < (S.n[1] + 1) / 2 ? iy : iy - S.n[1];
+    const int kz = iz < (S.n[2] + 1) / 2 ? iz : iz - S.n[2];
+    const int lo1 = -(S.Ns[1] / 2), hi1 = (S.Ns[1] - 1) / 2;
+    const int lo2 = -(S.Ns[2] / 2), hi2 = (S.Ns[2] - 1) / 2;
+    const int64_t cstride = S.ncgrid;
+    double2 r[3] = {{0, 0}, {0, 0}, {0, 0}};
+    if (ix < S.nkx && ky >= lo1 && ky <= hi1 && kz >= lo2 && kz <= hi2) {
+        const int ry = ky < 0 ? ky + S.Ns[1] : ky;
+        const int rz = kz < 0 ? kz + S.Ns[2] : kz;
+        const int64_t u = ((int64_t)rz * S.Ns[1] + ry) * S.nkx + ix;
+        const double2 w0 = uhat[u], w1 = uhat[S.nmodes + u], w2 = uhat[2 * S.nmodes + u];
+        const double kx = k0x * ix, kyy = k0y * ky, kzz = k0z * kz;
+        const double k2 = kx * kx + kyy * kyy + kzz * kzz;
+        const double k2inv = k2 == 0.0 ? 0.0 : 1.0 / k2;
+        const double f = dec0[ix] * dec1[ry] * dec2[rz];
+        if (quantity == 1) {
+            r[0] = w0;
+            r[1] = w1;
+            r[2] = w2;
+        } else if (quantity == 2) {
+            r[0] = make_double2(w0.x * k2inv, w0.y * k2inv);
+            r[1] = make_double2(w1.x * k2inv, w1.y * k2inv);
+            r[2] = make_double2(w2.x * k2inv, w2.y * k2inv);
+        } else {
+            // i k x w / k^2 ; (i w).x = -w.y, (i w).y = w.x
+            r[0] = make_double2(-(kyy * w2.y - kzz * w1.y) * k2inv, (kyy * w2.x - kzz * w1.x) * k2inv);
+            r[1] = make_double2(-(kzz * w0.y - kx * w2.y) * k2inv, (kzz * w0.x - kx * w2.x) * k2inv);
+            r[2] = make_double2(-(kx * w1.y - kyy * w0.y) * k2inv, (kx * w1.x - kyy * w0.x) * k2inv);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) r[c] = make_double2(r[c].x * f, r[c].y * f);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gc[c * cstride + idx] = mkc<C>(r[c].x, r[c].y);
+}
+
+template <typename T>
+int longrange_interpolate_t(vpbs_handle* h, int quantity, double* out) {
+    using C = typename std::conditional<std::is_same<T, double>::value, double2, float2>::type;
+    const LRSizes& S = h->lr;
+    const vpbs_params& P = h->P;
+    int rc;
+    const double sx[3] = {2.0 * kPi / P.L[0], 2.0 * kPi / P.L[1], 2.0 * kPi / P.L[2]};
+    T* grid = (T*)h->grid_r.p;
+    C* gc = (C*)h->grid_c.p;
+    const double* dec0 = (const double*)h->decx.p;
+    const double* dec1 = dec0 + S.nkx;
+    const double* dec2 = dec1 + S.Ns[1];
+    field_grid_kernel<C><<<grid_for(S.ncgrid, 256), 256, 0, h->stream>>>(S, sx[0], sx[1], sx[2], quantity, dec0, dec1,
+                                                                         dec2, (const double2*)h->uhat.p, gc);
+    h->launches++;
+    if ((rc = check_cuda(h, cudaGetLastError(), "field grid kernel"))) return rc;
+    if ((rc = check_fft(h, cufftSetStream(h->plan_c2r, h->stream), "set stream"))) return rc;
+    if ((rc = check_fft(h, exec_c2r(h->plan_c2r, gc, grid), "exec c2r"))) return rc;
+    if ((rc = check_cuda(h, cudaMemsetAsync(out, 0, sizeof(double) * 3 * h->Np, h->stream), "memset"))) return rc;
+    const int32_t* order = (const int32_t*)h->dst_order.p;
+    auto launch_interp = [&](auto kern) {
+        kern<<<grid_for(h->Np, 8), 256, 0, h->stream>>>(S, h->Np, order, (const double*)h->nodes.p, sx[0], sx[1], sx[2],
+                                                        grid, out);
+    };
+    switch (S.m) {
+        case 1: launch_interp(interp_warp_kernel<2, T>); break;
+        case 2: launch_interp(interp_warp_kernel<4, T>); break;
+        case 3: launch_interp(interp_warp_kernel<6, T>); break;
+        case 4: launch_interp(interp_warp_kernel<8, T>); break;
+        case 5: launch_interp(interp_warp_kernel<10, T>); break;
+        case 6: launch_interp(interp_warp_kernel<12, T>); break;
+        case 7: launch_interp(interp_warp_kernel<14, T>); break;
+        default: launch_interp(interp_warp_kernel<16, T>); break;
+    }
+    h->launches++;
+    return check_cuda(h, cudaGetLastError(), "interp kernel");
+}
+
 int longrange_compute(vpbs_handle* h, int fields) {
     return h->P.precision == VPBS_PRECISION_MIXED ? longrange_compute_t<float>(h, fields)
                                                   : longrange_compute_t<double>(h, fields);
 }
 
 }  // namespace vpbs
+
+using namespace vpbs;
+
+extern "C" int vpbs_interpolate_field(vpbs_handle* h, int32_t quantity, double* out_xyz) {
+    if (!h || !out_xyz) return VPBS_ERR_ARG;
+    if (quantity < 1 || quantity > 3)
+        return set_error(h, VPBS_ERR_ARG, "quantity must be 1 (vorticity), 2 (streamfunction) or 3 (velocity)");
+    if (!h->have_uhat || !h->have_points || h->Np == 0)
+        return set_error(h, VPBS_ERR_STATE, "no long-range field: run a long-range computation first");
+    int rc = check_cuda(h, cudaSetDevice(h->device), "cudaSetDevice");
+    if (rc) return rc;
+    const int64_t Np = h->Np;
+    double* d = nullptr;
+    if ((rc = check_cuda(h, cudaMalloc(&d, sizeof(double) * 3 * Np), "cudaMalloc"))) return rc;
+    rc = h->P.precision == VPBS_PRECISION_MIXED ? longrange_interpolate_t<float>(h, quantity, d)
+                                                : longrange_interpolate_t<double>(h, quantity, d);
+    std::vector<double> soa;
+    if (!rc) {
+        soa.resize((size_t)3 * Np);
+        rc = check_cuda(h, cudaMemcpyAsync(soa.data(), d, sizeof(double) * 3 * Np, cudaMemcpyDeviceToHost, h->stream),
+                        "D2H");
+    }
+    if (!rc) rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sync");
+    cudaFree(d);
+    if (rc) return rc;
+    for (int64_t i = 0; i < Np; ++i)
+        for (int c = 0; c < 3; ++c) out_xyz[3 * i + c] = soa[(size_t)c * Np + i];
+    return 0;
+}
 
 extern "C" int32_t vpbs_fft_size(int32_t Ns, double sigma) {
     int n = (int)std::ceil(sigma * Ns - 1e-9);

@@ -25,18 +25,22 @@ def _spectrum(kind: int, out: np.ndarray, ks: np.ndarray, cache: BiotSavartCache
         raise ValueError("incompatible dimensions of vectors")
     if ks[0] != 0:
         raise ValueError("output wavenumbers should include k = 0")
-    if cache.state.quantity != "vorticity" or cache.state.smoothing_scale != 0:
+    q = cache.state.quantity
+    if q not in ("velocity", "vorticity") or cache.state.smoothing_scale != 0:
         raise RuntimeError(f"the current state of the long-range cache ({cache.state}) is currently not supported")
+    if kind == 0 and q == "velocity":
+        kind = 2  # |v_k|^2 instead of |w_k|^2 / k^2 (spectra.jl:95-98)
     dk = float(ks[1] - ks[0]) if len(ks) > 1 else 2 * np.pi / cache.params.splitting.Ls[0]
     buf = np.zeros(len(ks))
     _lib.check(cache._lib.vpbs_spectrum(cache.handle, kind, dk, _lib.dptr(buf), len(buf)), cache.handle,
-               "energy_spectrum!" if kind == 0 else "helicity_spectrum!")
+               "helicity_spectrum!" if kind == 1 else "energy_spectrum!")
     out[...] = buf
     return ks, out
 
 
 def energy_spectrum_(Ek: np.ndarray, ks: np.ndarray, cache: BiotSavartCache):
-    """energy_spectrum! (spectra.jl:89-108) from the vorticity coefficients in the cache."""
+    """energy_spectrum! (spectra.jl:89-108) from the velocity or (unsmoothed) vorticity the
+    cache holds."""
     return _spectrum(0, Ek, ks, cache)
 
 
@@ -47,7 +51,8 @@ def energy_spectrum(cache: BiotSavartCache):
 
 
 def helicity_spectrum_(Hk: np.ndarray, ks: np.ndarray, cache: BiotSavartCache):
-    """helicity_spectrum! (spectra_helicity.jl:48-73) from the vorticity coefficients."""
+    """helicity_spectrum! (spectra_helicity.jl:48-73) from the velocity or (unsmoothed)
+    vorticity the cache holds (the same value from either)."""
     return _spectrum(1, Hk, ks, cache)
 
 
