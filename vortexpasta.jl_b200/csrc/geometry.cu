@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(128) point_data_kernel(
     const double* __restrict__ coef, const double* __restrict__ dcoef1, const double* __restrict__ dcoef2,
     double* __restrict__ nodes, int32_t* __restrict__ idx_prev, double* __restrict__ d1, double* __restrict__ d2,
     double* __restrict__ dm, double* __restrict__ dp, double* __restrict__ points, double* __restrict__ charges,
-    double* __restrict__ li_vel, double* __restrict__ li_psi, int want_li) {
+    double* __restrict__ li_vel, double* __restrict__ li_psi, int want_li, int fuse_quad) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= Np) return;
     const int fidx = fil_of_node[k];
@@ -338,11 +338,29 @@ __global__ void __launch_bounds__(128) point_data_kernel(
     }
     const double g = K.lia_fraction;
     const bool has_g = g > 0;
-    dm[k] = seg_len(f, c1, i - 1, K.nquad, K.qz, K.qw, has_g ? 1.0 - g : 0.0, 1.0);
-    dp[k] = seg_len(f, c1, i, K.nquad, K.qz, K.qw, 0.0, has_g ? g : 1.0);
-    (void)Nq;
-    (void)points;
-    (void)charges;
+    if (fuse_quad) {
+        // full segments (no lia_segment_fraction): the quadrature points and charges of segment i
+        // (as quad_points_kernel computes them) and its length from the same s' values, in the
+        // operation order of seg_len; delta^- is the previous node's delta^+ (dm_from_prev_kernel)
+        const double dt = knot_at(f, i + 1) - knot_at(f, i);
+        double acc = 0.0;
+        for (int q = 0; q < K.nquad; ++q) {
+            double s[3], sp[3];
+            eval_seg<0>(f, c, i, K.qz[q], s);
+            eval_seg<1>(f, c1, i, K.qz[q], sp);
+            const int64_t mq = k * K.nquad + q;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                points[d * Nq + mq] = fold(s[d], K.L[d], K.open_domain);
+                charges[d * Nq + mq] = K.qw[q] * dt * sp[d];
+            }
+            acc += K.qw[q] * sqrt(sp[0] * sp[0] + sp[1] * sp[1] + sp[2] * sp[2]);
+        }
+        dp[k] = dt * 1.0 * acc;
+    } else {
+        dm[k] = seg_len(f, c1, i - 1, K.nquad, K.qz, K.qw, has_g ? 1.0 - g : 0.0, 1.0);
+        dp[k] = seg_len(f, c1, i, K.nquad, K.qz, K.qw, 0.0, has_g ? g : 1.0);
+    }
     if (want_li) {
         // nonlia_integration_limits: ((0, 1-g), (g, 1))  (local_integrals.jl:103-104)
         double v[3] = {0, 0, 0}, ps[3] = {0, 0, 0};
@@ -380,6 +398,13 @@ __global__ void __launch_bounds__(128) point_data_kernel(
 
 // One thread per quadrature point: points = fold(s(zeta_q)), charges = w_q dt s'(zeta_q) on the
 // segment to the right of node i (pointdata_impl.jl:93-103).
+// delta^-_k = delta^+ of the previous node (the length of the same segment).
+__global__ void dm_from_prev_kernel(int64_t Np, const int32_t* __restrict__ idx_prev, const double* __restrict__ dp,
+                                    double* __restrict__ dm) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < Np) dm[k] = dp[idx_prev[k]];
+}
+
 __global__ void __launch_bounds__(128) quad_points_kernel(
     KParams K, int64_t Np, const int64_t* __restrict__ offsets, const int32_t* __restrict__ fil_of_node,
     const double* __restrict__ knots, const double* __restrict__ periods, const double* __restrict__ coef,
@@ -447,14 +472,21 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
         (double*)h->dcoef1.p, (double*)h->dcoef2.p, (double*)h->spline_scratch.p, status, smem_n, keep_knots ? 1 : 0);
     h->launches++;
     const bool want_li = h->K.lia_fraction > 0;
+    // without lia_segment_fraction the point-data kernel also writes the quadrature points
+    // and charges (one pass of spline evaluations per segment instead of two)
+    const bool fuse = !want_li;
     point_data_kernel<<<grid_for(Np, 128), 128, 0, h->stream>>>(
         h->K, Np, d_offsets, (const int32_t*)h->fil_of_node.p, d_nodes, knots, periods, (const double*)h->coefs.p,
         (const double*)h->dcoef1.p, (const double*)h->dcoef2.p, (double*)h->nodes.p, (int32_t*)h->idx_prev.p,
         (double*)h->d1.p, (double*)h->d2.p, (double*)h->dm.p, (double*)h->dp.p, (double*)h->points.p,
-        (double*)h->charges.p, (double*)h->li_vel.p, (double*)h->li_psi.p, want_li ? 1 : 0);
-    quad_points_kernel<<<grid_for(Np * h->K.nquad, 128), 128, 0, h->stream>>>(
-        h->K, Np, d_offsets, (const int32_t*)h->fil_of_node.p, knots, periods, (const double*)h->coefs.p,
-        (const double*)h->dcoef1.p, (double*)h->points.p, (double*)h->charges.p);
+        (double*)h->charges.p, (double*)h->li_vel.p, (double*)h->li_psi.p, want_li ? 1 : 0, fuse ? 1 : 0);
+    if (fuse)
+        dm_from_prev_kernel<<<grid_for(Np, 256), 256, 0, h->stream>>>(Np, (const int32_t*)h->idx_prev.p,
+                                                                       (const double*)h->dp.p, (double*)h->dm.p);
+    else
+        quad_points_kernel<<<grid_for(Np * h->K.nquad, 128), 128, 0, h->stream>>>(
+            h->K, Np, d_offsets, (const int32_t*)h->fil_of_node.p, knots, periods, (const double*)h->coefs.p,
+            (const double*)h->dcoef1.p, (double*)h->points.p, (double*)h->charges.p);
     h->launches += 2;
     return check_cuda(h, cudaGetLastError(), "geometry kernels");
 }
@@ -568,7 +600,8 @@ extern "C" int vpbs_point_data_noalloc(const vpbs_params* params, int64_t nfil, 
                                                           dcoef1, dcoef2, scratch, status, 0, 0);
     point_data_kernel<<<grid_for(Np, 128), 128, 0, s>>>(K, Np, d_offsets, fil_of_node, nodes_xyz, knots, periods, coefs,
                                                         dcoef1, dcoef2, nodes, node_idx_prev, deriv1, deriv2,
-                                                        delta_minus, delta_plus, points, charges, nullptr, nullptr, 0);
+                                                        delta_minus, delta_plus, points, charges, nullptr, nullptr, 0,
+                                                        0);
     quad_points_kernel<<<grid_for(Np * K.nquad, 128), 128, 0, s>>>(K, Np, d_offsets, fil_of_node, knots, periods, coefs,
                                                                    dcoef1, points, charges);
     e = cudaGetLastError();

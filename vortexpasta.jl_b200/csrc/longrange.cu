@@ -360,10 +360,11 @@ __global__ void __launch_bounds__(kBrickThreads) spread_brick_kernel(
 // in disjoint banks (RX = 24 for P = 8: row offsets 0, 24, 16, 8; RX = 20 for P = 4).
 // Measured on the B200: FP32 shared atomicAdd sustains 2.0 T updates/s conflict-free against
 // 4.2 T for plain read-modify-writes, and the per-point work (footprint tests, kernel rows) is
-// done once per point and batch instead of by every lane of a warp.  Two variants measured
-// slower on the 1M-node tangle (m = 4, spread 5.9 ms here): float4 cells (one 16-byte load and
-// store per update, 8 instead of 6 shared wavefronts: 6.2 ms) and the plane held in registers
-// (lane per column, 8 rows of 3 components: more instructions per point, 8.3 ms).
+// done once per point and batch instead of by every lane of a warp.  Variants measured slower
+// on the 1M-node tangle (m = 4, spread 5.9 ms here): float4 cells (one 16-byte load and store
+// per update, 8 instead of 6 shared wavefronts: 6.2 ms), the plane held in registers (lane per
+// column, 8 rows of 3 components: more instructions per point, 8.3 ms) and a warp-uniform skip
+// of patch iterations whose rows miss the brick (6.3 ms).
 constexpr int kPlaneB = 16;
 constexpr int kPlaneThreads = 512;
 constexpr int kPlaneBatch = 128;
@@ -503,9 +504,6 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) spread_plane_kernel(
                 const int xs = sl.xs, ys = sl.ys;
 #pragma unroll
                 for (int it = 0; it < kIter; ++it) {
-                    // patch rows [ys + 32 it / P, ys + 32 (it + 1) / P): skip when all miss the brick
-                    const int r0 = ys + 32 * it / P;
-                    if (r0 >= kPlaneB || r0 + 32 / P <= 0) continue;  // warp-uniform
                     const int cx = xs + cxo[it], cy = ys + cyo[it];
                     if (live0 && (unsigned)cx < (unsigned)kPlaneB && (unsigned)cy < (unsigned)kPlaneB) {
                         const float g = sl.px[cxo[it]] * sl.py[cyo[it]];
