@@ -158,3 +158,25 @@ def test_kaiser_bessel_variant_meets_tolerance_when_chosen():
     vref = learned.reference_velocity(fs, L)
     _, v = tuning.measure(fs, ch, L, "mixed")
     assert info["fallback"] or tuning.rel_errors(v, vref)[0] <= 1e-5
+
+
+def test_kaiser_bessel_variants_parameters():
+    """The Kaiser-Bessel candidates keep the predicted cut-off, take beta from the reference's
+    rule at rtol / 4 (kaiser_bessel.jl:104-109) and resolve k_max = beta / r_cut with FFT sizes
+    that are multiples of 16; the predicted NUFFT comes first, duplicates are dropped."""
+    ch = tuning.EwaldChoice(alpha=23.07, rcut=L / 45, Ns=320, sigma=1.25, m=4)
+    kbs = learned.kaiser_bessel_variants(ch, L, 1e-5)
+    beta = -math.log(1e-5 / learned.KB_MARGIN / 10 ** -0.2)
+    assert [(k.sigma, k.m) for k in kbs] == [(1.25, 4)] + list(learned.KB_NUFFT)
+    for k in kbs:
+        assert k.beta == pytest.approx(beta) and k.rcut == ch.rcut
+        assert k.fft_size() % tuning.FFT_MULTIPLE == 0
+        kmax = 2 * math.pi * ((k.Ns - 1) // 2) / L
+        assert kmax >= beta / k.rcut
+        sp = k.splitting(L)
+        assert sp.Ns == (k.Ns,) * 3 and sp.rtol == pytest.approx(10 ** -0.2 * math.exp(-beta))
+        p = k.params(L)
+        assert p.splitting is not None and p.precision == "mixed" and p.backend_long.m == k.m
+        assert k.as_dict()["splitting"] == "kaiser_bessel"
+    again = learned.kaiser_bessel_variants(tuning.EwaldChoice(alpha=20.0, rcut=L / 40, Ns=300, sigma=1.5, m=3), L, 1e-5)
+    assert len(again) == 2  # (1.5, 3) predicted and in KB_NUFFT: one candidate
