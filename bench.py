@@ -370,12 +370,19 @@ def ensemble_systems(vp, nsys=64, seed=64):
     return out
 
 
-def measure_ensemble(vp, args, local_rank):
-    """RK4 steps of the whole ensemble replayed as one CUDA graph per step, against the same
-    steps issued system by system without a graph."""
+def measure_ensemble(vp, args, local_rank, rank=0, world=1):
+    """RK4 steps of the ensemble replayed as one CUDA graph per step, against the same steps
+    issued system by system without a graph.  With several ranks the systems are sharded by
+    estimated cost (timestepping.shard_systems; no data exchange), each rank steps its shard,
+    and the job's time is the max over ranks."""
     import torch
-    from vortexpasta_b200 import timestepping
-    systems = ensemble_systems(vp)
+    from vortexpasta_b200 import timestepping, tuning
+    all_systems = ensemble_systems(vp)
+    costs = [timestepping.system_cost(sum(len(f) for f in fs), tuning.fft_size(p.splitting.Ns[0], p.backend_long.sigma))
+             for fs, p, _ in all_systems]
+    mine = timestepping.shard_systems(costs, world)[rank]
+    systems = [all_systems[i] for i in mine]
+    nodes_all = sum(sum(len(f) for f in fs) for fs, _, _ in all_systems)
     nodes = sum(sum(len(f) for f in fs) for fs, _, _ in systems)
     t0 = time.perf_counter()
     ens = timestepping.Ensemble([(fs, p.with_(device=local_rank), dt) for fs, p, dt in systems], device=local_rank,
@@ -402,11 +409,13 @@ def measure_ensemble(vp, args, local_rank):
         finite = all(bool(torch.isfinite(x).all()) for x in ens.nodes)
     finally:
         ens.close()
-    evals = 4 * nodes * args.ensemble_steps
-    return {"systems": len(systems), "nodes_total": nodes, "rk4_steps": args.ensemble_steps,
+    ms_graph, ms_seq, nonfinite = max_over_ranks([ms_graph, ms_seq, 0.0 if finite else 1.0], local_rank, world)
+    evals = 4 * nodes_all * args.ensemble_steps
+    return {"systems": len(all_systems), "nodes_total": nodes_all, "rk4_steps": args.ensemble_steps,
+            "ranks": world, "systems_on_rank0": len(systems), "nodes_on_rank0": nodes,
             "node_velocities_per_s": evals / (ms_graph * 1e-3), "ms_per_step": ms_graph / args.ensemble_steps,
             "sequential_node_velocities_per_s": evals / (ms_seq * 1e-3), "graph_speedup": ms_seq / ms_graph,
-            "pair_blocks_autotuned": ens.tuned, "setup_s": t_setup, "finite": finite,
+            "pair_blocks_autotuned": ens.tuned, "setup_s": t_setup, "finite": nonfinite == 0.0,
             "description": "64 random tangles, N log-uniform in [2k, 200k] (200-node rings), Ns = nearest power of "
                            "two to N^(1/3)*4 in [64, 256], beta = 3.5, mixed precision, RK4 with dt = min(1e-3 L^2/Gamma, "
                            "Kelvin-wave period of the shortest segment); one CUDA graph launch per RK4 step (all "
@@ -447,6 +456,8 @@ def run_ours(args):
         tuned = measure_form(vp, pt, fs, args, dev, world, local_rank)
     head = tuned if tuned is not None else m64
     head_p = pt if tuned is not None else p
+    # every rank steps its shard of the ensemble (the timing reduction inside is a collective)
+    ensemble = measure_ensemble(vp, args, local_rank, rank, world) if args.ensemble_steps > 0 else None
 
     if rank == 0:
         peaks = device_peaks(local_rank)
@@ -506,8 +517,8 @@ def run_ours(args):
             "clocks": head["clk"].summary(),
             "pairs_in_range": fh["pairs_in_range"],
         }
-        if world == 1 and args.ensemble_steps > 0:
-            line["ensemble"] = measure_ensemble(vp, args, local_rank)
+        if ensemble is not None:
+            line["ensemble"] = ensemble
         if world == 1 and not args.no_cpu_baseline:
             cores = host_cores()
             sfs, sp, desc = cpu_sample(vp, args.workload)

@@ -1,5 +1,6 @@
 """Multi-rank logic of bench.py on CPU (gloo, world size 2): each rank gets an independent
-system and the job time is the max over ranks."""
+system, the job time is the max over ranks, and the batching-form ensemble is sharded by
+system (the same deterministic partition on every rank, no data exchanged)."""
 
 import os
 import socket
@@ -29,7 +30,12 @@ def _worker(rank, world, port, out):
         vp = load_package()
         fs, _ = bench.rank_workload(vp, "tangle20k", rank)
         t = bench.max_over_ranks([1.0 + rank, 5.0 - rank], "cpu", world)
-        out[rank] = (float(fs[0][0, 0]), len(fs), t)
+        from vortexpasta_b200 import timestepping
+        costs = [float((7 * i) % 13 + 1) for i in range(20)]
+        shard = timestepping.shard_systems(costs, world)[rank]  # computed locally, nothing exchanged
+        gathered = [None] * world
+        dist.all_gather_object(gathered, shard)  # only to check the partition in the test
+        out[rank] = (float(fs[0][0, 0]), len(fs), t, gathered)
     finally:
         dist.destroy_process_group()
 
@@ -44,3 +50,22 @@ def test_two_ranks_gloo():
     assert r0[1] == r1[1] == 100
     assert r0[0] != r1[0]  # independent tangles per rank
     assert r0[2] == r1[2] == [2.0, 5.0]  # max over ranks, identical on every rank
+    # ensemble sharding: both ranks derive the same partition, covering every system once
+    assert r0[3] == r1[3]
+    assert sorted(i for sh in r0[3] for i in sh) == list(range(20))
+
+
+def test_shard_systems_balances_cost():
+    from conftest import load_package
+    load_package()
+    from vortexpasta_b200 import timestepping
+    costs = [100.0, 90.0, 40.0, 35.0, 30.0, 5.0, 1.0]
+    shards = timestepping.shard_systems(costs, 3)
+    assert sorted(i for sh in shards for i in sh) == list(range(7))
+    loads = [sum(costs[i] for i in sh) for sh in shards]
+    assert max(loads) - min(loads) <= max(costs)  # greedy bound
+    assert shards == timestepping.shard_systems(costs, 3)  # deterministic
+    assert timestepping.shard_systems(costs, 1) == [list(range(7))]
+    assert timestepping.system_cost(1000, 16) == 1000 + 0.125 * 16 ** 3
+    with pytest.raises(ValueError):
+        timestepping.shard_systems(costs, 0)

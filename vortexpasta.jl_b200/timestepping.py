@@ -21,6 +21,30 @@ from . import _lib, curves
 from .biotsavart import BiotSavartCache, init_cache
 
 
+def system_cost(nodes: int, fft_size: int) -> float:
+    """Relative cost of one velocity evaluation of a system: its nodes (pairs, spreading,
+    interpolation and geometry scale with them at a fixed density) plus its FFT grid points
+    (the 3-D transforms and the Fourier pass) at a lower weight."""
+    return float(nodes) + 0.125 * float(fft_size) ** 3
+
+
+def shard_systems(costs, world: int) -> list[list[int]]:
+    """Independent systems over `world` ranks, greedy by cost (largest first onto the least
+    loaded rank; ties to the lower rank): every index appears in exactly one shard, each shard
+    in increasing index order.  Deterministic, so every rank computes the same partition without
+    exchanging anything."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    loads = [0.0] * world
+    shards: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (loads[k], k))
+        shards[r].append(i)
+        loads[r] += costs[i]
+    return [sorted(sh) for sh in shards]
+
+
 def rk4_step(cache: BiotSavartCache, nodes_ptr: int, dt: float) -> None:
     """One RK4 step of the filaments loaded in `cache` (vpbs_set_filaments); `nodes_ptr` is a
     device AoS [Np][3] float64 array with the same layout, advanced in place."""
