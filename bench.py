@@ -323,6 +323,10 @@ def form_summary(p, m, Np, Nq, world, args, peaks):
             ach = amount / (ms * 1e-3) / 1e9
             stages[name] = {"ms": ms, "bound": "hbm", "achieved": ach, "unit": "GB/s", "peak": peaks["hbm"],
                             "frac": ach / peaks["hbm"]}
+    if "spread" in stages:
+        # grid-value updates of the spreading, Nq (2m)^3 x 3 components (its on-chip work; the HBM
+        # figure above counts only the points read and the grid written once)
+        stages["spread"]["grid_updates_per_s"] = Nq * (2 * p.backend_long.m) ** 3 * 3 / (stages["spread"]["ms"] * 1e-3)
     dom = max(avg, key=avg.get)
     return {"value": world * Np * args.steps / (m["total_ms"] * 1e-3), "ms_per_step": m["total_ms"] / args.steps,
             "e2e_value": world * Np * args.steps / (m["e2e_ms"] * 1e-3), "stages": stages, "dominant": dom,

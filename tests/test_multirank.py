@@ -69,3 +69,27 @@ def test_shard_systems_balances_cost():
     assert timestepping.system_cost(1000, 16) == 1000 + 0.125 * 16 ** 3
     with pytest.raises(ValueError):
         timestepping.shard_systems(costs, 0)
+
+
+def test_form_summary_stage_model():
+    """bench.form_summary on synthetic stage times: throughput from the timed total, each stage
+    against its bound, and the spread's grid-update rate Nq (2m)^3 x 3 / time."""
+    import argparse
+    from conftest import load_package
+    vp = load_package()
+    import bench
+    fs, p = vp.configs.ring64()
+    Np = sum(len(f) for f in fs)
+    Nq = 3 * Np
+    stage_ms = {k: [1.0, 1.0] for k in ("geometry", "cell_lists", "spread", "fft_forward", "fourier", "fft_inverse",
+                                        "interp", "local_self", "pairs")}
+    stage_ms["pairs"] = [2.0, 2.0]
+    m = {"stage_ms": stage_ms, "pairs_in_range": 1000, "total_ms": 20.0, "e2e_ms": 40.0}
+    args = argparse.Namespace(steps=2)
+    peaks = {"hbm": 6000.0, "fp64": 30.0, "fp32": 60.0, "hbm_source": "test"}
+    out = bench.form_summary(p, m, Np, Nq, 1, args, peaks)
+    assert out["value"] == pytest.approx(Np * 2 / 0.020)
+    assert out["e2e_value"] == pytest.approx(Np * 2 / 0.040)
+    assert out["dominant"] == "pairs" and out["stages"]["pairs"]["bound"] == "fp64"
+    assert out["stages"]["spread"]["grid_updates_per_s"] == pytest.approx(Nq * 8 ** 3 * 3 / 1e-3)
+    assert all(0 < st["frac"] for st in out["stages"].values())
