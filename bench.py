@@ -182,14 +182,15 @@ def stage_model(stage, S):
     return "hbm", 0.0, "byte"
 
 
-def read_traffic(kernel_stage):
-    """DRAM bytes per launch from the committed ncu summary, if present."""
-    f = ROOT / "profiles" / "dram_traffic_tangle20k.txt"
+def read_traffic(kernel_stage, workload, form):
+    """DRAM bytes per launch of a stage's kernel from the committed ncu-derived table for this
+    workload and form (profiles/dram_traffic_<workload>_<form>.txt), if present."""
+    f = ROOT / "profiles" / f"dram_traffic_{workload}_{form}.txt"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
         parts = line.split()
-        if len(parts) >= 2 and parts[0] == kernel_stage:
+        if len(parts) >= 2 and not parts[0].startswith("#") and parts[0] == kernel_stage:
             try:
                 return float(parts[1])
             except ValueError:
@@ -469,7 +470,8 @@ def run_ours(args):
         fh = form_summary(head_p, head, Np, Nq, world, args, peaks)
         d = fh["stages"][fh["dominant"]]
         roof = {"kernel": fh["dominant"], "bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"],
-                "unit": d["unit"], "frac": d["frac"], "traffic": read_traffic(fh["dominant"]),
+                "unit": d["unit"], "frac": d["frac"],
+                "traffic": read_traffic(fh["dominant"], args.workload, "tuned" if tuned is not None else "fp64"),
                 "peak_source": {"fp64": "measured FP64 FMA throughput (vpbs_fma_throughput)",
                                 "fp32": "measured FP32 FMA throughput (vpbs_fma_throughput)"}.get(d["bound"],
                                                                                                    peaks["hbm_source"])}
