@@ -228,3 +228,16 @@ def test_gpu_vorticity_coefficients_independent_of_splitting(vp, built_lib):
             cache.close()
     for a, b in zip(*fields):
         assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("m,tol", [(4, 3e-6), (6, 1e-9)])
+def test_oracle_nufft_vs_exact_sum(vp, oracle, m, tol):
+    """test/trefoil.jl:135-245 with the Kaiser-Bessel filter: the long-range velocity and
+    streamfunction by NUFFT against the ExactSumBackend restatement."""
+    fs, Ls = trefoil_case(vp)
+    sp = vp.KaiserBesselSplitting(Ls=Ls, rcut=0.5, rtol=1e-8)
+    p = vp.ParamsBiotSavart(Gamma=7.4, a=1e-5, splitting=sp, backend_long=vp.NonuniformFFTsBackend(1.5, m))
+    vn, pn, _ = oracle.compute_on_nodes(p, fs, streamfunction=True, shortrange=False)
+    ve, pe, _ = oracle.compute_on_nodes(p, fs, streamfunction=True, shortrange=False, exact=True)
+    assert rel(vn, ve) < tol
+    assert rel(pn, pe) < tol
