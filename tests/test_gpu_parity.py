@@ -1,6 +1,6 @@
 """Parity of the CUDA library (through its C ABI) with the CPU oracle.
 
-Bar (north star): the plain FP64 GPU form matches the FP64 oracle to <= 1e-10 relative L2
+Bar: the plain FP64 GPU form matches the FP64 oracle to <= 1e-10 relative L2
 per node-velocity (and streamfunction) field.  Pair counts are integers and must match
 exactly.
 """
