@@ -6,6 +6,7 @@ import ctypes as ct
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
@@ -32,7 +33,10 @@ def test_params_struct_layout(vp):
     # offsets of the C struct computed by the C compiler rules for the declared members
     P = _lib.VpbsParams
     assert P.L.offset == 24 and P.Ns.offset == 64 and P.sigma.offset == 80
-    assert ct.sizeof(P) % 8 == 0
+    # the Kaiser-Bessel fields appended after `device`: int32 then two doubles (8-byte aligned)
+    assert P.splitting.offset == P.device.offset + 4
+    assert P.kb_beta.offset % 8 == 0 and P.kb_rtol.offset == P.kb_beta.offset + 8
+    assert ct.sizeof(P) == P.kb_rtol.offset + 8
 
 
 def _params(vp, **kw):
@@ -78,6 +82,14 @@ def test_null_arguments(vp):
     assert lib.vpbs_destroy(None) == 0
     assert lib.vpbs_compute(None, 1, 1, 1, 1, 0.0) == -1
     assert lib.vpbs_launch_count(None) == 0
+    # long-range diagnostics entry points check their arguments before any device work
+    buf = np.zeros(6)
+    assert lib.vpbs_spectrum(None, 0, 1.0, _lib.dptr(buf), 6) == -1
+    assert lib.vpbs_coarse_grain(None, 0.1, 1) == -1
+    assert lib.vpbs_get_field_fourier(None, 1, _lib.dptr(buf), 6) == -1
+    assert lib.vpbs_interpolate_field(None, 1, _lib.dptr(buf)) == -1
+    assert lib.vpbs_kb_weights(14.0, 0.5, 1e-6, None, 1, None, None, None, None) == -1
+    assert lib.vpbs_kb_weights(-1.0, 0.5, 1e-6, _lib.dptr(buf), 1, None, None, None, None) == -1
 
 
 def test_python_params_mirror_reference_errors(vp):
