@@ -35,6 +35,7 @@ METRIC = "Biot–Savart node-velocities/s at 1e-5 rel err: tuned FP32 vs plain F
 UNIT = "node-velocities/s"
 F_PAIR_VEL = 40.0  # flops per in-range pair (velocity), convention of the roofline model
 L2_FLUSH_BYTES = 256 << 20
+L2_BYTES = 126e6  # B200 L2 cache
 
 
 def load_package():
@@ -170,11 +171,16 @@ def stage_model(stage, S):
     if stage == "interp":
         return "hbm", 3 * n3 * g + Np * 3 * 8 + Np * 3 * 8, "byte"
     if stage == "fourier":
-        return "hbm", 2 * 3 * nc3 * 2 * g, "byte"
+        # reads the retained modes of the forward transform, writes the whole (zero-padded) grid
+        # for the inverse transform and the FP64 vorticity coefficients
+        return "hbm", 3 * S["nm"] * 2 * g + 3 * nc3 * 2 * g + 3 * S["nm"] * 16, "byte"
     if stage in ("fft_forward", "fft_inverse"):
         return "hbm", 2 * 2 * 3 * n3 * g, "byte"
     if stage == "local_self":
-        return "hbm", Np * (11 * 8 + 6 * S["nq"] * 6 * 8) + Np * 3 * 8, "byte"
+        # per node: position, previous index, s', s'', delta^-, delta^+, output read + write; each
+        # quadrature point (position + charge) is gathered by the two nodes of its segment but
+        # counted once
+        return "hbm", Np * (3 * 8 + 4 + 6 * 8 + 2 * 8 + 2 * 3 * 8) + Nq * 6 * 8, "byte"
     if stage == "geometry":
         return "hbm", Np * 3 * 8 + Np * (3 * 3 * 8 + 12 * 8) + Np * (11 * 8) + Nq * 6 * 8, "byte"
     if stage == "cell_lists":
@@ -306,7 +312,9 @@ def form_summary(p, m, Np, Nq, world, args, peaks):
     from vortexpasta_b200 import _lib
     n = [_lib.load().vpbs_fft_size(N, p.backend_long.sigma) for N in p.splitting.Ns]
     fp32 = p.precision == "mixed"
+    Ns = p.splitting.Ns
     S = {"Np": Np, "Nq": Nq, "n3": n[0] * n[1] * n[2], "nc3": (n[0] // 2 + 1) * n[1] * n[2],
+         "nm": (Ns[0] // 2 + 1) * Ns[1] * Ns[2],
          "pairs": m["pairs_in_range"], "nq": len(p.quadrature), "gsz": 4 if fp32 else 8,
          "pair_bound": "fp32" if fp32 else "fp64"}
     avg = {k: statistics.mean(v) for k, v in m["stage_ms"].items()}
@@ -324,6 +332,11 @@ def form_summary(p, m, Np, Nq, world, args, peaks):
             ach = amount / (ms * 1e-3) / 1e9
             stages[name] = {"ms": ms, "bound": "hbm", "achieved": ach, "unit": "GB/s", "peak": peaks["hbm"],
                             "frac": ach / peaks["hbm"]}
+            if amount < 2 * L2_BYTES:
+                # the stage's algorithmic bytes are within twice the L2 (126 MB): much of its
+                # traffic is served from L2, so a fraction of the HBM peak means nothing
+                stages[name]["frac"] = None
+                stages[name]["note"] = "working set within 2x L2; no HBM fraction"
     if "spread" in stages:
         # grid-value updates of the spreading, Nq (2m)^3 x 3 components (its on-chip work; the HBM
         # figure above counts only the points read and the grid written once)
@@ -420,7 +433,7 @@ def measure_ensemble(vp, args, local_rank, rank=0, world=1):
             "ranks": world, "systems_on_rank0": len(systems), "nodes_on_rank0": nodes,
             "node_velocities_per_s": evals / (ms_graph * 1e-3), "ms_per_step": ms_graph / args.ensemble_steps,
             "sequential_node_velocities_per_s": evals / (ms_seq * 1e-3), "graph_speedup": ms_seq / ms_graph,
-            "pair_blocks_autotuned": ens.tuned, "setup_s": t_setup, "finite": nonfinite == 0.0,
+            "pair_blocks_autotuned": {"systems_off_rule": sum(1 for t in ens.tuned if t), "edges": sorted(set(ens.tuned))}, "setup_s": t_setup, "finite": nonfinite == 0.0,
             "description": "64 random tangles, N log-uniform in [2k, 200k] (200-node rings), Ns = nearest power of "
                            "two to N^(1/3)*4 in [64, 256], beta = 3.5, mixed precision, RK4 with dt = min(1e-3 L^2/Gamma, "
                            "Kelvin-wave period of the shortest segment); one CUDA graph launch per RK4 step (all "
@@ -452,13 +465,16 @@ def run_ours(args):
     mixed = measure_form(vp, p.with_(precision="mixed"), fs, args, dev, world, local_rank) if args.mixed else None
     # tuned form: parameters from the learned predictor (checked against a plain FP64 evaluation,
     # default rule on a miss), FP32 bulk arithmetic
-    tuned = None
+    tuned = tuned64 = None
     if args.tuned:
         t0 = time.perf_counter()
         choice, info = learned.choose_parameters(fs, L, rtol=args.rtol, device=local_rank)
         t_choose = time.perf_counter() - t0
         pt = choice.params(L, "mixed", device=local_rank)
         tuned = measure_form(vp, pt, fs, args, dev, world, local_rank)
+        # FP64 at the tuned parameters: separates the gain of the parameter choice from that of
+        # the FP32 arithmetic
+        tuned64 = measure_form(vp, pt.with_(precision="fp64"), fs, args, dev, world, local_rank) if args.mixed else None
     head = tuned if tuned is not None else m64
     head_p = pt if tuned is not None else p
     # every rank steps its shard of the ensemble (the timing reduction inside is a collective)
@@ -503,6 +519,13 @@ def run_ours(args):
                               "description": ("mixed precision at the cut-off and NUFFT predicted by the learned MLP; "
                                               "Gaussian or Kaiser-Bessel split, whichever met the tolerance in less "
                                               "time in the FP64-checked trial")}
+            if tuned64 is not None:
+                ft = form_summary(pt.with_(precision="fp64"), tuned64, Np, Nq, world, args, peaks)
+                forms["fp64_tuned"] = {**{k: ft[k] for k in ("value", "ms_per_step", "e2e_value")},
+                                       "speedup_vs_fp64": ft["value"] / f64["value"],
+                                       **errors_vs(tuned64["v"], m64["v"]),
+                                       "stages_ms": {k: v["ms"] for k, v in ft["stages"].items()},
+                                       "description": "plain FP64 arithmetic at the tuned form's parameters"}
         line = {
             "metric": METRIC, "value": fh["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": fh["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -531,13 +554,48 @@ def run_ours(args):
             t_cpu, v_cpu = cpu_oracle_time(sfs, sp, cores, args.cpu_reps)
             line["cpu_baseline"] = {"value": sum(len(f) for f in sfs) / t_cpu, "unit": UNIT, "cores": cores,
                                     "kind": "port", "sample": desc}
-            if args.workload != "tangle1m":
-                line["accuracy"] = {"fp64_rel_l2_vs_oracle": float(np.linalg.norm(m64["v"] - v_cpu) /
-                                                                   np.linalg.norm(v_cpu))}
+            line["accuracy"] = sample_accuracy(vp, args, sfs, sp, v_cpu, pt if tuned is not None else None,
+                                               local_rank)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def sample_velocity(vp, p, fs):
+    """Node velocities of one evaluation of `fs` with parameters `p` (host copy)."""
+    from vortexpasta_b200 import _lib
+    c = vp.init_cache(p)
+    try:
+        c.set_filaments(fs)
+        c.compute(_lib.VELOCITY)
+        return c.get(_lib.VELOCITY)
+    finally:
+        c.close()
+
+
+def sample_accuracy(vp, args, sfs, sp, v_oracle, p_tuned, device):
+    """Relative L2 errors against the FP64 oracle on the CPU sample of the workload (for tangle1m
+    the 1/64-volume sample, with every parameter set carried over at the same absolute cut-off,
+    splitting parameter and grid spacing): the plain FP64 and mixed forms at the workload's
+    parameters, and the tuned form at its chosen parameters -- the metric's accuracy condition."""
+    def rel(v):
+        return float(np.linalg.norm(v - v_oracle) / np.linalg.norm(v_oracle))
+    sp = sp.with_(device=device)
+    out = {"sample": "the cpu_baseline sample; oracle = FP64 CPU restatement at the workload's parameters",
+           "fp64_rel_l2_vs_oracle": rel(sample_velocity(vp, sp, sfs))}
+    if args.mixed:
+        out["mixed_rel_l2_vs_oracle"] = rel(sample_velocity(vp, sp.with_(precision="mixed"), sfs))
+    if p_tuned is not None:
+        k = SAMPLE_K[args.workload]
+        pts = (vp.configs.sample_params(p_tuned, k) if k > 1 else p_tuned).with_(device=device)
+        out["tuned_rel_l2_vs_oracle"] = rel(sample_velocity(vp, pts, sfs))
+        out["tuned_fp64_rel_l2_vs_oracle"] = rel(sample_velocity(vp, pts.with_(precision="fp64"), sfs))
+        out["tuned_meets_target"] = out["tuned_rel_l2_vs_oracle"] <= args.rtol
+    return out
+
+
+SAMPLE_K = {"tangle1m": 4, "tangle20k": 1, "ring64": 1}  # CPU sample = cube of side L / k
 
 
 def cpu_sample(vp, workload):

@@ -217,8 +217,12 @@ const char* vpbs_stage_name(int32_t i);
  * NULL).  Outputs (device pointers, same layouts as vpbs_get_pointdata): nodes, s', s'' (SoA
  * 3*Np), node_idx_prev (Np, 0-based), delta_minus, delta_plus (Np), points, charges (SoA 3*Nq).
  * Limits: at most VPBS_NOALLOC_MAX_NODES nodes and VPBS_NOALLOC_MAX_FILAMENTS filaments; larger
- * inputs are rejected with VPBS_ERR_ARG.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * inputs are rejected with VPBS_ERR_ARG.  `nodes_xyz` and every output must be device (or managed)
+ * memory of params->device, else VPBS_ERR_ARG; the caller's current device is restored on return.
+ * Every call looks up the array's device address (cudaGetSymbolAddress, no allocation).  Under
+ * CUDA's lazy module loading (the default since CUDA 12.2) the driver materialises the array, and
+ * this file's kernels, at the first call on each device: make one warm-up call on every device
+ * before an external pool claims the device memory, and before any stream capture.
  * All calls share the one array: calls that overlap on the GPU (other streams, other threads)
  * race and must be serialised by the caller.  Errors: vpbs_last_error(NULL). Asynchronous. */
 #define VPBS_NOALLOC_MAX_NODES 32768
@@ -241,6 +245,13 @@ int vpbs_ewald_table_eval(double xmax, const double* x, int64_t n, double* erfc_
  * Exists to test the tables and the series; no counterpart in the reference. */
 int vpbs_kb_weights(double beta, double rcut, double rtol, const double* r, int64_t n, double* a_table,
                     double* g_table, double* a_series, double* g_series);
+
+/* Host evaluation of the device's periodic helpers (the same inline code, periodic.cuh): x folded
+ * into [0, L) (min_distance.jl:5-20; O(1) for any x, NaN for a non-finite x) and the cell index
+ * trunc(folded / L * nc) clamped to [0, nc) (CellLists.jl:194-204, 0-based), or the sentinel nc for
+ * a non-finite coordinate.  Either output may be NULL.  Exists to test them; no counterpart in the
+ * reference. */
+int vpbs_periodic_eval(double L, int32_t nc, const double* x, int64_t n, double* folded, int64_t* cell);
 
 /* Measured CUDA-core FMA throughput of `device` in TFLOP/s (fp64 = 1: double, 0: float); the
  * denominator of the pair kernel's roofline.  Measurement support; no counterpart in the

@@ -3,6 +3,7 @@ declares, rejects bad parameters before touching a GPU, and reports errors throu
 vpbs_last_error (host-side fault injection, no GPU needed)."""
 
 import ctypes as ct
+import math
 import re
 from pathlib import Path
 
@@ -139,3 +140,37 @@ def test_ewald_weight_tables_accuracy(vp):
         assert np.max(np.abs(g - eg)) < 1e-15
         small = x <= 4.0  # relative accuracy where erfc is not yet negligible (erfc(4) ~ 1.5e-8)
         assert np.max(np.abs(a - ea)[small] / ea[small]) < 1e-13
+
+
+def test_periodic_helpers_on_host(vp, built_lib):
+    """The device's folding and cell-index helpers (the same inline code, run on the CPU): the
+    reference's subtraction loops within a few periods (min_distance.jl:5-20), O(1) beyond, NaN
+    for a non-finite coordinate, and the sentinel cell nc for it (so that a blown-up point is
+    left out of every neighbourhood instead of stalling the pair search)."""
+    from vortexpasta_b200 import _lib
+    lib = _lib.load()
+    L, nc = 2 * math.pi, 16
+    x = np.array([0.0, 1.0, -1e-17, L, -L, 3.5 * L + 0.25, -3.9 * L, 1e6, -1e300, 1e300,
+                  np.inf, -np.inf, np.nan, L - 1e-16, 5 * L])
+    folded = np.zeros_like(x)
+    cell = np.zeros(len(x), dtype=np.int64)
+    assert lib.vpbs_periodic_eval(L, nc, _lib.dptr(x), len(x), _lib.dptr(folded), cell.ctypes.data_as(_lib.c_int64_p)) == 0
+    fin = np.isfinite(x)
+    assert np.all(np.isnan(folded[~fin]))
+    assert np.all(cell[~fin] == nc)
+    f = folded[fin]
+    assert np.all((f >= 0) & (f < L))
+    # folded values are congruent to x modulo L (to the rounding of one subtraction per period)
+    mod = fin & (np.abs(x) < 1e7)
+    k = np.round((x[mod] - folded[mod]) / L)
+    assert np.allclose(x[mod] - k * L, folded[mod], rtol=0, atol=1e-8)
+    assert np.all((cell[fin] >= 0) & (cell[fin] < nc))
+    np.testing.assert_array_equal(cell[fin], np.minimum((f / L * nc).astype(np.int64), nc - 1))
+    # within four periods: the reference's loops exactly
+    for xi, fi in zip(x[:7], folded[:7]):
+        y = xi
+        while y < 0:
+            y += L
+        while y >= L:
+            y -= L
+        assert fi == y

@@ -68,6 +68,7 @@ SIGNATURES = {
     "vpbs_ewald_table_eval": (ct.c_int, [ct.c_double, c_double_p, ct.c_int64, c_double_p, c_double_p]),
     "vpbs_kb_weights": (ct.c_int, [ct.c_double, ct.c_double, ct.c_double, c_double_p, ct.c_int64, c_double_p,
                                    c_double_p, c_double_p, c_double_p]),
+    "vpbs_periodic_eval": (ct.c_int, [ct.c_double, ct.c_int32, c_double_p, ct.c_int64, c_double_p, c_int64_p]),
     "vpbs_point_data_noalloc": (ct.c_int, [ct.POINTER(VpbsParams), ct.c_int64, c_int64_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p]),

@@ -56,10 +56,44 @@ def tangle1m_cpu_sample(seed: int = 42, **kw):
     x 200 nodes (15,600 nodes: the same node density) with radii scaled by 1/4, and the same
     absolute parameters -- r_cut = L/16 (= L'/4), alpha = 4 / r_cut, the same grid spacing
     (Ns = 128, FFT 192^3), m = 5 -- so every node sees the same work as in the full workload."""
-    Ls = L / 4
-    fs = curves.random_tangle(78, 200, L=Ls, rmin=Ls / 8, rmax=Ls / 4, seed=seed)
-    rcut = Ls / 4
-    p = ParamsBiotSavart(Gamma=1.0, a=1e-8, Delta=0.25,
-                         splitting=GaussianSplitting(Ls=Ls, alpha=4.0 / rcut, rcut=rcut, Ns=128),
-                         quadrature=GaussLegendre(3), backend_long=NonuniformFFTsBackend(1.5, 5), **kw)
-    return fs, p
+    return tangle1m_sample(4, seed, **kw)
+
+
+def tangle1m_sample(k: int, seed: int = 42, **kw):
+    """Volume sample of ``tangle1m``: a cube of side L/k holding round(5000/k^3) rings x 200 nodes
+    (the node density of the full tangle) with radii in [L/(8k), L/(4k)], at tangle1m's absolute
+    parameters (``sample_params``): r_cut = L/16, alpha = 4 / r_cut, FFT 768/k per side, m = 5.
+    k = 4 gives 78 rings (15,600 nodes, FFT 192^3); k = 2 gives 625 rings (125,000 nodes, FFT 384^3)."""
+    Ls = L / k
+    fs = curves.random_tangle(int(round(5000 / k ** 3)), 200, L=Ls, rmin=Ls / 8, rmax=Ls / 4, seed=seed)
+    return fs, sample_params(tangle1m_params(**kw), k)
+
+
+def tangle1m_params(**kw) -> ParamsBiotSavart:
+    return params_for(L / 16, 4.0, 512, 5, **kw)
+
+
+def sample_params(p: ParamsBiotSavart, k: int) -> ParamsBiotSavart:
+    """Parameters of `p` (a periodic cube of side L) carried over to a cube of side L/k with the
+    same absolute cut-off, the same splitting parameter (alpha, or the Kaiser-Bessel beta and
+    rtol), the same NUFFT (sigma, m) and the same grid spacing: the oversampled FFT has n/k points
+    per side when n/k is an FFT size of the library (Ns then the largest count mapping to it, as
+    the tuned grids are chosen), else the smallest FFT size above n/k."""
+    from .params import KaiserBesselSplitting
+    from . import tuning
+    sp = p.splitting
+    Lk = sp.Ls[0] / k
+    sigma = p.backend_long.sigma
+    n = tuning.fft_size(sp.Ns[0], sigma)
+    target = max(n // k, 2 * p.backend_long.m)
+    Ns = int(math.floor(target / sigma + 1e-9))
+    while Ns > 1 and tuning.fft_size(Ns, sigma) > target:
+        Ns -= 1
+    if tuning.fft_size(Ns, sigma) < target:
+        Ns += 1
+    if isinstance(sp, KaiserBesselSplitting):
+        s = KaiserBesselSplitting(Ls=Lk, beta=sp.beta, rcut=sp.rcut)
+        s.Ns, s.rtol = (Ns,) * 3, sp.rtol
+    else:
+        s = GaussianSplitting(Ls=Lk, alpha=sp.alpha, rcut=sp.rcut, Ns=Ns)
+    return p.with_(splitting=s)

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "vpbs_internal.cuh"
+#include "periodic.cuh"
 
 namespace {
 thread_local std::string g_create_error;
@@ -882,6 +883,15 @@ extern "C" int vpbs_fma_throughput(int32_t device, int32_t fp64, double* tflops)
     return 0;
 }
 
-extern "C" {
-
-}  // extern "C"
+extern "C" int vpbs_periodic_eval(double L, int32_t nc, const double* x, int64_t n, double* folded, int64_t* cell) {
+    using namespace vpbs;
+    if (!(L > 0) || nc < 1 || n < 0 || (n > 0 && !x)) return set_error(nullptr, VPBS_ERR_ARG, "vpbs_periodic_eval: bad arguments");
+    const int ncs[3] = {nc, 1, 1};
+    const double Ls[3] = {L, 1.0, 1.0};
+    for (int64_t i = 0; i < n; ++i) {
+        const double f = fold(x[i], L, 0);
+        if (folded) folded[i] = f;
+        if (cell) cell[i] = cell_index(ncs, Ls, f, 0.5, 0.5);
+    }
+    return 0;
+}

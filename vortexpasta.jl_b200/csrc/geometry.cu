@@ -8,6 +8,7 @@
 // by seven lanes in parallel, and the corners are folded back with the Woodbury identity.
 // A second kernel evaluates the splines at the nodes and quadrature points, one thread per node.
 #include "vpbs_internal.cuh"
+#include "periodic.cuh"
 
 namespace vpbs {
 namespace {
@@ -66,29 +67,6 @@ __device__ __forceinline__ void eval_seg(const FilView& f, const double* coef, l
         out[1] += coef[3 * j + 1] * N[s];
         out[2] += coef[3 * j + 2] * N[s];
     }
-}
-
-// Fold into [0, L) (min_distance.jl:5-20).  Within four periods the reference's subtraction
-// loops (at most five iterations, same rounding); beyond that, or for a non-finite coordinate,
-// one exact fmod, so the cost never depends on the value (inf and NaN come out as NaN).
-__device__ __forceinline__ double fold(double x, double L, int open) {
-    if (open) return x;
-    if (!(fabs(x) <= 4.0 * L)) {
-        x = fmod(x, L);  // exact, |x| < L; NaN for inf / NaN
-        if (x < 0.0) x += L;
-        if (x >= L) x = 0.0;  // -tiny + L rounded to L
-        return x;
-    }
-    while (x < 0.0) x += L;
-    while (x >= L) x -= L;
-    return x;
-}
-
-__device__ __forceinline__ double deper(double r, double L, double Lh, int open) {
-    if (open) return r;
-    r = (r >= Lh) ? r - L : r;
-    r = (r < -Lh) ? r + L : r;
-    return r;
 }
 
 // Solve the 4x4 Woodbury capacitance system with partial pivoting (3 right-hand sides).
@@ -504,8 +482,6 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
 // array of fixed size instead of cudaMalloc'd buffers; every GPU that loads the library holds
 // this array (about 6 MB) until the process exits.
 // ---------------------------------------------------------------------------------------------
-#include <mutex>
-
 namespace {
 
 constexpr int64_t kNoAllocMaxNodes = VPBS_NOALLOC_MAX_NODES;
@@ -518,29 +494,42 @@ constexpr int64_t kNoAllocDoubles =
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-double* g_noalloc_ptr[kMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on the current device, looked up once per device.  In
-// host code the symbol itself is only a host-side stand-in, never a device address.
+// Device address of g_noalloc_scratch on the current device.  In host code the symbol itself is
+// only a host-side stand-in, never a device address.  The address is looked up on every call (a
+// cheap host query once the module is loaded, and it allocates nothing): a cached address would
+// go stale if the caller reset the device and the module were loaded again elsewhere.
 int noalloc_scratch(double** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-        return vpbs::set_error(nullptr, VPBS_ERR_CUDA, "vpbs_point_data_noalloc: no usable CUDA device");
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return vpbs::set_error(nullptr, VPBS_ERR_CUDA,
-                                   std::string("vpbs_point_data_noalloc: cudaGetSymbolAddress failed: ") +
-                                       cudaGetErrorString(e));
-        g_noalloc_ptr[dev] = (double*)p;
-    }
-    *out = g_noalloc_ptr[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return vpbs::set_error(nullptr, VPBS_ERR_CUDA,
+                               std::string("vpbs_point_data_noalloc: cudaGetSymbolAddress failed: ") +
+                                   cudaGetErrorString(e));
+    *out = (double*)p;
     return 0;
 }
+
+// Device memory of `device` (or managed memory) that the kernels may read and write.
+bool on_device(const void* p, int device) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();  // clear the (non-sticky) error so that later calls do not report it
+        return false;
+    }
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == device;
+}
+
+// Restores the caller's current device when the entry point returns.
+struct DeviceRestore {
+    int prev = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    }
+    ~DeviceRestore() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
 
 }  // namespace
 
@@ -577,8 +566,15 @@ extern "C" int vpbs_point_data_noalloc(const vpbs_params* params, int64_t nfil, 
     for (int q = 0; q < P.nquad; ++q) { K.qz[q] = P.quad_zeta[q]; K.qw[q] = P.quad_w[q]; }
     K.nquad_near = K.nquad;
     K.lia_fraction = P.lia_segment_fraction > 0 ? P.lia_segment_fraction : 0.0;
+    DeviceRestore restore;
     if (cudaSetDevice(P.device) != cudaSuccess)
         return set_error(nullptr, VPBS_ERR_CUDA, "vpbs_point_data_noalloc: cudaSetDevice failed");
+    const void* dev_ptrs[] = {nodes_xyz, nodes, node_idx_prev, deriv1, deriv2, delta_minus, delta_plus, points, charges};
+    for (const void* p : dev_ptrs)
+        if (!on_device(p, P.device))
+            return set_error(nullptr, VPBS_ERR_ARG,
+                             "vpbs_point_data_noalloc: node and output arrays must be device memory of params->device (" +
+                                 std::to_string(P.device) + ")");
     double* base = nullptr;
     int rc = noalloc_scratch(&base);
     if (rc) return rc;

@@ -12,31 +12,13 @@
 #include <vector>
 
 #include "vpbs_internal.cuh"
+#include "periodic.cuh"
 
 namespace vpbs {
 namespace {
 
-__device__ __forceinline__ double deper(double r, double L, double Lh, int open) {
-    if (open) return r;
-    r = (r >= Lh) ? r - L : r;
-    r = (r < -Lh) ? r + L : r;
-    return r;
-}
-
-__device__ __forceinline__ int cell_coord(double x, double L, int nc) {
-    int c = (int)((x / L) * nc);
-    return c < 0 ? 0 : (c >= nc ? nc - 1 : c);
-}
-
-// Cell (slab) of a point; a point with a non-finite coordinate goes to the sentinel cell
-// `ncell`, which no neighbourhood contains (its pairs are skipped instead of piling up in
-// cell 0 and making the pair search quadratic).
 __device__ __forceinline__ int64_t cell_of(const CellGrid& cg, const KParams& K, double x, double y, double z) {
-    if (!(isfinite(x) && isfinite(y) && isfinite(z))) return cg.ncell;
-    int cx = cell_coord(x, K.L[0], cg.nc[0]);
-    int cy = cell_coord(y, K.L[1], cg.nc[1]);
-    int cz = cell_coord(z, K.L[2], cg.nc[2]);
-    return ((int64_t)cz * cg.nc[1] + cy) * cg.nc[0] + cx;
+    return cell_index(cg.nc, K.L, x, y, z);
 }
 
 // Cell of every element and its rank within the cell (atomic counter).
