@@ -633,6 +633,8 @@ def run_kernel_case(args):
     for name, p in cases:
         c = vp.init_cache(p)
         try:
+            if args.pair_block:
+                _lib.check(_lib.load().vpbs_pair_block(c.handle, args.pair_block), c.handle, "pair_block")
             c.set_filaments(fs)
             c.stage_timing(True)
             for _ in range(3):
@@ -663,6 +665,8 @@ def main():
                     help="RK4 steps of the batching-form ensemble reported under 'ensemble' (0: skip)")
     ap.add_argument("--kernel-case", choices=sorted(KERNEL_CASES), default=None,
                     help="run a small fixed workload for kernel profiling instead of the benchmark")
+    ap.add_argument("--pair-block", type=int, default=0,
+                    help="with --kernel-case: the pair kernel's cells per CTA edge (0: the built-in rule)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

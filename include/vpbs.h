@@ -122,6 +122,17 @@ int vpbs_set_stream(vpbs_handle* h, void* stream);
 int vpbs_set_filaments(vpbs_handle* h, int64_t nfil, const int64_t* offsets, const double* nodes_xyz,
                        int32_t on_device);
 
+/* End-to-end offsets of unclosed (infinite) filaments, ClosedFilament's Xoffset
+ * (src/Filaments/closed_filament.jl:118-132, 196-207): host [nfil][3], or NULL / all zero for closed
+ * filaments.  They apply to the following vpbs_set_filaments / vpbs_set_filament_list /
+ * vpbs_set_staged_filaments calls (which must pass nfil filaments) and RK4 steps, until changed.
+ * The splines then interpolate the periodic y_i = X_i - (t_i / T) offset (spline.jl:163-194,
+ * quintic.jl:9-17), and when the offsets add up to p != 0 the short range adds the streamfunction
+ * of the compensating background vorticity, -(p Gamma / V) C, to every node
+ * (background_vorticity_correction!, src/BiotSavart/BiotSavart.jl:255-286; C = 1 / (4 alpha^2),
+ * or int_0^rcut r^2 f(r) dr / 2 for the Kaiser-Bessel splitting). */
+int vpbs_set_filament_offsets(vpbs_handle* h, int64_t nfil, const double* offsets_xyz);
+
 /* Plugin-contract entry: PointData computed by the caller (the reference computes it on the
  * host in add_point_charges!).  Layout per src/BiotSavart/pointdata.jl:21-31: nodes, derivatives
  * and charges as SoA views; node_idx_prev is 1-based as in the reference; points/charges hold
@@ -246,6 +257,15 @@ int vpbs_ewald_table_eval(double xmax, const double* x, int64_t n, double* erfc_
 int vpbs_kb_weights(double beta, double rcut, double rtol, const double* r, int64_t n, double* a_table,
                     double* g_table, double* a_series, double* g_series);
 
+/* Host evaluation of the mixed form's FP32 pair-kernel weights (the cubic tables on 1/32-wide
+ * intervals, built as on the device and evaluated with the same float operations): a = erfc(alpha r)
+ * and g = erfc(alpha r) + 2/sqrt(pi) alpha r exp(-(alpha r)^2) for splitting = VPBS_SPLITTING_GAUSSIAN
+ * (splitting/gaussian.jl:273-279), a = 1 - F(r) and g = 1 - F(r) + r f(r) of the truncated Chebyshev
+ * series for VPBS_SPLITTING_KAISER_BESSEL (kaiser_bessel.jl:139-147; alpha ignored), for r in
+ * [0, rcut].  Exists to test the tables; no counterpart in the reference. */
+int vpbs_f32_weights_eval(int32_t splitting, double alpha, double rcut, double kb_beta, double kb_rtol, const double* r,
+                          int64_t n, float* a, float* g);
+
 /* Host evaluation of the device's periodic helpers (the same inline code, periodic.cuh): x folded
  * into [0, L) (min_distance.jl:5-20; O(1) for any x, NaN for a non-finite x) and the cell index
  * trunc(folded / L * nc) clamped to [0, nc) (CellLists.jl:194-204, 0-based), or the sentinel nc for
@@ -319,6 +339,11 @@ const char* vpbs_ensemble_last_error(void);
  * evaluations (`chosen`: 0 = the rule, else the edge).  Overwrites the handle's output fields.
  * Synchronous. */
 int vpbs_autotune(vpbs_handle* h, int32_t* chosen);
+
+/* Sets the pair kernel's cells per CTA edge for later evaluations (0: the built-in rule; an edge
+ * whose neighbourhood does not fit the kernel's tables falls back to the rule), as vpbs_autotune
+ * does with its choice.  Tuning support; no counterpart in the reference. */
+int vpbs_pair_block(vpbs_handle* h, int32_t cells);
 
 /* ---- Learned parameter predictor (no counterpart in the reference, which removed its alpha
  * autotuner; the fallback is the default rule of splitting/gaussian.jl:133-200). ---- */

@@ -26,7 +26,7 @@ class OParams(ct.Structure):
         ("m", ct.c_int), ("nquad", ct.c_int), ("nquad_near", ct.c_int), ("lia_segment_fraction", ct.c_double),
         ("avoid_explicit_erf", ct.c_int), ("truncate_spherical", ct.c_int), ("nsubdiv", ct.c_int),
         ("longrange_exact", ct.c_int), ("nthreads", ct.c_int), ("splitting", ct.c_int), ("kb_beta", ct.c_double),
-        ("kb_rtol", ct.c_double),
+        ("kb_rtol", ct.c_double), ("fil_offsets", ct.c_void_p),
     ]
 
 
@@ -115,12 +115,21 @@ def _pack(fs):
     return nodes, offsets
 
 
+def end_to_end_offsets(fs):
+    """[nfil, 3] end-to-end offsets (a filament's `offset` attribute, zero when absent), or None
+    when every filament is closed."""
+    offs = np.array([np.asarray(getattr(f, "offset", np.zeros(3)), dtype=np.float64) for f in fs]).reshape(len(fs), 3)
+    return np.ascontiguousarray(offs) if np.any(offs != 0) else None
+
+
 def compute_on_nodes(p, fs, *, velocity=True, streamfunction=False, LIA=True, shortrange=True, longrange=True,
                      exact=False, nthreads=0):
     """Oracle compute_on_nodes!: returns (vel [Np,3] or None, psi [Np,3] or None, stats dict)."""
     lib = load()
     o = make_params(p, exact=exact, nthreads=nthreads)
     nodes, offsets = _pack(fs)
+    foff = end_to_end_offsets(fs)
+    o.fil_offsets = foff.ctypes.data if foff is not None else None
     Np = int(offsets[-1])
     vel = np.zeros((Np, 3)) if velocity else None
     psi = np.zeros((Np, 3)) if streamfunction else None
@@ -140,6 +149,8 @@ def point_data(p, fs):
     lib = load()
     o = make_params(p)
     nodes, offsets = _pack(fs)
+    foff = end_to_end_offsets(fs)
+    o.fil_offsets = foff.ctypes.data if foff is not None else None
     Np = int(offsets[-1])
     nq = o.nquad
     out = {k: np.zeros((Np, 3)) for k in ("nodes", "d1", "d2")}
@@ -190,6 +201,15 @@ def gl_rule(n):
     w = np.zeros(n)
     lib.vpo_gl_rule(n, _dp(z), _dp(w))
     return z, w
+
+
+def background_factor(p):
+    """Streamfunction factor of a uniform background vorticity (1/(4 alpha^2), or the Kaiser-Bessel
+    integral), as the oracle applies it."""
+    lib = load()
+    lib.vpo_background_factor.restype = ct.c_double
+    lib.vpo_background_factor.argtypes = [ct.POINTER(OParams)]
+    return lib.vpo_background_factor(ct.byref(make_params(p)))
 
 
 def fft_size(Ns, sigma):

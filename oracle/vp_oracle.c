@@ -128,6 +128,7 @@ typedef struct {
     double* c;         /* [n][3] B-spline coefficients, order 6 */
     double* d1;        /* [n][3] coefficients of s', order 5 */
     double* d2;        /* [n][3] coefficients of s'', order 4 */
+    double off[3];     /* end-to-end offset: the curve is y(t) + (t / T) off with y periodic */
 } spline_t;
 
 static inline double knot(const spline_t* S, long j) {
@@ -160,7 +161,9 @@ static void bsplvb(const spline_t* S, long i, double x, int k, double* N) {
     }
 }
 
-/* Evaluate derivative `der` (0,1,2) of the spline at parameter x within interval i. */
+/* Evaluate derivative `der` (0,1,2) of the spline at parameter x within interval i.  With an
+ * end-to-end offset the periodic spline y is deperiodised: s = y + (x / T) off, s' = y' + off / T,
+ * s'' = y'' (spline.jl:185-194). */
 static void spline_eval(const spline_t* S, long i, double x, int der, double* out) {
     int k = 6 - der;
     const double* cs = der == 0 ? S->c : (der == 1 ? S->d1 : S->d2);
@@ -171,6 +174,10 @@ static void spline_eval(const spline_t* S, long i, double x, int der, double* ou
         long j = pmod(i - k + 1 + s, S->n);
         for (int d = 0; d < 3; ++d) out[d] += cs[3 * j + d] * N[s];
     }
+    if (der == 0)
+        for (int d = 0; d < 3; ++d) out[d] += (x / S->T) * S->off[d];
+    else if (der == 1)
+        for (int d = 0; d < 3; ++d) out[d] += S->off[d] / S->T;
 }
 
 /* Evaluate at local coordinate zeta in [0,1] on segment i (spline.jl:116-124). */
@@ -207,14 +214,18 @@ static int solve4(double H[4][4], double r[4][3]) {
     return 0;
 }
 
-/* Build the periodic quintic interpolating spline through X_0..X_{n-1} (closed curve).
+/* Build the periodic quintic interpolating spline through X_0..X_{n-1} (closed curve; with an
+ * end-to-end offset `off` (NULL: zero) the node after X_{n-1} is X_0 + off, the chordal knots
+ * include that closing segment and the periodic spline interpolates y_i = X_i - (t_i / T) off,
+ * closed_filament.jl:196-207, spline.jl:163-182, quintic.jl:9-17).
  * The cyclic pentadiagonal collocation system is split as A = B + U W with B the
  * (non-cyclic) pentadiagonal part and U W the four wrap-around corner rows; B is
  * factorised by banded elimination without pivoting (B-spline collocation matrices
  * are totally positive) and the corners are handled with the Woodbury identity. */
-static int spline_build(spline_t* S, int n, const double* X) {
+static int spline_build(spline_t* S, int n, const double* X, const double* off) {
     if (n < 5) return -1;
     S->n = n;
+    for (int d = 0; d < 3; ++d) S->off[d] = off ? off[d] : 0.0;
     S->t = (double*)malloc(sizeof(double) * n);
     S->c = (double*)malloc(sizeof(double) * 3 * n);
     S->d1 = (double*)malloc(sizeof(double) * 3 * n);
@@ -224,8 +235,9 @@ static int spline_build(spline_t* S, int n, const double* X) {
     for (int i = 0; i < n; ++i) {
         S->t[i] = t;
         int j = (i + 1) % n;
-        double dx = X[3 * j] - X[3 * i], dy = X[3 * j + 1] - X[3 * i + 1], dz = X[3 * j + 2] - X[3 * i + 2];
-        t += sqrt(dx * dx + dy * dy + dz * dz);
+        double e[3];
+        for (int d = 0; d < 3; ++d) e[d] = X[3 * j + d] + (j == 0 ? S->off[d] : 0.0) - X[3 * i + d];
+        t += sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
     }
     S->T = t;
 
@@ -264,7 +276,7 @@ static int spline_build(spline_t* S, int n, const double* X) {
     /* right-hand sides: 3 coordinates + 4 columns of U */
     double* Y = (double*)malloc(sizeof(double) * 7 * n);
     for (int i = 0; i < n; ++i) {
-        for (int d = 0; d < 3; ++d) Y[7 * i + d] = X[3 * i + d];
+        for (int d = 0; d < 3; ++d) Y[7 * i + d] = X[3 * i + d] - (S->t[i] / S->T) * S->off[d];
         for (int q = 0; q < 4; ++q) Y[7 * i + 3 + q] = (i == Urow[q]) ? 1.0 : 0.0;
     }
     for (int i = 0; i < n; ++i)          /* forward (unit lower) */
@@ -379,7 +391,10 @@ int vpo_point_data(const vpo_params* p, int nfil, const int64_t* offsets, const 
         int64_t off = offsets[f];
         int n = (int)(offsets[f + 1] - off);
         spline_t S;
-        if (spline_build(&S, n, nodes_xyz + 3 * off) != 0) { err |= 1; continue; }
+        if (spline_build(&S, n, nodes_xyz + 3 * off, p->fil_offsets ? p->fil_offsets + 3 * f : NULL) != 0) {
+            err |= 1;
+            continue;
+        }
         filament_point_data(p, &S, nodes_xyz + 3 * off, off, zq, wq, nodes_f, idx_prev, d1, d2, dm, dp, points, charges);
         spline_free(&S);
     }
@@ -1234,6 +1249,50 @@ int vpo_vorticity_fourier(const vpo_params* p, int64_t Nq, const double* points,
 /* compute_on_nodes!  (reference: src/BiotSavart/BiotSavart.jl:395-612)      */
 /* ------------------------------------------------------------------------- */
 
+/* Streamfunction factor of a uniform background vorticity (background_vorticity_correction_factor):
+ * 1 / (4 alpha^2) for the Gaussian splitting (gaussian.jl:241), and for the Kaiser-Bessel one
+ * C = int_0^rcut r^2 f(r) dr / 2 with f(r) = beta / (rcut sinh beta) I0(beta sqrt(1 - r^2/rcut^2))
+ * (kaiser_bessel.jl:160-165, 280), here by 64-point Gauss-Legendre quadrature (the integrand is
+ * analytic in r^2 on [0, rcut]). */
+double vpo_background_factor(const vpo_params* p) {
+    if (p->splitting == 1) {
+        double z[64], w[64];
+        vpo_gl_rule(64, z, w);
+        const double rc = p->rcut, beta = p->kb_beta;
+        double acc = 0.0;
+        for (int q = 0; q < 64; ++q) {
+            const double r = z[q] * rc, u = r / rc;
+            const double f = beta / (rc * sinh(beta)) * bessel_i0(beta * sqrt(fmax(0.0, 1.0 - u * u)));
+            acc += w[q] * rc * r * r * f;
+        }
+        return acc / 2.0;
+    }
+    return 1.0 / (4.0 * p->alpha * p->alpha);
+}
+
+/* background_vorticity_correction! (BiotSavart.jl:255-286): with a non-zero sum p of the
+ * end-to-end offsets, psi += -(p Gamma / V) C on every node. */
+static void background_correction(const vpo_params* p, int nfil, int64_t Np, double* psi) {
+    if (!p->fil_offsets || !psi) return;
+    double ptot[3] = {0, 0, 0};
+    for (int f = 0; f < nfil; ++f)
+        for (int d = 0; d < 3; ++d) ptot[d] += p->fil_offsets[3 * f + d];
+    /* isapprox(p + Ls, Ls) with the default rtol sqrt(eps): nothing to do */
+    double dn = 0.0, na = 0.0, nb = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        dn += ptot[d] * ptot[d];
+        na += (ptot[d] + p->L[d]) * (ptot[d] + p->L[d]);
+        nb += p->L[d] * p->L[d];
+    }
+    if (sqrt(dn) <= sqrt(2.220446049250313e-16) * fmax(sqrt(na), sqrt(nb))) return;
+    const double V = p->L[0] * p->L[1] * p->L[2];
+    const double C = vpo_background_factor(p);
+    double back[3];
+    for (int d = 0; d < 3; ++d) back[d] = -ptot[d] * (p->Gamma / V) * C;
+    for (int64_t i = 0; i < Np; ++i)
+        for (int d = 0; d < 3; ++d) psi[3 * i + d] += back[d];
+}
+
 int vpo_compute_on_nodes(const vpo_params* p, int nfil, const int64_t* offsets, const double* nodes_xyz,
                          int lia_mode, int shortrange, int longrange,
                          double* vel_out, double* psi_out, vpo_stats* st) {
@@ -1305,11 +1364,16 @@ int vpo_compute_on_nodes(const vpo_params* p, int nfil, const int64_t* offsets, 
             for (int f = 0; f < nfil; ++f) {
                 spline_t S;
                 int64_t off = offsets[f];
-                if (spline_build(&S, (int)(offsets[f + 1] - off), nodes_xyz + 3 * off) != 0) { err = -2; break; }
+                if (spline_build(&S, (int)(offsets[f + 1] - off), nodes_xyz + 3 * off,
+                                 p->fil_offsets ? p->fil_offsets + 3 * f : NULL) != 0) {
+                    err = -2;
+                    break;
+                }
                 local_integrals(p, &S, off, nodes_f, vel_out, psi_out);
                 spline_free(&S);
             }
         }
+        if (lia_mode != 2 && ewald_on(p)) background_correction(p, nfil, Np, psi_out);
     }
 done:
     free(nodes_f); free(idx_prev); free(d1); free(d2); free(dm); free(dp); free(points); free(charges);

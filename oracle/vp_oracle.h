@@ -40,6 +40,8 @@ typedef struct {
     int    splitting;                /* 0: Gaussian (alpha) / none; 1: Kaiser-Bessel */
     double kb_beta;                  /* Kaiser-Bessel shape parameter */
     double kb_rtol;                  /* Kaiser-Bessel rtol (Chebyshev truncation) */
+    const double* fil_offsets;       /* [nfil][3] end-to-end offsets of the filaments (NULL: all
+                                        zero, closed filaments; closed_filament.jl:118-132) */
 } vpo_params;
 
 /* Kaiser-Bessel short-range weights 1 - F(r) and 1 - F(r) + r f(r) from the truncated
@@ -73,6 +75,10 @@ int vpo_point_data(const vpo_params* p, int nfil, const int64_t* offsets, const 
  * interleaved: out[((c*Ns2 + iz)*Ns1 + iy)*(Ns0/2+1) + ix] (re, im). */
 int vpo_vorticity_fourier(const vpo_params* p, int64_t Nq, const double* points, const double* charges,
                           double* uhat_out, vpo_stats* st);
+
+/* Streamfunction factor of a uniform background vorticity: 1 / (4 alpha^2) (Gaussian) or
+ * int_0^rcut r^2 f(r) dr / 2 (Kaiser-Bessel); reference: BiotSavart.jl:255-286. */
+double vpo_background_factor(const vpo_params* p);
 
 /* Full compute_on_nodes! (reference: src/BiotSavart/BiotSavart.jl:395-612).
  * lia_mode: 0 = Val(false), 1 = Val(true), 2 = Val(:only).

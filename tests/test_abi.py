@@ -174,3 +174,32 @@ def test_periodic_helpers_on_host(vp, built_lib):
         while y >= L:
             y -= L
         assert fi == y
+
+
+@pytest.mark.parametrize("case", ["gaussian_beta4", "gaussian_beta5.5", "kaiser_bessel_12.44", "kaiser_bessel_30"])
+def test_f32_pair_weights(vp, built_lib, case):
+    """The mixed form's FP32 pair-kernel weights (cubic tables on 1/32-wide intervals in x = alpha r)
+    against FP64: erfc / erfc + 2x/sqrt(pi) e^-x^2 (gaussian.jl:273-279) and the oracle's Kaiser-Bessel
+    series (kaiser_bessel.jl:139-147), to 2e-7 absolute over [0, r_cut]."""
+    from scipy.special import erfc
+    from vortexpasta_b200 import _lib
+    from oracle import oracle as O
+    lib = _lib.load()
+    rcut = 0.3
+    r = np.linspace(0.0, rcut, 20001)
+    a = np.zeros(len(r), dtype=np.float32)
+    g = np.zeros(len(r), dtype=np.float32)
+    fp = lambda x: x.ctypes.data_as(_lib.c_float_p)
+    if case.startswith("gaussian"):
+        beta = float(case.split("beta")[1])
+        alpha = beta / rcut
+        assert lib.vpbs_f32_weights_eval(0, alpha, rcut, 0.0, 0.0, _lib.dptr(r), len(r), fp(a), fp(g)) == 0
+        x = alpha * r
+        ea, eg = erfc(x), erfc(x) + 2 / math.sqrt(math.pi) * x * np.exp(-x * x)
+    else:
+        beta = float(case.split("_")[-1])
+        rtol = 10 ** (-0.2) * math.exp(-beta)
+        assert lib.vpbs_f32_weights_eval(1, 0.0, rcut, beta, rtol, _lib.dptr(r), len(r), fp(a), fp(g)) == 0
+        ea, eg, _ = O.kb_weights(beta, rcut, rtol, r)
+    assert np.abs(a - ea).max() < 2e-7
+    assert np.abs(g - eg).max() < 2e-7

@@ -152,3 +152,57 @@ def test_golden_ring64(vp, oracle):
     v, psi, st = oracle.compute_on_nodes(p, fs, streamfunction=True)
     assert rel(v, g["velocity"]) < 1e-13 and rel(psi, g["streamfunction"]) < 1e-13
     assert st["pairs_in_range"] == int(g["pairs_in_range"])
+
+
+def _helical_lines(vp, Np=64, Nx=4):
+    """The 4x4 array of aligned periodic lines with identical helical perturbations of the
+    reference's test/background_vorticity.jl:34-50 (L = 2 pi, PeriodicLine(r = t -> cispi(4t) / 100))."""
+    L = 2 * math.pi
+    xs = np.linspace(0, L, 2 * Nx + 1)[1::2]
+    return [vp.curves.periodic_line(Np, L, r=lambda t: np.exp(4j * np.pi * t) / 100, translate=(x, y, L / 2))
+            for x in xs for y in xs]
+
+
+@pytest.mark.parametrize("splitting", ["gaussian", "kaiser_bessel"])
+def test_infinite_lines_independent_of_splitting(vp, oracle, splitting):
+    """test/background_vorticity.jl:57-81: infinite lines with a non-zero mean vorticity give the same
+    velocity (rtol 2e-6) and streamfunction (rtol 2e-7, thanks to the background-vorticity correction
+    of BiotSavart.jl:255-286) with Ns = 32 and 64 (alpha changes by a factor 2)."""
+    L = 2 * math.pi
+    fs = _helical_lines(vp)
+    assert all(np.allclose(vp.curves.end_to_end_offset(f), [0, 0, L]) for f in fs)
+    res = []
+    for Ng in (32, 64):
+        sp = (vp.GaussianSplitting(Ls=L, rtol=1e-6, Ns=Ng) if splitting == "gaussian"
+              else vp.KaiserBesselSplitting(Ls=L, rtol=1e-6, Ns=(Ng,) * 3))
+        p = vp.ParamsBiotSavart(Gamma=2.0, a=1e-8, splitting=sp, backend_long=vp.NonuniformFFTsBackend(1.5, 4))
+        v, psi, _ = oracle.compute_on_nodes(p, fs, streamfunction=True)
+        # the correction the oracle applied: -(sum of offsets) Gamma / V * C
+        back = -(16 * L) * 2.0 / L ** 3 * oracle.background_factor(p)
+        res.append((v, psi, back))
+    Np = 64
+    for i in range(len(fs)):
+        s = slice(i * Np, (i + 1) * Np)
+        (v1, p1, b1), (v2, p2, b2) = res
+        assert np.linalg.norm(v1[s] - v2[s]) <= 2e-6 * np.linalg.norm(v2[s])
+        assert np.linalg.norm(p1[s] - p2[s]) <= 2e-7 * np.linalg.norm(p2[s])
+        # without the correction the streamfunction would depend on the splitting
+        q1, q2 = p1[s].copy(), p2[s].copy()
+        q1[:, 2] -= b1
+        q2[:, 2] -= b2
+        assert np.linalg.norm(q1 - q2) > 100 * 2e-7 * np.linalg.norm(q2)
+
+
+def test_straight_infinite_line(vp, oracle):
+    """A straight periodic line along z: zero velocity (no curvature, images cancel), streamfunction
+    along z and uniform along the line; closing spline segment and offset handled (s' = L / T along z)."""
+    L = 2 * math.pi
+    f = vp.curves.periodic_line(32, L, translate=(L / 3, L / 5, L / 2))
+    p = vp.configs.params_for(L / 4, 3.5, 32, 5)
+    v, psi, _ = oracle.compute_on_nodes(p, [f], streamfunction=True)
+    assert np.abs(v).max() < 1e-7 * np.abs(psi).max()
+    assert np.abs(psi[:, :2]).max() < 1e-10 * np.abs(psi[:, 2]).max()
+    assert np.ptp(psi[:, 2]) < 1e-8 * np.abs(psi[:, 2]).max()
+    pd = oracle.point_data(p, [f])
+    np.testing.assert_allclose(pd["d1"][:, 2], 1.0, rtol=1e-12)  # chordal knots: |s'| = 1
+    np.testing.assert_allclose(pd["dp"], L / 32, rtol=1e-12)

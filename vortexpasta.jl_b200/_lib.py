@@ -49,6 +49,7 @@ SIGNATURES = {
     "vpbs_last_error": (ct.c_char_p, [ct.c_void_p]),
     "vpbs_set_stream": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
     "vpbs_set_filaments": (ct.c_int, [ct.c_void_p, ct.c_int64, c_int64_p, ct.c_void_p, ct.c_int32]),
+    "vpbs_set_filament_offsets": (ct.c_int, [ct.c_void_p, ct.c_int64, c_double_p]),
     "vpbs_set_points": (ct.c_int, [ct.c_void_p, ct.c_int64, CVec3, c_int32_p, CVec3, CVec3, c_double_p, c_double_p,
                                    CVec3, CVec3]),
     "vpbs_compute": (ct.c_int, [ct.c_void_p, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_double]),
@@ -68,6 +69,8 @@ SIGNATURES = {
     "vpbs_ewald_table_eval": (ct.c_int, [ct.c_double, c_double_p, ct.c_int64, c_double_p, c_double_p]),
     "vpbs_kb_weights": (ct.c_int, [ct.c_double, ct.c_double, ct.c_double, c_double_p, ct.c_int64, c_double_p,
                                    c_double_p, c_double_p, c_double_p]),
+    "vpbs_f32_weights_eval": (ct.c_int, [ct.c_int32, ct.c_double, ct.c_double, ct.c_double, ct.c_double, c_double_p,
+                                         ct.c_int64, c_float_p, c_float_p]),
     "vpbs_periodic_eval": (ct.c_int, [ct.c_double, ct.c_int32, c_double_p, ct.c_int64, c_double_p, c_int64_p]),
     "vpbs_point_data_noalloc": (ct.c_int, [ct.POINTER(VpbsParams), ct.c_int64, c_int64_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
@@ -92,6 +95,7 @@ SIGNATURES = {
     "vpbs_ensemble_destroy": (ct.c_int, [ct.c_void_p]),
     "vpbs_ensemble_last_error": (ct.c_char_p, []),
     "vpbs_autotune": (ct.c_int, [ct.c_void_p, c_int32_p]),
+    "vpbs_pair_block": (ct.c_int, [ct.c_void_p, ct.c_int32]),
     "vpbs_mlp_create": (ct.c_int, [ct.c_int32, ct.c_int32, ct.POINTER(ct.c_void_p)]),
     "vpbs_mlp_destroy": (ct.c_int, [ct.c_void_p]),
     "vpbs_mlp_last_error": (ct.c_char_p, [ct.c_void_p]),

@@ -16,7 +16,7 @@ import ctypes as ct
 
 import numpy as np
 
-from . import _lib
+from . import _lib, curves
 from .curves import concat
 from .params import KaiserBesselSplitting, NoSplitting, ParamsBiotSavart
 
@@ -105,10 +105,32 @@ class BiotSavartCache:
     def set_stream(self, stream_ptr: int | None):
         _lib.check(self._lib.vpbs_set_stream(self._h, ct.c_void_p(stream_ptr or 0)), self._h, "set_stream")
 
-    def set_filaments(self, fs, on_device_ptr: int | None = None, offsets=None):
+    def set_end_to_end_offsets(self, offs):
+        """End-to-end offsets of the next filaments ([nfil, 3], or None for closed filaments), the
+        ``Xoffset`` of unclosed filaments (closed_filament.jl:118-132); re-sent only when changed."""
+        offs = None if offs is None else np.ascontiguousarray(offs, dtype=np.float64).reshape(-1, 3)
+        if offs is not None and not np.any(offs):
+            offs = None
+        prev = getattr(self, "_fil_off", None)
+        if (offs is None and prev is None) or (offs is not None and prev is not None and prev.shape == offs.shape
+                                               and np.array_equal(prev, offs)):
+            return
+        if offs is None:
+            rc = self._lib.vpbs_set_filament_offsets(self._h, 0, None)
+        else:
+            rc = self._lib.vpbs_set_filament_offsets(self._h, len(offs), _lib.dptr(offs))
+        _lib.check(rc, self._h, "set_filament_offsets")
+        self._fil_off = None if offs is None else offs.copy()
+
+    def set_filaments(self, fs, on_device_ptr: int | None = None, offsets=None, end_to_end=None):
         """add_point_charges! on the device. `fs`: list of (N, 3) arrays (assembled straight into
-        the handle's pinned staging buffer), or None with a device pointer to AoS nodes plus host
-        `offsets`."""
+        the handle's pinned staging buffer; an array with an ``offset`` attribute is an unclosed
+        filament, ``curves.InfiniteFilament``), or None with a device pointer to AoS nodes plus host
+        `offsets` (and the filaments' end-to-end offsets `end_to_end`, [nfil, 3], if any)."""
+        if on_device_ptr is None:
+            self.set_end_to_end_offsets(np.array([curves.end_to_end_offset(f) for f in fs]))
+        else:
+            self.set_end_to_end_offsets(end_to_end)
         if on_device_ptr is None:
             n = len(fs)
             counts = np.fromiter(map(len, fs), dtype=np.int64, count=n)
@@ -130,9 +152,10 @@ class BiotSavartCache:
         self.Np = int(offsets[-1])
         self._offsets = np.asarray(offsets)
 
-    def set_filaments_flat(self, nodes: np.ndarray, offsets: np.ndarray):
+    def set_filaments_flat(self, nodes: np.ndarray, offsets: np.ndarray, end_to_end=None):
         """add_point_charges! from one host AoS array [Np][3] and filament offsets (the flat C-ABI
-        call vpbs_set_filaments with host nodes)."""
+        call vpbs_set_filaments with host nodes); `end_to_end`: [nfil, 3] offsets of unclosed filaments."""
+        self.set_end_to_end_offsets(end_to_end)
         nodes = np.ascontiguousarray(nodes, dtype=np.float64)
         offsets = np.ascontiguousarray(offsets, dtype=np.int64)
         rc = self._lib.vpbs_set_filaments(self._h, len(offsets) - 1, offsets.ctypes.data_as(_lib.c_int64_p),

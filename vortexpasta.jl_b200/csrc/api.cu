@@ -254,8 +254,17 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
                 tab2[2 * (k * kEwaldNC + n)] = tab[k * kEwaldNC + n];
                 tab2[2 * (k * kEwaldNC + n) + 1] = tab[(ntab + k) * kEwaldNC + n];
             }
+        // FP32 cubic tables of the mixed form's pair kernel, stored after the interleaved table
+        const double xmax_c = kb ? kb_table_xmax(P.kb_beta) : P.alpha * P.rcut;
+        const int ntab_c = f32_table_size(xmax_c);
+        std::vector<float4> tabc((size_t)2 * ntab_c);
+        f32_table_host(tab.data(), ntab, xmax_c, tabc.data());
         const size_t bytes_d = sizeof(double) * tab.size(), bytes_f = sizeof(float) * tabf.size();
-        if (!rc) rc = ensure(h, h->ewald_tab, 2 * bytes_d + bytes_f, "Ewald tables");
+        const size_t off_c = (2 * bytes_d + bytes_f + 15) / 16 * 16, bytes_c = sizeof(float4) * tabc.size();
+        if (!rc) rc = ensure(h, h->ewald_tab, off_c + bytes_c, "Ewald tables");
+        if (!rc)
+            rc = check_cuda(h, cudaMemcpy((char*)h->ewald_tab.p + off_c, tabc.data(), bytes_c, cudaMemcpyHostToDevice),
+                            "copy Ewald tables");
         if (!rc)
             rc = check_cuda(h, cudaMemcpy((char*)h->ewald_tab.p + bytes_d + bytes_f, tab2.data(), bytes_d,
                                           cudaMemcpyHostToDevice), "copy Ewald tables");
@@ -268,6 +277,26 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
         h->K.ewald_tab_f = (const float*)((const char*)h->ewald_tab.p + bytes_d);
         h->K.ewald_tab2 = (const double2*)((const char*)h->ewald_tab.p + bytes_d + bytes_f);
         h->K.ewald_ntab = ntab;
+        h->K.tab_c = (const float4*)((const char*)h->ewald_tab.p + off_c);
+        h->K.ntab_c = ntab_c;
+        // streamfunction factor of a uniform background vorticity (BiotSavart.jl:255-286): 1 / (4 alpha^2)
+        // for the Gaussian splitting (gaussian.jl:241); int_0^rcut r^2 f(r) dr / 2 for the Kaiser-Bessel one
+        // (kaiser_bessel.jl:160-165, 280), with f(r) = beta / (rcut sinh beta) I0(beta sqrt(1 - r^2 / rcut^2)),
+        // by 64-point Gauss-Legendre quadrature (the integrand is analytic in r^2)
+        if (kb) {
+            std::vector<double> gx, gw;
+            gauss_legendre(64, gx, gw);
+            double acc = 0.0;
+            const double rc_ = P.rcut, b_ = P.kb_beta;
+            for (int q = 0; q < 64; ++q) {
+                const double z = 0.5 * (gx[q] + 1.0), w = 0.5 * gw[q], r = z * rc_, u = r / rc_;
+                const double f = b_ / (rc_ * std::sinh(b_)) * std::cyl_bessel_i(0.0, b_ * std::sqrt(std::fmax(0.0, 1.0 - u * u)));
+                acc += w * rc_ * r * r * f;
+            }
+            h->bg_factor = acc / 2.0;
+        } else {
+            h->bg_factor = 1.0 / (4.0 * P.alpha * P.alpha);
+        }
     }
     if (rc) {
         g_create_error = h->err;
@@ -364,6 +393,9 @@ static int set_filaments_staged(vpbs_handle* h, int64_t nfil, const int64_t* off
         d_nodes = (const double*)h->nodes_in.p;
     }
     if ((rc = check_cuda(h, cudaEventRecord(h->h2d_done, h->stream), "event record"))) return rc;
+    if (h->have_fil_offsets && h->nfil_off != nfil)
+        return set_error(h, VPBS_ERR_ARG, "end-to-end offsets were set for " + std::to_string(h->nfil_off) +
+                                              " filaments, not " + std::to_string(nfil));
     h->nfil = nfil;
     h->host_offsets.assign(offsets, offsets + nfil + 1);
     int64_t nmax = 0;
@@ -422,6 +454,34 @@ int vpbs_set_filaments(vpbs_handle* h, int64_t nfil, const int64_t* offsets, con
             return rc;
     }
     return set_filaments_staged(h, nfil, offsets, (const double*)h->nodes_in.p);
+}
+
+int vpbs_set_filament_offsets(vpbs_handle* h, int64_t nfil, const double* offsets_xyz) {
+    if (!h) return VPBS_ERR_ARG;
+    if (nfil < 0 || (nfil > 0 && !offsets_xyz)) return set_error(h, VPBS_ERR_ARG, "vpbs_set_filament_offsets: bad arguments");
+    int rc;
+    if ((rc = activate(h))) return rc;
+    double sum[3] = {0.0, 0.0, 0.0};
+    bool any = false;
+    for (int64_t f = 0; f < nfil; ++f)
+        for (int d = 0; d < 3; ++d) {
+            const double v = offsets_xyz[3 * f + d];
+            if (!std::isfinite(v)) return set_error(h, VPBS_ERR_ARG, "vpbs_set_filament_offsets: non-finite offset");
+            any = any || v != 0.0;
+            sum[d] += v;
+        }
+    // the geometry kernels of earlier calls may still read the previous offsets
+    if ((rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync"))) return rc;
+    if (any) {
+        if ((rc = ensure(h, h->fil_off, sizeof(double) * 3 * nfil, "filament offsets"))) return rc;
+        if ((rc = check_cuda(h, cudaMemcpy(h->fil_off.p, offsets_xyz, sizeof(double) * 3 * nfil, cudaMemcpyHostToDevice),
+                             "H2D filament offsets")))
+            return rc;
+    }
+    h->have_fil_offsets = any;
+    h->nfil_off = nfil;
+    for (int d = 0; d < 3; ++d) h->offset_sum[d] = any ? sum[d] : 0.0;
+    return 0;
 }
 
 int vpbs_stage_filaments(vpbs_handle* h, int64_t nfil, int64_t Np, int64_t** offsets, double** nodes) {
@@ -880,6 +940,40 @@ extern "C" int vpbs_fma_throughput(int32_t device, int32_t fp64, double* tflops)
     cudaFree(out);
     if (err != cudaSuccess) return set_error(nullptr, VPBS_ERR_CUDA, cudaGetErrorString(err));
     *tflops = best;
+    return 0;
+}
+
+extern "C" int vpbs_f32_weights_eval(int32_t splitting, double alpha, double rcut, double kb_beta, double kb_rtol,
+                                     const double* r, int64_t n, float* a, float* g) {
+    using namespace vpbs;
+    if (!r || !a || !g || n < 0 || !(rcut > 0)) return set_error(nullptr, VPBS_ERR_ARG, "vpbs_f32_weights_eval: bad arguments");
+    const bool kb = splitting == VPBS_SPLITTING_KAISER_BESSEL;
+    if (!kb && !(alpha > 0)) return set_error(nullptr, VPBS_ERR_ARG, "vpbs_f32_weights_eval: alpha must be positive");
+    int ntab = 0;
+    std::vector<double> tab;
+    double xmax, s;
+    if (kb) {
+        const KBSeries S = kb_series(kb_beta, rcut, kb_rtol);
+        if (S.f.empty()) return set_error(nullptr, VPBS_ERR_PARAMS, "Kaiser-Bessel series did not converge");
+        kb_table_host(S, &ntab, nullptr);
+        tab.resize((size_t)2 * ntab * kEwaldNC);
+        kb_table_host(S, &ntab, tab.data());
+        xmax = kb_table_xmax(kb_beta);
+    } else {
+        xmax = alpha * rcut;
+        ewald_table_host(xmax, &ntab, nullptr);
+        tab.resize((size_t)2 * ntab * kEwaldNC);
+        ewald_table_host(xmax, &ntab, tab.data());
+    }
+    s = xmax / rcut;
+    const int nf = f32_table_size(xmax);
+    std::vector<float4> tabc((size_t)2 * nf);
+    f32_table_host(tab.data(), ntab, xmax, tabc.data());
+    for (int64_t i = 0; i < n; ++i) {
+        if (!(r[i] >= 0.0 && r[i] <= rcut)) return set_error(nullptr, VPBS_ERR_ARG, "vpbs_f32_weights_eval: r outside [0, rcut]");
+        // the kernel forms x = (r^2 rsqrt(r^2)) alpha in FP32; here x = alpha r rounded to FP32
+        f32_table_eval_host(tabc.data(), nf, (float)(s * r[i]), &a[i], &g[i]);
+    }
     return 0;
 }
 

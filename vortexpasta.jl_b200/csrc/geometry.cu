@@ -17,7 +17,20 @@ struct FilView {
     const double* t;  // knots of this filament (n values, t[0] = 0)
     double T;         // knot period
     int n;
+    double o[3];      // end-to-end offset (zero for a closed filament)
 };
+
+// FilView of filament fidx; `foff` ([nfil][3] end-to-end offsets) may be null (closed filaments).
+__device__ __forceinline__ FilView fil_view(const double* knots, const double* periods, const double* foff,
+                                            int64_t off, int n, int64_t fidx) {
+    FilView f{knots + off, periods[fidx], n, {0.0, 0.0, 0.0}};
+    if (foff) {
+        f.o[0] = foff[3 * fidx];
+        f.o[1] = foff[3 * fidx + 1];
+        f.o[2] = foff[3 * fidx + 2];
+    }
+    return f;
+}
 
 __device__ __forceinline__ long pmodl(long j, long n) {
     long r = j % n;
@@ -67,6 +80,15 @@ __device__ __forceinline__ void eval_seg(const FilView& f, const double* coef, l
         out[1] += coef[3 * j + 1] * N[s];
         out[2] += coef[3 * j + 2] * N[s];
     }
+    // an unclosed (infinite) filament is the periodic spline y plus (x / T) offset (spline.jl:185-194)
+    if (D == 0) {
+        const double r = x / f.T;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) out[d] += r * f.o[d];
+    } else if (D == 1) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) out[d] += f.o[d] / f.T;
+    }
 }
 
 // Solve the 4x4 Woodbury capacitance system with partial pivoting (3 right-hand sides).
@@ -101,7 +123,8 @@ __global__ void __launch_bounds__(128) spline_solve_kernel(
     int64_t nfil, const int64_t* __restrict__ offsets, const double* __restrict__ X,
     double* __restrict__ knots, double* __restrict__ periods, int32_t* __restrict__ fil_of_node,
     double* __restrict__ coef, double* __restrict__ dcoef1, double* __restrict__ dcoef2,
-    double* __restrict__ scratch, int32_t* __restrict__ status, int smem_n, int keep_knots) {
+    double* __restrict__ scratch, int32_t* __restrict__ status, int smem_n, int keep_knots,
+    const double* __restrict__ foff) {
     extern __shared__ double sm_work[];
     const int lane = threadIdx.x & 31;
     const int64_t fidx = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -128,6 +151,11 @@ __global__ void __launch_bounds__(128) spline_solve_kernel(
         if (i < n) {
             int j = (i + 1 == n) ? 0 : i + 1;
             double dx = Xf[3 * j] - Xf[3 * i], dy = Xf[3 * j + 1] - Xf[3 * i + 1], dz = Xf[3 * j + 2] - Xf[3 * i + 2];
+            if (j == 0 && foff) {  // closing segment of an unclosed filament: to X_0 + offset
+                dx += foff[3 * fidx];
+                dy += foff[3 * fidx + 1];
+                dz += foff[3 * fidx + 2];
+            }
             len = sqrt(dx * dx + dy * dy + dz * dz);
             fil_of_node[off + i] = (int32_t)fidx;
         }
@@ -143,7 +171,11 @@ __global__ void __launch_bounds__(128) spline_solve_kernel(
     const double T = carry;
     if (lane == 0 && !keep_knots) periods[fidx] = T;
     __syncwarp();
-    FilView f{t, T, n};
+    FilView f{t, T, n, {0.0, 0.0, 0.0}};
+    // an unclosed filament is interpolated as the periodic y_i = X_i - (t_i / T) offset
+    // (spline.jl:163-182, quintic.jl:9-17)
+    const double o0 = foff ? foff[3 * fidx] : 0.0, o1 = foff ? foff[3 * fidx + 1] : 0.0,
+                 o2 = foff ? foff[3 * fidx + 2] : 0.0;
 
     // 2. collocation rows, band part only (corners handled below)
     for (int i = lane; i < n; i += 32) {
@@ -154,8 +186,10 @@ __global__ void __launch_bounds__(128) spline_solve_kernel(
             int col = i + s - 2;
             band[5 * i + s] = (col >= 0 && col < n) ? N[s] : 0.0;
         }
-#pragma unroll
-        for (int d = 0; d < 3; ++d) Y[7 * i + d] = Xf[3 * i + d];
+        const double r = t[i] / T;
+        Y[7 * i + 0] = Xf[3 * i + 0] - r * o0;
+        Y[7 * i + 1] = Xf[3 * i + 1] - r * o1;
+        Y[7 * i + 2] = Xf[3 * i + 2] - r * o2;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             int ur = (q == 0) ? 0 : (q == 1) ? 1 : (q == 2) ? n - 2 : n - 1;
@@ -286,14 +320,15 @@ __global__ void __launch_bounds__(128) point_data_kernel(
     const double* __restrict__ coef, const double* __restrict__ dcoef1, const double* __restrict__ dcoef2,
     double* __restrict__ nodes, int32_t* __restrict__ idx_prev, double* __restrict__ d1, double* __restrict__ d2,
     double* __restrict__ dm, double* __restrict__ dp, double* __restrict__ points, double* __restrict__ charges,
-    double* __restrict__ li_vel, double* __restrict__ li_psi, int want_li, int fuse_quad) {
+    double* __restrict__ li_vel, double* __restrict__ li_psi, int want_li, int fuse_quad,
+    const double* __restrict__ foff) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= Np) return;
     const int fidx = fil_of_node[k];
     const int64_t off = offsets[fidx];
     const int n = (int)(offsets[fidx + 1] - off);
     const int i = (int)(k - off);
-    FilView f{knots + off, periods[fidx], n};
+    const FilView f = fil_view(knots, periods, foff, off, n, fidx);
     const double* c = coef + 3 * off;
     const double* c1 = dcoef1 + 3 * off;
     const double* c2 = dcoef2 + 3 * off;
@@ -386,7 +421,8 @@ __global__ void dm_from_prev_kernel(int64_t Np, const int32_t* __restrict__ idx_
 __global__ void __launch_bounds__(128) quad_points_kernel(
     KParams K, int64_t Np, const int64_t* __restrict__ offsets, const int32_t* __restrict__ fil_of_node,
     const double* __restrict__ knots, const double* __restrict__ periods, const double* __restrict__ coef,
-    const double* __restrict__ dcoef1, double* __restrict__ points, double* __restrict__ charges) {
+    const double* __restrict__ dcoef1, double* __restrict__ points, double* __restrict__ charges,
+    const double* __restrict__ foff) {
     const int64_t Nq = Np * K.nquad;
     const int64_t mq = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (mq >= Nq) return;
@@ -396,7 +432,7 @@ __global__ void __launch_bounds__(128) quad_points_kernel(
     const int64_t off = offsets[fidx];
     const int n = (int)(offsets[fidx + 1] - off);
     const int i = (int)(k - off);
-    FilView f{knots + off, periods[fidx], n};
+    const FilView f = fil_view(knots, periods, foff, off, n, fidx);
     double s[3], sp[3];
     eval_seg<0>(f, coef + 3 * off, i, K.qz[q], s);
     eval_seg<1>(f, dcoef1 + 3 * off, i, K.qz[q], sp);
@@ -443,11 +479,13 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
     double* knots = (double*)h->knots.p;
     double* periods = knots + Np;
     int32_t* status = (int32_t*)((double*)h->spline_scratch.p + 12 * Np);
+    const double* foff = h->have_fil_offsets ? (const double*)h->fil_off.p : nullptr;
     StageScope st(h, ST_GEOMETRY);
     if ((rc = check_cuda(h, cudaMemsetAsync(status, 0, sizeof(int32_t), h->stream), "memset"))) return rc;
     spline_solve_kernel<<<grid_for(nfil, 4), 128, smem_bytes, h->stream>>>(
         nfil, d_offsets, d_nodes, knots, periods, (int32_t*)h->fil_of_node.p, (double*)h->coefs.p,
-        (double*)h->dcoef1.p, (double*)h->dcoef2.p, (double*)h->spline_scratch.p, status, smem_n, keep_knots ? 1 : 0);
+        (double*)h->dcoef1.p, (double*)h->dcoef2.p, (double*)h->spline_scratch.p, status, smem_n, keep_knots ? 1 : 0,
+        foff);
     h->launches++;
     const bool want_li = h->K.lia_fraction > 0;
     // without lia_segment_fraction the point-data kernel also writes the quadrature points
@@ -457,14 +495,14 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
         h->K, Np, d_offsets, (const int32_t*)h->fil_of_node.p, d_nodes, knots, periods, (const double*)h->coefs.p,
         (const double*)h->dcoef1.p, (const double*)h->dcoef2.p, (double*)h->nodes.p, (int32_t*)h->idx_prev.p,
         (double*)h->d1.p, (double*)h->d2.p, (double*)h->dm.p, (double*)h->dp.p, (double*)h->points.p,
-        (double*)h->charges.p, (double*)h->li_vel.p, (double*)h->li_psi.p, want_li ? 1 : 0, fuse ? 1 : 0);
+        (double*)h->charges.p, (double*)h->li_vel.p, (double*)h->li_psi.p, want_li ? 1 : 0, fuse ? 1 : 0, foff);
     if (fuse)
         dm_from_prev_kernel<<<grid_for(Np, 256), 256, 0, h->stream>>>(Np, (const int32_t*)h->idx_prev.p,
                                                                        (const double*)h->dp.p, (double*)h->dm.p);
     else
         quad_points_kernel<<<grid_for(Np * h->K.nquad, 128), 128, 0, h->stream>>>(
             h->K, Np, d_offsets, (const int32_t*)h->fil_of_node.p, knots, periods, (const double*)h->coefs.p,
-            (const double*)h->dcoef1.p, (double*)h->points.p, (double*)h->charges.p);
+            (const double*)h->dcoef1.p, (double*)h->points.p, (double*)h->charges.p, foff);
     h->launches += 2;
     return check_cuda(h, cudaGetLastError(), "geometry kernels");
 }
@@ -593,13 +631,13 @@ extern "C" int vpbs_point_data_noalloc(const vpbs_params* params, int64_t nfil, 
     if (e != cudaSuccess)
         return set_error(nullptr, VPBS_ERR_CUDA, std::string("vpbs_point_data_noalloc: ") + cudaGetErrorString(e));
     spline_solve_kernel<<<grid_for(nfil, 4), 128, 0, s>>>(nfil, d_offsets, nodes_xyz, knots, periods, fil_of_node, coefs,
-                                                          dcoef1, dcoef2, scratch, status, 0, 0);
+                                                          dcoef1, dcoef2, scratch, status, 0, 0, nullptr);
     point_data_kernel<<<grid_for(Np, 128), 128, 0, s>>>(K, Np, d_offsets, fil_of_node, nodes_xyz, knots, periods, coefs,
                                                         dcoef1, dcoef2, nodes, node_idx_prev, deriv1, deriv2,
                                                         delta_minus, delta_plus, points, charges, nullptr, nullptr, 0,
-                                                        0);
+                                                        0, nullptr);
     quad_points_kernel<<<grid_for(Np * K.nquad, 128), 128, 0, s>>>(K, Np, d_offsets, fil_of_node, knots, periods, coefs,
-                                                                   dcoef1, points, charges);
+                                                                   dcoef1, points, charges, nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess)
         return set_error(nullptr, VPBS_ERR_CUDA, std::string("vpbs_point_data_noalloc: ") + cudaGetErrorString(e));

@@ -17,7 +17,6 @@
 #include "vpbs_internal.cuh"
 
 namespace vpbs {
-namespace {
 
 // Gauss-Legendre rule on [-1, 1] by Newton iteration on P_n (host).
 void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
@@ -49,6 +48,9 @@ void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
         w[i] = 2.0 / ((1.0 - z * z) * dp * dp);
     }
 }
+
+namespace {
+
 
 // Fourier transform of the shifted ES kernel psi(u) = exp(beta (sqrt(1 - (u/m)^2) - 1)) - e^{-beta}, |u| <= m,
 // at frequency xi (radians per grid spacing): m * int_{-pi/2}^{pi/2} (e^{beta(cos t - 1)} - e^{-beta})

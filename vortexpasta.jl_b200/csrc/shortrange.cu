@@ -9,12 +9,40 @@
 //    stride over the contiguous cell-sorted source ranges of the (2M+1)^2 neighbour rows,
 //    warp-shuffle reduction at the end.
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "vpbs_internal.cuh"
 #include "periodic.cuh"
 
 namespace vpbs {
+
+// Interval and local coordinate of x in the FP32 cubic tables: k = floor(32 x) (rounded through
+// the 1.5 * 2^23 trick, no conversion instruction), t = 32 x - k; k is clamped into [0, nf).
+__host__ __device__ __forceinline__ void f32_table_pos(float x, int nf, int* k, float* t) {
+    const float u = fmaf(x, kTabCInvH, -0.5f);
+#if defined(__CUDA_ARCH__)
+    const float y = __fadd_rn(u, 12582912.0f);
+    const float kf = __fsub_rn(y, 12582912.0f);
+    int kk = __float_as_int(y) - 0x4B400000;
+#else
+    volatile float yv = u + 12582912.0f;
+    const float y = yv;
+    volatile float kv = y - 12582912.0f;
+    const float kf = kv;
+    int kk;
+    std::memcpy(&kk, &y, sizeof(int));
+    kk -= 0x4B400000;
+#endif
+    *t = fmaf(x, kTabCInvH, -kf);
+    const unsigned top = (unsigned)(nf - 1);
+    *k = (int)((unsigned)kk < top ? (unsigned)kk : top);
+}
+
+__host__ __device__ __forceinline__ float f32_cubic(float4 c, float t) {
+    return fmaf(fmaf(fmaf(c.w, t, c.z), t, c.y), t, c.x);
+}
+
 namespace {
 
 __device__ __forceinline__ int64_t cell_of(const CellGrid& cg, const KParams& K, double x, double y, double z) {
@@ -639,25 +667,30 @@ __global__ void __launch_bounds__(kPairThreads, 2) pair_cell_kernel(
             T1 = S.off[rf * WX] > T0 ? S.off[rf * WX] : min(T0 + kTile, ntot);
             const int rb = min(last_row_le(S.off, WX, nrow, T1 - 1) + 1, nrow);
             __syncthreads();  // previous tile consumed, destinations loaded
-            for (int ci = warp; ci < ncb; ci += kPairThreads / 32) {
-                const int o = S.off[ci];
-                const int a = o > T0 ? o : T0, b = S.off[ci + 1] < T1 ? S.off[ci + 1] : T1;
-                if (a >= b) continue;
-                // periodic image of this slab next to the destination cell
-                const int r = ci / WX, k = ci % WX;
-                const int xu = xs0 + k, yu = ry0 + r % WY, zu = rz0 + r / WY;
-                const double sx = xu < 0 ? -K.L[0] : (xu >= nc0 ? K.L[0] : 0.0);
+            // staging, a warp per row (periodic image of each slab next to the destination block): the
+            // slabs of a row are consecutive cells, so its sources are one contiguous range of the
+            // cell-sorted arrays, or two where the row wraps around the period in x
+            const int kw = xs0 < 0 ? -xs0 : (xs0 + WX > nc0 ? nc0 - xs0 : WX);  // first slab past the wrap
+            const double sxA = xs0 < 0 ? -K.L[0] : 0.0, sxB = xs0 < 0 ? 0.0 : K.L[0];
+            for (int r = ra + warp; r < rb; r += kPairThreads / 32) {
+                const int rowA = S.off[r * WX], rowE = S.off[(r + 1) * WX];
+                const int a = rowA > T0 ? rowA : T0, b = rowE < T1 ? rowE : T1;
+                if (a >= b) continue;  // warp-uniform
+                const int yu = ry0 + r % WY, zu = rz0 + r / WY;
                 const double sy = yu < 0 ? -K.L[1] : (yu >= nc1 ? K.L[1] : 0.0);
                 const double sz = zu < 0 ? -K.L[2] : (zu >= nc2 ? K.L[2] : 0.0);
-                const int g0 = S.cstart[ci] + (a - o);
-                for (int e = lane; e < b - a; e += 32) {
-                    const int j = g0 + e;
-                    const int t = a - T0 + e;
+                const int offB = S.off[r * WX + kw];
+                const int gA = S.cstart[r * WX];
+                const int gB = kw < WX ? S.cstart[r * WX + kw] : 0;
+                for (int t = a + lane; t < b; t += 32) {
+                    const bool inA = t < offB;
+                    const int j = inA ? gA + (t - rowA) : gB + (t - offB);
+                    const double sx = inA ? sxA : sxB;
                     const double u0 = src[j] + sx - o0, u1 = src[Ns + j] + sy - o1, u2 = src[2 * Ns + j] + sz - o2;
                     const float f0 = (float)u0, f1 = (float)u1, f2 = (float)u2;
-                    S.hi[t] = make_float4(f0, f1, f2, __int_as_float(j));
-                    S.lo[t] = make_float4((float)(u0 - f0), (float)(u1 - f1), (float)(u2 - f2),
-                                          __int_as_float(SKIP ? seg[j] : 0));
+                    S.hi[t - T0] = make_float4(f0, f1, f2, __int_as_float(j));
+                    S.lo[t - T0] = make_float4((float)(u0 - f0), (float)(u1 - f1), (float)(u2 - f2),
+                                               __int_as_float(SKIP ? seg[j] : 0));
                 }
             }
             __syncthreads();
@@ -739,6 +772,404 @@ __global__ void __launch_bounds__(kPairThreads, 2) pair_cell_kernel(
     }
 }
 
+// ---- FP32 pair kernel of the mixed form ----
+// Same decomposition as pair_cell_kernel (CTA per block of cells, the block's neighbour slabs
+// concatenated in (row, slab) order and streamed through shared memory in row-aligned tiles,
+// per-node candidate ranges trimmed to the slabs within r_cut), with every per-pair operation in
+// FP32 and every operand in shared memory:
+//  * staging: source position relative to the block corner split into FP32 hi + lo parts (from
+//    the FP64 position), FP32 charge, segment index; 32-source units spread over all warps;
+//  * per node, only the (2M+1)^2 rows around its own cell are examined (a lane each), and only
+//    the non-empty ones are walked;
+//  * screen: hi parts only, against r_cut^2 (1 + 2e-5) (their rounding is below 1e-6 r_cut^2);
+//  * separation of a queued pair: (x_hi - s_hi) + (x_lo - s_lo) -- the FP64 separation rounded
+//    to FP32 within ~2 ulps (the hi difference is rounded relative to the separation itself);
+//  * decision r^2 <= r_cut^2 in FP32, redone in FP64 from the hi + lo parts when r^2 lies within
+//    4e-6 r_cut^2 of the cut-off, so the pair set equals the FP64 one; local segments (avoid
+//    explicit erf off) are left out here;
+//  * weights from cubic tables on 1/32-wide intervals in x = alpha r (FP32, ~3e-8 absolute),
+//    interval index without a conversion instruction;
+//  * per-lane FP32 sums (a few pairs per lane and node), FP32 warp reduction, FP64 output sums.
+constexpr int kF32Tile = 1280;
+constexpr int kF32TilePad = kF32Tile + 32;  // a chunk of 32 lanes may read past the tile end (masked)
+constexpr int kF32MaxDst = 128;
+constexpr int kF32MaxNb = 576;    // neighbour slabs of a block: rows x slabs per row
+constexpr int kF32MaxRows = 36;   // (y, z) rows of a block's neighbourhood
+constexpr int kF32EvalU = 1;      // screened pairs per lane and evaluation (2: interleaved; measured slower)
+constexpr int kF32Queue = 32 * kF32EvalU + 32;  // screened pairs, evaluated 32 kF32EvalU at a time
+constexpr int kF32TabMax = 192;   // intervals per weight table (x = alpha r_cut <= 5.9)
+constexpr float kF32Band = 4e-6f; // relative band around r_cut^2 decided in FP64
+constexpr int kF32StageUnroll = 1;
+
+struct F32Smem {
+    float4 P[kF32TilePad];  // hi parts of the position, segment (int bits)
+    float4 Q[kF32TilePad];  // lo parts of the position, charge x
+    float2 R[kF32TilePad];  // charge y, z
+    float4 tab[2][kF32TabMax];
+    int32_t queue[kPairThreads / 32][kF32Queue];
+    double dx[kF32MaxDst][3];
+    float acc[kF32MaxDst][6];
+    int32_t di[kF32MaxDst], dprev[kF32MaxDst], drow[kF32MaxDst];  // drow: the node's own row, y | z << 8
+    int32_t dr_start[kMaxBlockRows], dr_cnt[kMaxBlockRows], dr_base[kMaxBlockRows + 1];
+    int32_t off[kF32MaxNb + 1];
+    int32_t cstart[kF32MaxNb];
+    int32_t row_gA[kF32MaxRows], row_gB[kF32MaxRows];  // first cell-sorted source of the row's two runs
+    int32_t row_code[kF32MaxRows];  // periodic image of the row: bits 0-1 / 2-3 = -L, 0, +L in y / z
+    double dc[9];  // block constants: corner o0, o1, o2; x images sxA, sxB; cell sizes hx, h1, h2; 1 / hx
+};
+static_assert(sizeof(F32Smem) <= 74 * 1024, "three FP32 pair-kernel CTAs must fit in one SM's shared memory");
+
+// U queued pairs per lane (tile indices t[u]; `valid[u]` false for the entries past the queue's end,
+// which evaluate a valid entry and add nothing); the U evaluations are interleaved.
+template <bool VEL, bool PSI, bool SKIP, int U>
+__device__ __forceinline__ void f32_eval(const KParams& K, const F32Smem& S, float3 xh, float3 xl, float rc2,
+                                         float alpha, int nf, int i, int iprev, const int (&t)[U],
+                                         const bool (&valid_in)[U], float acc[6], unsigned& ninr) {
+    float d0[U], d1[U], d2[U], s2[U], q0[U], q1[U], q2[U];
+    bool ok[U], near[U], anynear = false;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const float4 p = S.P[t[u]];
+        const float4 q = S.Q[t[u]];
+        const float2 qr = S.R[t[u]];
+        d0[u] = (xh.x - p.x) + (xl.x - q.x);
+        d1[u] = (xh.y - p.y) + (xl.y - q.y);
+        d2[u] = (xh.z - p.z) + (xl.z - q.z);
+        q0[u] = q.w;
+        q1[u] = qr.x;
+        q2[u] = qr.y;
+        s2[u] = fmaf(d0[u], d0[u], fmaf(d1[u], d1[u], d2[u] * d2[u]));
+        bool valid = valid_in[u];
+        if (SKIP) {
+            const int sg = __float_as_int(p.w);
+            valid = valid && sg != i && sg != iprev;
+        }
+        ok[u] = valid && s2[u] <= rc2;
+        near[u] = valid && fabsf(s2[u] - rc2) <= kF32Band * rc2;
+        anynear = anynear || near[u];
+    }
+    if (__any_sync(0xffffffffu, anynear)) {
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (near[u]) {  // the FP64 decision on the hi + lo separation (rare)
+                const float4 p = S.P[t[u]];
+                const float4 q = S.Q[t[u]];
+                const double e0 = ((double)xh.x + (double)xl.x) - ((double)p.x + (double)q.x);
+                const double e1 = ((double)xh.y + (double)xl.y) - ((double)p.y + (double)q.y);
+                const double e2 = ((double)xh.z + (double)xl.z) - ((double)p.z + (double)q.z);
+                ok[u] = e0 * e0 + e1 * e1 + e2 * e2 <= K.rcut2;
+            }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        ninr += __popc(__ballot_sync(0xffffffffu, ok[u]));
+        const float rinv = rsqrtf(s2[u]);
+        int k;
+        float tt;
+        f32_table_pos(s2[u] * rinv * alpha, nf, &k, &tt);
+        if (VEL) {
+            const float wg = f32_cubic(S.tab[1][k], tt);
+            const float f = ok[u] ? wg * (rinv * rinv * rinv) : 0.0f;
+            acc[0] = fmaf(f, fmaf(q1[u], d2[u], -q2[u] * d1[u]), acc[0]);
+            acc[1] = fmaf(f, fmaf(q2[u], d0[u], -q0[u] * d2[u]), acc[1]);
+            acc[2] = fmaf(f, fmaf(q0[u], d1[u], -q1[u] * d0[u]), acc[2]);
+        }
+        if (PSI) {
+            const float wa = f32_cubic(S.tab[0][k], tt);
+            const float f = ok[u] ? wa * rinv : 0.0f;
+            acc[3] = fmaf(f, q0[u], acc[3]);
+            acc[4] = fmaf(f, q1[u], acc[4]);
+            acc[5] = fmaf(f, q2[u], acc[5]);
+        }
+    }
+}
+
+template <bool VEL, bool PSI, bool SKIP>
+__global__ void __launch_bounds__(kPairThreads, 3) pair_f32_kernel(
+    KParams K, CellGrid cg, int64_t Np, int64_t Ns, const int32_t* __restrict__ dst_start,
+    const int32_t* __restrict__ dst_order, const double* __restrict__ nodes, const int32_t* __restrict__ idx_prev,
+    const double* __restrict__ src, const int32_t* __restrict__ src_start, const int32_t* __restrict__ seg,
+    double* __restrict__ vel, double* __restrict__ psi, unsigned long long* __restrict__ counters, int3 bk,
+    int3 nb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    F32Smem& S = *reinterpret_cast<F32Smem*>(smem_raw);
+    const int M = cg.M, G = cg.G;
+    const int nc0 = cg.nc[0], nc1 = cg.nc[1], nc2 = cg.nc[2];
+    const int ncc = nc0 / G;
+    const int bxi = blockIdx.x % nb.x, byi = (blockIdx.x / nb.x) % nb.y, bzi = blockIdx.x / (nb.x * nb.y);
+    const int cx0 = bxi * bk.x, cx1 = min(cx0 + bk.x, ncc);
+    const int cy0 = byi * bk.y, cy1 = min(cy0 + bk.y, nc1);
+    const int cz0 = bzi * bk.z, cz1 = min(cz0 + bk.z, nc2);
+    const int ndr = (cy1 - cy0) * (cz1 - cz0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int WY = cy1 - cy0 + 2 * M, WZ = cz1 - cz0 + 2 * M, WX = (cx1 - cx0 + 2 * M) * G;
+    const int nrow = WY * WZ, ncb = nrow * WX;
+    const int ry0 = cy0 - M, rz0 = cz0 - M, xs0 = cx0 * G - M * G;
+    // ---- prologue: destination rows, weight tables, neighbour slabs (independent loads) ----
+    if (threadIdx.x < ndr) {
+        const int k = threadIdx.x;
+        const int yy = cy0 + k % (cy1 - cy0), zz = cz0 + k / (cy1 - cy0);
+        const int64_t s0 = ((int64_t)zz * nc1 + yy) * nc0 + (int64_t)cx0 * G;
+        const int a = dst_start[s0], b = dst_start[s0 + (int64_t)(cx1 - cx0) * G];
+        S.dr_start[k] = a;
+        S.dr_cnt[k] = b - a;
+    }
+    const int nf = K.ntab_c;
+    for (int k = threadIdx.x; k < 2 * nf; k += kPairThreads) S.tab[k / nf][k % nf] = K.tab_c[k];
+    for (int ci = threadIdx.x; ci < ncb; ci += kPairThreads) {
+        const int r = ci / WX, k = ci % WX;
+        int xx = xs0 + k, yy = ry0 + r % WY, zz = rz0 + r / WY;
+        xx = xx < 0 ? xx + nc0 : (xx >= nc0 ? xx - nc0 : xx);
+        yy = yy < 0 ? yy + nc1 : (yy >= nc1 ? yy - nc1 : yy);
+        zz = zz < 0 ? zz + nc2 : (zz >= nc2 ? zz - nc2 : zz);
+        const int64_t c = ((int64_t)zz * nc1 + yy) * nc0 + xx;
+        const int s0 = src_start[c];
+        S.cstart[ci] = s0;
+        S.off[ci + 1] = src_start[c + 1] - s0;
+    }
+    __syncthreads();
+    if (warp == 0) {  // slab counts -> concatenated offsets
+        int carry = 0;
+        for (int base = 0; base < ncb; base += 32) {
+            const int ci = base + lane;
+            int v = ci < ncb ? S.off[ci + 1] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += t;
+            }
+            if (ci < ncb) S.off[ci + 1] = carry + v;
+            carry += __shfl_sync(0xffffffffu, v, 31);
+        }
+        if (lane == 0) S.off[0] = 0;
+    } else if (warp == 1) {  // destination rows -> concatenated destination offsets
+        int v = lane < ndr ? S.dr_cnt[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += t;
+        }
+        if (lane < ndr) S.dr_base[lane + 1] = v;
+        if (lane == 0) S.dr_base[0] = 0;
+    }
+    // the two runs of every row in the cell-sorted arrays: slabs before / after the wrap in x
+    const int kw = xs0 < 0 ? -xs0 : (xs0 + WX > nc0 ? nc0 - xs0 : WX);  // first slab past the wrap
+    for (int r = threadIdx.x; r < nrow; r += kPairThreads) {
+        S.row_gA[r] = S.cstart[r * WX];
+        S.row_gB[r] = kw < WX ? S.cstart[r * WX + kw] : 0;
+        const int yu = ry0 + r % WY, zu = rz0 + r / WY;
+        S.row_code[r] = (yu < 0 ? 0 : (yu >= nc1 ? 2 : 1)) | ((zu < 0 ? 0 : (zu >= nc2 ? 2 : 1)) << 2);
+    }
+    if (threadIdx.x == 0) {
+        const double hx = K.L[0] / nc0, h1 = K.L[1] / nc1, h2 = K.L[2] / nc2;
+        S.dc[0] = cx0 * G * hx;
+        S.dc[1] = cy0 * h1;
+        S.dc[2] = cz0 * h2;
+        S.dc[3] = xs0 < 0 ? -K.L[0] : 0.0;
+        S.dc[4] = xs0 < 0 ? 0.0 : K.L[0];
+        S.dc[5] = hx;
+        S.dc[6] = h1;
+        S.dc[7] = h2;
+        S.dc[8] = nc0 / K.L[0];
+    }
+    __syncthreads();
+    const int nd = S.dr_base[ndr];
+    if (nd == 0) return;  // uniform over the CTA
+    const float rc2s = (float)(K.rcut2 * (1.0 + kScreenMargin));
+    const float rc2 = (float)K.rcut2;
+    const float alpha = (float)K.alpha;
+    const int ntot = S.off[ncb];
+    const int W = 2 * M + 1;  // rows around a node's own cell in y and in z
+    const int ldy = lane % W - M, ldz = lane / W - M;  // the row offset lane l examines (l < W^2)
+    const double pref = K.Gamma / (4.0 * kPi);
+    unsigned ninr = 0, ncand = 0;  // warp-uniform (a CTA sees far fewer than 2^32 candidates)
+    for (int p0 = 0; p0 < nd; p0 += kF32MaxDst) {
+        const int np = nd - p0 < kF32MaxDst ? nd - p0 : kF32MaxDst;
+        // row parts per destination: at least 16 items per CTA where the block has few nodes
+        const int P = np >= 16 ? 1 : (16 + np - 1) / np;
+        const int nitems = np * P;
+        for (int T0 = 0, T1 = 0; T0 < ntot; T0 = T1) {
+            const int ra = min(last_row_le(S.off, WX, nrow, T0), nrow - 1);
+            const int rf = last_row_le(S.off, WX, nrow, T0 + kF32Tile);
+            T1 = S.off[rf * WX] > T0 ? S.off[rf * WX] : min(T0 + kF32Tile, ntot);
+            const int rb = min(last_row_le(S.off, WX, nrow, T1 - 1) + 1, nrow);
+            __syncthreads();  // previous tile consumed; previous pass written out
+            if (T0 == 0) {
+                for (int t = threadIdx.x; t < np; t += kPairThreads) {
+                    const int tt = p0 + t;
+                    int k = 0;
+                    while (k + 1 < ndr && S.dr_base[k + 1] <= tt) ++k;
+                    const int i = dst_order[S.dr_start[k] + tt - S.dr_base[k]];
+                    S.di[t] = i;
+                    const int by = cy1 - cy0;
+                    S.drow[t] = ((M + k / by) << 8) | (M + k % by);  // (z, y) row coordinates, 8 bits each
+                    S.dprev[t] = idx_prev[i];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) S.dx[t][d] = nodes[d * Np + i];
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) S.acc[t][c] = 0.0f;
+                }
+            }
+            // staging in units of 32 consecutive sources, kF32StageUnroll units per warp at a time
+            // (their loads in flight together)
+            const int nunits = (T1 - T0 + 31) >> 5;
+            for (int u0 = warp; u0 < nunits; u0 += (kPairThreads / 32) * kF32StageUnroll) {
+                int jj[kF32StageUnroll], tt[kF32StageUnroll], code[kF32StageUnroll];
+#pragma unroll
+                for (int q = 0; q < kF32StageUnroll; ++q) {
+                    const int u = u0 + q * (kPairThreads / 32);
+                    const int t = T0 + (u << 5) + lane;
+                    tt[q] = -1;
+                    jj[q] = 0;
+                    code[q] = 0;
+                    if (u < nunits && t < T1) {
+                        int r = last_row_le(S.off, WX, nrow, T0 + (u << 5));
+                        while (r + 1 < nrow && S.off[(r + 1) * WX] <= t) ++r;
+                        const int rowA = S.off[r * WX], offB = S.off[r * WX + kw];
+                        const bool inA = t < offB;
+                        jj[q] = inA ? S.row_gA[r] + (t - rowA) : S.row_gB[r] + (t - offB);
+                        tt[q] = t - T0;
+                        // periodic image codes: bit 0 segment B in x; bits 1-2 / 3-4: -L, 0, +L in y / z
+                        code[q] = (inA ? 0 : 1) | (S.row_code[r] << 1);
+                    }
+                }
+                double v[kF32StageUnroll][6];
+                int sgv[kF32StageUnroll];
+#pragma unroll
+                for (int q = 0; q < kF32StageUnroll; ++q) {
+                    const int j = jj[q];
+                    if (tt[q] >= 0) {
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) v[q][c] = src[c * Ns + j];
+                        sgv[q] = SKIP ? seg[j] : 0;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kF32StageUnroll; ++q) {
+                    if (tt[q] >= 0) {
+                        const int cd = code[q];
+                        const double u0d = v[q][0] + S.dc[3 + (cd & 1)] - S.dc[0];
+                        const double u1d = v[q][1] + (double)(((cd >> 1) & 3) - 1) * K.L[1] - S.dc[1];
+                        const double u2d = v[q][2] + (double)(((cd >> 3) & 3) - 1) * K.L[2] - S.dc[2];
+                        const float f0 = (float)u0d, f1 = (float)u1d, f2 = (float)u2d;
+                        S.P[tt[q]] = make_float4(f0, f1, f2, __int_as_float(sgv[q]));
+                        S.Q[tt[q]] = make_float4((float)(u0d - f0), (float)(u1d - f1), (float)(u2d - f2), (float)v[q][3]);
+                        S.R[tt[q]] = make_float2((float)v[q][4], (float)v[q][5]);
+                    }
+                }
+            }
+            __syncthreads();
+            for (int it = warp; it < nitems; it += kPairThreads / 32) {
+                const int dl = it % np, part = it / np;
+                const double x[3] = {S.dx[dl][0], S.dx[dl][1], S.dx[dl][2]};
+                // lane l examines the row (dy, dz) = (l % W - M, l / W - M) around the node's own cell
+                int a = 0, b = 0;
+                if (lane < W * W) {
+                    const int own = S.drow[dl];
+                    const int yr = (own & 255) + ldy, zr = (own >> 8) + ldz;
+                    if (yr >= 0 && yr < WY && zr >= 0 && zr < WZ) {
+                        const int r = zr * WY + yr;
+                        if (r >= ra && r < rb) {
+                            const double h1 = S.dc[6], h2 = S.dc[7], hx = S.dc[5], inv_hx = S.dc[8];
+                            const double gy = box_gap(x[1], (ry0 + yr) * h1, h1);
+                            const double gz = box_gap(x[2], (rz0 + zr) * h2, h2);
+                            const double gyz = gy * gy + gz * gz;
+                            if (gyz <= K.rcut2) {
+                                const double w = (double)sqrtf((float)(K.rcut2 - gyz)) * (1.0 + 1e-6) + 1e-9 * hx;
+                                int klo = (int)floor((x[0] - w) * inv_hx) - xs0;
+                                int khi = (int)floor((x[0] + w) * inv_hx) - xs0;
+                                klo = klo < 0 ? 0 : klo;
+                                khi = khi > WX - 1 ? WX - 1 : khi;
+                                if (klo <= khi) {
+                                    a = max(S.off[r * WX + klo], T0) - T0;
+                                    b = min(S.off[r * WX + khi + 1], T1) - T0;
+                                }
+                            }
+                        }
+                    }
+                }
+                unsigned rows = __ballot_sync(0xffffffffu, a < b);
+                float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                int qcount = 0;
+                int32_t* Qu = S.queue[warp];
+                const double xd0 = x[0] - S.dc[0], xd1 = x[1] - S.dc[1], xd2 = x[2] - S.dc[2];
+                const float3 xh = make_float3((float)xd0, (float)xd1, (float)xd2);
+                const float3 xl = make_float3((float)(xd0 - xh.x), (float)(xd1 - xh.y), (float)(xd2 - xh.z));
+                const int i = S.di[dl], iprev = S.dprev[dl];
+                for (int nrw = 0, next = part; rows; ++nrw, rows &= rows - 1) {
+                    if (nrw != next) continue;  // warp-uniform: rows are dealt to the parts in turn
+                    next += P;
+                    const int src_lane = __ffs(rows) - 1;
+                    const int ra_ = __shfl_sync(0xffffffffu, a, src_lane);
+                    const int rb_ = __shfl_sync(0xffffffffu, b, src_lane);
+                    ncand += rb_ - ra_;
+                    for (int base = ra_; base < rb_; base += 32) {
+                        const int t = base + lane;
+                        const float4 p = S.P[t];
+                        const float e0 = xh.x - p.x, e1 = xh.y - p.y, e2 = xh.z - p.z;
+                        const bool inr = t < rb_ && fmaf(e0, e0, fmaf(e1, e1, e2 * e2)) <= rc2s;
+                        const unsigned m = __ballot_sync(0xffffffffu, inr);
+                        if (inr) Qu[qcount + __popc(m & ((1u << lane) - 1u))] = t;
+                        qcount += __popc(m);
+                        __syncwarp();
+                        if (qcount >= 32 * kF32EvalU) {
+                            int tq[kF32EvalU];
+                            bool vq[kF32EvalU];
+#pragma unroll
+                            for (int u = 0; u < kF32EvalU; ++u) {
+                                tq[u] = Qu[32 * u + lane];
+                                vq[u] = true;
+                            }
+                            f32_eval<VEL, PSI, SKIP, kF32EvalU>(K, S, xh, xl, rc2, alpha, nf, i, iprev, tq, vq, acc, ninr);
+                            __syncwarp();
+                            if (lane < qcount - 32 * kF32EvalU) Qu[lane] = Qu[32 * kF32EvalU + lane];
+                            __syncwarp();
+                            qcount -= 32 * kF32EvalU;
+                        }
+                    }
+                }
+                for (int q0 = 0; q0 < qcount; q0 += 32) {  // warp-uniform remainder, one pair per lane
+                    const int tq[1] = {q0 + lane < qcount ? Qu[q0 + lane] : Qu[0]};
+                    const bool vq[1] = {q0 + lane < qcount};
+                    f32_eval<VEL, PSI, SKIP, 1>(K, S, xh, xl, rc2, alpha, nf, i, iprev, tq, vq, acc, ninr);
+                }
+                __syncwarp();  // the queue is reused by the warp's next item
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    if ((c < 3 && !VEL) || (c >= 3 && !PSI)) continue;
+                    float v = acc[c];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    acc[c] = v;
+                }
+                if (lane == 0) {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c)
+                        if ((c < 3 && VEL) || (c >= 3 && PSI)) atomicAdd(&S.acc[dl][c], acc[c]);
+                }
+            }
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < np; t += kPairThreads) {
+            const int64_t i = S.di[t];
+            if (VEL) {
+                vel[i] += pref * (double)S.acc[t][0];
+                vel[Np + i] += pref * (double)S.acc[t][1];
+                vel[2 * Np + i] += pref * (double)S.acc[t][2];
+            }
+            if (PSI) {
+                psi[i] += pref * (double)S.acc[t][3];
+                psi[Np + i] += pref * (double)S.acc[t][4];
+                psi[2 * Np + i] += pref * (double)S.acc[t][5];
+            }
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&counters[0], (unsigned long long)ninr);
+        atomicAdd(&counters[1], (unsigned long long)ncand);
+    }
+}
+
 // Local term (overwrites nothing: adds into the zeroed outputs), self-interaction removal
 // and, when lia_segment_fraction is set, the local integrals over the excluded sub-segments.
 __global__ void __launch_bounds__(128) local_self_kernel(
@@ -746,7 +1177,7 @@ __global__ void __launch_bounds__(128) local_self_kernel(
     const double* __restrict__ nodes, const int32_t* __restrict__ idx_prev, const double* __restrict__ d1,
     const double* __restrict__ d2, const double* __restrict__ dm, const double* __restrict__ dp,
     const double* __restrict__ points, const double* __restrict__ charges, const double* __restrict__ li_vel,
-    const double* __restrict__ li_psi, double* __restrict__ vel, double* __restrict__ psi) {
+    const double* __restrict__ li_psi, double* __restrict__ vel, double* __restrict__ psi, double3 psi_bg) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= Np) return;
     const bool want_v = fields & VPBS_VELOCITY, want_p = fields & VPBS_STREAMFUNCTION;
@@ -823,8 +1254,13 @@ __global__ void __launch_bounds__(128) local_self_kernel(
     }
     if (want_v)
         for (int d = 0; d < 3; ++d) vel[d * Np + i] += v[d];
-    if (want_p)
+    if (want_p) {
+        // streamfunction of the uniform background vorticity of unclosed filaments (zero otherwise)
+        p[0] += psi_bg.x;
+        p[1] += psi_bg.y;
+        p[2] += psi_bg.z;
         for (int d = 0; d < 3; ++d) psi[d * Np + i] += p[d];
+    }
 }
 
 }  // namespace
@@ -915,6 +1351,72 @@ void ewald_table_host(double xmax, int* ntab, double* tab) {
     }
 }
 
+void table_eval_host(const double* tab, int ntab, double x, double* a, double* g) {
+    int k = (int)(x * kEwaldInvH);
+    k = k < ntab ? (k < 0 ? 0 : k) : ntab - 1;
+    const double t = x - (k + 0.5) * kEwaldH;
+    const double* ce = tab + (size_t)k * kEwaldNC;
+    const double* cg = tab + (size_t)(ntab + k) * kEwaldNC;
+    double va = ce[kEwaldNC - 1], vg = cg[kEwaldNC - 1];
+    for (int m = kEwaldNC - 2; m >= 0; --m) {
+        va = std::fma(va, t, ce[m]);
+        vg = std::fma(vg, t, cg[m]);
+    }
+    *a = va;
+    *g = vg;
+}
+
+int f32_table_size(double xmax) { return (int)std::floor(xmax * kTabCInvH) + 2; }
+
+// Cubic interpolants of both weights on every interval [k/32, (k+1)/32], through the values of
+// the FP64 table at the 4 Chebyshev points of the interval, in powers of t = 32 x - k (t in
+// [0, 1]).  Over [0, xmax] they agree with the FP64 weights to ~3e-8 absolute (the FP32
+// rounding of the coefficients), for the Gaussian and the Kaiser-Bessel weights alike.
+void f32_table_host(const double* tab, int ntab, double xmax, float4* out) {
+    const int nf = f32_table_size(xmax);
+    for (int k = 0; k < nf; ++k) {
+        double T[4], Va[4], Vg[4];
+        for (int j = 0; j < 4; ++j) {
+            T[j] = 0.5 + 0.5 * std::cos((2 * j + 1) * kPi / 8.0);
+            table_eval_host(tab, ntab, (k + T[j]) / (double)kTabCInvH, &Va[j], &Vg[j]);
+        }
+        for (int w = 0; w < 2; ++w) {
+            // solve the 4x4 Vandermonde system sum_n c_n T_j^n = V_j (Gaussian elimination, pivoting)
+            double A[4][5];
+            for (int j = 0; j < 4; ++j) {
+                double p = 1.0;
+                for (int n = 0; n < 4; ++n, p *= T[j]) A[j][n] = p;
+                A[j][4] = w == 0 ? Va[j] : Vg[j];
+            }
+            for (int c = 0; c < 4; ++c) {
+                int piv = c;
+                for (int r = c + 1; r < 4; ++r)
+                    if (std::fabs(A[r][c]) > std::fabs(A[piv][c])) piv = r;
+                for (int n = 0; n < 5; ++n) std::swap(A[c][n], A[piv][n]);
+                for (int r = c + 1; r < 4; ++r) {
+                    const double f = A[r][c] / A[c][c];
+                    for (int n = c; n < 5; ++n) A[r][n] -= f * A[c][n];
+                }
+            }
+            double cf[4];
+            for (int c = 3; c >= 0; --c) {
+                double v = A[c][4];
+                for (int n = c + 1; n < 4; ++n) v -= A[c][n] * cf[n];
+                cf[c] = v / A[c][c];
+            }
+            out[(size_t)w * nf + k] = make_float4((float)cf[0], (float)cf[1], (float)cf[2], (float)cf[3]);
+        }
+    }
+}
+
+void f32_table_eval_host(const float4* tabc, int nf, float x, float* a, float* g) {
+    int k;
+    float t;
+    f32_table_pos(x, nf, &k, &t);
+    *a = f32_cubic(tabc[k], t);
+    *g = f32_cubic(tabc[nf + k], t);
+}
+
 int exclusive_scan(vpbs_handle* h, const int32_t* counts, int32_t* start, int64_t n, DevBuf& tmp) {
     const int64_t nblk = (n + kScanChunk - 1) / kScanChunk;
     if (nblk <= 1) {
@@ -977,6 +1479,50 @@ int pair_interactions(vpbs_handle* h, int fields) {
             return w <= ncc && w <= cg.nc[1] && w <= cg.nc[2] && w * w <= kMaxRows && w * w * w * cg.G <= kMaxNbCells &&
                    nb * nb <= kMaxBlockRows;
         };
+        const bool mixed = h->P.precision == VPBS_PRECISION_MIXED;
+        const int nrow_max = kF32MaxRows, ncb_max = kF32MaxNb;
+        auto fits_f32 = [&](int b) {
+            const int w = b + 2 * cg.M;
+            return fits(b) && w * w <= nrow_max && w * w * w * cg.G <= ncb_max;
+        };
+        if (mixed && h->K.ewald_ntab > 0 && h->K.ntab_c > 0 && h->K.ntab_c <= kF32TabMax && fits_f32(1)) {
+            // FP32 kernel: blocks grown while they hold at most ~96 nodes on average (one pass of
+            // destinations) and at least 2 CTAs per SM remain; a neighbourhood of two tiles costs less
+            // than a block of few nodes (1M-node tangle at r_cut = L/45: 2 x 2 x 2 cells per CTA, two
+            // tiles, 2.8 ms; one cell, one tile, 4.2 ms)
+            int Bc = 1;
+            if (h->pair_block > 0 && fits_f32(h->pair_block)) {
+                Bc = h->pair_block;  // chosen by vpbs_autotune
+            } else {
+                while (fits_f32(Bc + 1) && (Bc + 1) * (Bc + 1) * (Bc + 1) * per_cell <= 96.0 &&
+                       ncoarse / ((double)(Bc + 1) * (Bc + 1) * (Bc + 1)) >= 2.0 * nsm)
+                    ++Bc;
+            }
+            const int3 bk = make_int3(Bc, Bc, Bc);
+            const int3 nb = make_int3((ncc + Bc - 1) / Bc, (cg.nc[1] + Bc - 1) / Bc, (cg.nc[2] + Bc - 1) / Bc);
+            const size_t smem = sizeof(F32Smem);
+            const unsigned nblocks = (unsigned)((int64_t)nb.x * nb.y * nb.z);
+            auto launch_f32 = [&](auto kern) {
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+                kern<<<nblocks, kPairThreads, smem, h->stream>>>(
+                    h->K, h->cg, Np, Nq, (const int32_t*)h->dst_start.p, (const int32_t*)h->dst_order.p,
+                    (const double*)h->nodes.p, (const int32_t*)h->idx_prev.p, (const double*)h->src_sorted.p,
+                    (const int32_t*)h->src_start.p, (const int32_t*)h->src_seg.p, (double*)h->vel.p, (double*)h->psi.p,
+                    (unsigned long long*)h->counters.p, bk, nb);
+            };
+            if (skip_local) {
+                if (v && p) launch_f32(pair_f32_kernel<true, true, true>);
+                else if (v) launch_f32(pair_f32_kernel<true, false, true>);
+                else launch_f32(pair_f32_kernel<false, true, true>);
+            } else {
+                if (v && p) launch_f32(pair_f32_kernel<true, true, false>);
+                else if (v) launch_f32(pair_f32_kernel<true, false, false>);
+                else launch_f32(pair_f32_kernel<false, true, false>);
+            }
+            h->launches++;
+            return check_cuda(h, cudaGetLastError(), "FP32 pair kernel");
+        }
         int Bc = 1;
         if (h->pair_block > 0 && fits(h->pair_block)) {
             Bc = h->pair_block;  // chosen by vpbs_autotune
@@ -1004,7 +1550,6 @@ int pair_interactions(vpbs_handle* h, int fields) {
             else if (v) launch_tiled(pair_cell_kernel<true, false, SK, R>);
             else launch_tiled(pair_cell_kernel<false, true, SK, R>);
         };
-        const bool mixed = h->P.precision == VPBS_PRECISION_MIXED;
         if (skip_local) {
             if (mixed) by_fields(std::true_type{}, PrecTag<float>{});
             else by_fields(std::true_type{}, PrecTag<double>{});
@@ -1047,12 +1592,31 @@ int local_and_self(vpbs_handle* h, int fields, int lia_mode, int with_pairs_self
     const int do_local = (lia_mode == VPBS_LIA_TRUE || lia_mode == VPBS_LIA_ONLY) ? 1 : 0;
     const int do_self = with_pairs_self ? 1 : 0;
     const int do_li = (with_pairs_self && K.lia_fraction > 0) ? 1 : 0;
+    // background_vorticity_correction! (BiotSavart.jl:255-286), applied with the short range: unclosed
+    // filaments whose end-to-end offsets add up to p carry a mean vorticity p Gamma / V, which the
+    // long range removes (k = 0 mode); the short-range streamfunction gets that of the compensating
+    // uniform background, -(p Gamma / V) C
+    double3 bg = make_double3(0.0, 0.0, 0.0);
+    if (with_pairs_self && h->have_fil_offsets && !K.open_domain) {
+        const double* p = h->offset_sum;
+        double dn = 0.0, na = 0.0, nb = 0.0;
+        for (int d = 0; d < 3; ++d) {
+            dn += p[d] * p[d];
+            na += (p[d] + K.L[d]) * (p[d] + K.L[d]);
+            nb += K.L[d] * K.L[d];
+        }
+        // isapprox(p + Ls, Ls) (default rtol sqrt(eps)): no mean vorticity
+        if (std::sqrt(dn) > std::sqrt(2.220446049250313e-16) * std::fmax(std::sqrt(na), std::sqrt(nb))) {
+            const double f = -(K.Gamma / (K.L[0] * K.L[1] * K.L[2])) * h->bg_factor;
+            bg = make_double3(f * p[0], f * p[1], f * p[2]);
+        }
+    }
     StageScope st(h, ST_LOCAL_SELF);
     local_self_kernel<<<grid_for(h->Np, 128), 128, 0, h->stream>>>(
         K, h->Np, fields, do_local, do_self, do_li, rv, rpsi, (const double*)h->nodes.p, (const int32_t*)h->idx_prev.p,
         (const double*)h->d1.p, (const double*)h->d2.p, (const double*)h->dm.p, (const double*)h->dp.p,
         (const double*)h->points.p, (const double*)h->charges.p, (const double*)h->li_vel.p,
-        (const double*)h->li_psi.p, (double*)h->vel.p, (double*)h->psi.p);
+        (const double*)h->li_psi.p, (double*)h->vel.p, (double*)h->psi.p, bg);
     h->launches++;
     return check_cuda(h, cudaGetLastError(), "local term kernel");
 }

@@ -224,4 +224,10 @@ int vpbs_autotune(vpbs_handle* h, int32_t* chosen) {
     return rc;
 }
 
+int vpbs_pair_block(vpbs_handle* h, int32_t cells) {
+    if (!h || cells < 0 || cells > 8) return VPBS_ERR_ARG;
+    h->pair_block = cells;
+    return 0;
+}
+
 }  // extern "C"

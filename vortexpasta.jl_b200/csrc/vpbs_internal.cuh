@@ -33,6 +33,10 @@ struct KParams {
     const float* ewald_tab_f;  // FP32 copy (first kEwaldNCf coefficients) for the mixed form
     const double2* ewald_tab2; // interleaved (erfc, g) coefficient pairs, for both weights at once
     int ewald_ntab;       // number of intervals (0: no splitting, weights are 1)
+    // FP32 cubic tables of the mixed form's pair kernel: intervals of width 1/32 in x, one float4
+    // (c0, c1, c2, c3) in powers of t = 32 x - k per interval k; weight a then weight g
+    const float4* tab_c;
+    int ntab_c;
 };
 
 // Ewald weight tables: intervals of width 1/16 in x = alpha r, degree-9 Taylor polynomials
@@ -43,6 +47,17 @@ constexpr double kEwaldInvH = 16.0;
 constexpr double kEwaldH = 1.0 / 16.0;
 void ewald_table_host(double xmax, int* ntab, double* tab);  // tab: 2 * ntab * kEwaldNC doubles
 int ewald_table_size(double xmax);
+// Both weights from a table in the layout of ewald_table_host (host evaluation, FP64).
+void table_eval_host(const double* tab, int ntab, double x, double* a, double* g);
+// FP32 cubic tables fitted to an FP64 table over [0, xmax] (layout of KParams::tab_c): nf intervals.
+constexpr float kTabCInvH = 32.0f;
+int f32_table_size(double xmax);
+void f32_table_host(const double* tab, int ntab, double xmax, float4* out);  // out: 2 * f32_table_size(xmax)
+// Device-identical host evaluation of the FP32 cubic tables (same float operations).
+void f32_table_eval_host(const float4* tabc, int nf, float x, float* a, float* g);
+
+// Gauss-Legendre rule on [-1, 1] (host; longrange.cu).
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w);
 
 // Kaiser-Bessel splitting (splitting.cu): the reference's truncated Chebyshev series of the kernel
 // f and of its integral F (full coefficient vectors in u = r / rcut), and their weight tables in
@@ -122,6 +137,12 @@ struct vpbs_handle {
 
     // geometry inputs / scratch
     vpbs::DevBuf nodes_in, offsets, fil_of_node, knots, coefs, dcoef1, dcoef2, spline_scratch;
+    // end-to-end offsets of unclosed (infinite) filaments, [nfil][3] (closed_filament.jl:118-132)
+    vpbs::DevBuf fil_off;
+    bool have_fil_offsets = false;
+    double offset_sum[3] = {0.0, 0.0, 0.0};  // sum over the filaments (background vorticity)
+    int64_t nfil_off = 0;                     // filament count the offsets were given for
+    double bg_factor = 0.0;  // streamfunction of a unit uniform vorticity (background_vorticity_correction_factor)
 
     // point data (SoA; 3 consecutive blocks of Np or Nq doubles for vectors)
     vpbs::DevBuf nodes, idx_prev, d1, d2, dm, dp, points, charges;

@@ -90,6 +90,38 @@ def random_tangle(nrings: int, nodes_per_ring: int, L: float = 2 * np.pi, rmin: 
     return out
 
 
+class InfiniteFilament(np.ndarray):
+    """Nodes of an infinite, unclosed filament that repeats itself periodically: node i + N sits at
+    node i + `offset` (the end-to-end offset of ``ClosedFilament``, src/Filaments/closed_filament.jl:
+    118-132, 196-207).  An (N, 3) float64 array with an ``offset`` attribute."""
+
+    def __new__(cls, nodes, offset):
+        obj = np.ascontiguousarray(nodes, dtype=np.float64).view(cls)
+        obj.offset = np.asarray(offset, dtype=np.float64).reshape(3).copy()
+        return obj
+
+    def __array_finalize__(self, obj):
+        self.offset = getattr(obj, "offset", np.zeros(3))
+
+
+def end_to_end_offset(f) -> np.ndarray:
+    """end_to_end_offset(f): zero for a closed filament (closed_filament.jl:196-207)."""
+    return np.asarray(getattr(f, "offset", np.zeros(3)), dtype=np.float64).reshape(3)
+
+
+def periodic_line(n: int, L: float, x: float = 0.0, y: float = 0.0, r=None, sign: int = 1,
+                  translate=(0.0, 0.0, 0.0)) -> InfiniteFilament:
+    """``PeriodicLine`` of src/PredefinedCurves/periodic_line.jl scaled by L (``define_curve(p; scale = L,
+    translate, orientation = sign)``): S(t) = translate + L (x + Re r(t), y + Im r(t), t - 1/2), nodes at
+    t_j = (2j - 1) / (2N) (orientation -1 reverses t), end-to-end offset (0, 0, sign L).  `r` is a
+    1-periodic complex function (None: straight line)."""
+    t = node_parameters(n)
+    tau = t if sign > 0 else 1.0 - t
+    rr = np.zeros(n, dtype=complex) if r is None else np.asarray([r(v) for v in tau], dtype=complex)
+    X = np.stack([x + rr.real, y + rr.imag, tau - 0.5], axis=1) * L + np.asarray(translate, dtype=np.float64)
+    return InfiniteFilament(X, (0.0, 0.0, sign * L))
+
+
 def concat(filaments) -> tuple[np.ndarray, np.ndarray]:
     """Pack a list of filaments into (AoS nodes [Np, 3], offsets [nfil + 1] int64)."""
     counts = np.array([len(f) for f in filaments], dtype=np.int64)
