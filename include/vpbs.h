@@ -340,6 +340,11 @@ const char* vpbs_ensemble_last_error(void);
  * Synchronous. */
 int vpbs_autotune(vpbs_handle* h, int32_t* chosen);
 
+/* Spreading kernels of the FP32 (mixed) form for NUFFT half-supports m <= 4 on grids of 16^3 bricks:
+ * mode 0 (default) multiplies each brick on the tensor cores (tcgen05, 3xTF32); mode 1 uses the CUDA
+ * cores only (plane-owner kernel).  Tuning and testing support; no counterpart in the reference. */
+int vpbs_spread_mode(vpbs_handle* h, int32_t mode);
+
 /* Sets the pair kernel's cells per CTA edge for later evaluations (0: the built-in rule; an edge
  * whose neighbourhood does not fit the kernel's tables falls back to the rule), as vpbs_autotune
  * does with its choice.  Tuning support; no counterpart in the reference. */

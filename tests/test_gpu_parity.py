@@ -280,3 +280,30 @@ def test_host_entry_points_agree(vp):
         c.close()
     assert np.abs(v_flat - v_list).max() <= 1e-13 * np.abs(v_list).max()
     assert np.abs(v_ptr - v_list).max() <= 1e-13 * np.abs(v_list).max()
+
+
+@pytest.mark.parametrize("sigma,m", [(1.5, 3), (1.5, 4), (2.0, 2), (1.25, 3)])
+def test_tensor_core_spreading(vp, oracle, built_lib, sigma, m):
+    """Mixed form: the tensor-core brick product (tcgen05, 3xTF32) against the CUDA-core plane
+    kernel and the oracle -- vorticity coefficients (the spread grid after the forward FFT) and
+    velocities."""
+    from vortexpasta_b200 import _lib
+    fs, p = vp.configs.tangle20k(precision="mixed")
+    fs = fs[:40]
+    p = p.with_(backend_long=vp.NonuniformFFTsBackend(sigma, m))
+    assert _lib.load().vpbs_fft_size(p.splitting.Ns[0], sigma) % 16 == 0  # brick spreading applies
+    out = {}
+    for mode in (0, 1):
+        c = vp.init_cache(p)
+        try:
+            _lib.check(c._lib.vpbs_spread_mode(c.handle, mode), c.handle, "spread_mode")
+            vs = [np.zeros_like(f) for f in fs]
+            vp.compute_on_nodes_({"velocity": vs}, c, fs)
+            out[mode] = (np.concatenate(vs), np.stack(vp.get_longrange_field_fourier(c)["field"]))
+        finally:
+            c.close()
+    (v_tc, u_tc), (v_cc, u_cc) = out[0], out[1]
+    assert rel(v_tc, v_cc) < 1e-6
+    vo, _, _ = oracle.compute_on_nodes(p, fs)
+    assert rel(v_tc, vo) < MIXED_TOL
+    assert np.linalg.norm(u_tc - u_cc) / np.linalg.norm(u_cc) < 1e-6

@@ -77,6 +77,33 @@ int ensure_pinned(vpbs_handle* h, void** buf, size_t* cap, size_t bytes) {
     return 0;
 }
 
+int ensure_status(vpbs_handle* h) {
+    if (h->status_host) return 0;
+    void* p = nullptr;
+    cudaError_t e = cudaHostAlloc(&p, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e != cudaSuccess) return set_error(h, VPBS_ERR_OOM, std::string("mapped status word: ") + cudaGetErrorString(e));
+    *(volatile int*)p = 0;
+    void* d = nullptr;
+    e = cudaHostGetDevicePointer(&d, p, 0);
+    if (e != cudaSuccess) {
+        cudaFreeHost(p);
+        return set_error(h, VPBS_ERR_CUDA, std::string("mapped status word: ") + cudaGetErrorString(e));
+    }
+    h->status_host = (int*)p;
+    h->status_dev = (int*)d;
+    return 0;
+}
+
+int check_status(vpbs_handle* h) {
+    if (h->status_host && *(volatile int*)h->status_host) {
+        *(volatile int*)h->status_host = 0;
+        return set_error(h, VPBS_ERR_TIMEOUT,
+                         "a bounded device-side wait gave up (tensor-core spreading); the results of that evaluation are "
+                         "not valid");
+    }
+    return 0;
+}
+
 static void free_buf(DevBuf& b) {
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
@@ -318,9 +345,10 @@ int vpbs_destroy(vpbs_handle* h) {
                       &h->src_seg, &h->dst_cell, &h->dst_start, &h->dst_fill, &h->dst_order, &h->counters,
                       &h->grid_r, &h->grid_c, &h->grid_c2, &h->uhat, &h->decx, &h->decy, &h->decz, &h->nodes_lr,
                       &h->vel, &h->psi, &h->spread_bin, &h->spread_counts, &h->spread_start, &h->binned,
-                      &h->spread_foot, &h->ewald_tab, &h->scan_tmp, &h->scan_tmp_lr, &h->rk_vs, &h->rk_tmp};
+                      &h->spread_foot, &h->tc_counts, &h->tc_start, &h->tc_rec, &h->ewald_tab, &h->scan_tmp, &h->scan_tmp_lr, &h->rk_vs, &h->rk_tmp};
     for (DevBuf* b : bufs) free_buf(*b);
     if (h->pin_in) cudaFreeHost(h->pin_in);
+    if (h->status_host) cudaFreeHost(h->status_host);
     if (h->pin_out) cudaFreeHost(h->pin_out);
     if (h->h2d_done) cudaEventDestroy(h->h2d_done);
     if (h->aux_stream) cudaStreamSynchronize(h->aux_stream);
@@ -649,6 +677,7 @@ static int fetch_soa(vpbs_handle* h, int32_t field, const double** out) {
     const void* src = field == VPBS_VELOCITY ? h->vel.p : h->psi.p;
     if ((rc = check_cuda(h, cudaMemcpyAsync(h->pin_out, src, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H"))) return rc;
     if ((rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync"))) return rc;
+    if ((rc = check_status(h))) return rc;
     *out = (const double*)h->pin_out;
     return 0;
 }
@@ -670,6 +699,7 @@ static int fetch_aos(vpbs_handle* h, int32_t field, const double** out) {
     if ((rc = check_cuda(h, cudaMemcpyAsync(h->pin_out, h->aos_out.p, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H")))
         return rc;
     if ((rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync"))) return rc;
+    if ((rc = check_status(h))) return rc;
     *out = (const double*)h->pin_out;
     return 0;
 }
@@ -783,7 +813,8 @@ int vpbs_get_uhat(vpbs_handle* h, double* out, int64_t n_doubles) {
     if ((rc = activate(h))) return rc;
     if ((rc = check_cuda(h, cudaMemcpyAsync(out, h->uhat.p, sizeof(double) * n_doubles, cudaMemcpyDeviceToHost, h->stream), "D2H uhat")))
         return rc;
-    return check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync");
+    if ((rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync"))) return rc;
+    return check_status(h);
 }
 
 int vpbs_pair_counts(vpbs_handle* h, int64_t* in_range, int64_t* candidates) {
@@ -873,6 +904,7 @@ int vpbs_stage_times(vpbs_handle* h, double* ms, int32_t n) {
     int rc;
     if ((rc = activate(h))) return rc;
     if ((rc = check_cuda(h, cudaStreamSynchronize(h->stream), "stream sync"))) return rc;
+    if ((rc = check_status(h))) return rc;
     for (int s = 0; s < ST_COUNT; ++s) {
         double acc = 0.0;
         for (int k = 0; k < h->tcount[s] && k < 4; ++k) {
@@ -940,6 +972,12 @@ extern "C" int vpbs_fma_throughput(int32_t device, int32_t fp64, double* tflops)
     cudaFree(out);
     if (err != cudaSuccess) return set_error(nullptr, VPBS_ERR_CUDA, cudaGetErrorString(err));
     *tflops = best;
+    return 0;
+}
+
+extern "C" int vpbs_spread_mode(vpbs_handle* h, int32_t mode) {
+    if (!h || mode < 0 || mode > 1) return VPBS_ERR_ARG;
+    h->spread_mode = mode;
     return 0;
 }
 

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "vpbs_internal.cuh"
+#include "tc_sm100.cuh"
 
 namespace vpbs {
 
@@ -245,7 +246,7 @@ __global__ void spread_bin_count_kernel(LRSizes S, int B, int nb0, int nb1, int 
     const int b2 = footprint_start(src[2 * Nq + j], sx2, S.n[2], S.m) / B;
     const int32_t b = (b2 * nb1 + b1) * nb0 + b0;
     bin[j] = b;
-    rank[j] = atomicAdd(&counts[b], 1);
+    rank[j] = warp_aggregated_rank(counts, b);
 }
 
 // Scatter the points into bin order, with everything the brick kernel needs per point: the
@@ -527,6 +528,332 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) spread_plane_kernel(
         grid[c * ng + ((int64_t)(bs[2] + zz) * S.n[1] + (bs[1] + y)) * S.n[0] + bs[0] + x] =
             ptile[c * Lay::TC + zz * Lay::PL + y * Lay::RX + x];
     }
+}
+
+// ---- Tensor-core spreading (FP32 grids, NUFFT half-support m <= 4, bricks of 16^3) ----
+// The spread onto one brick is a dense product over the points p whose footprint meets it:
+//   grid[c][z][y][x] = sum_p (q_pc phi_z,p(z)) (phi_y,p(y) phi_x,p(x)),
+// i.e. D[(y, x), (c, z)] = sum_p A[(y, x), p] B[(c, z), p] with M = 256 rows in two halves of 128
+// (y < 8, y >= 8), N = 48 columns and K = the points, 16 per batch.  A pre-pass writes one record
+// per (point, brick) pair, grouped by brick: charges, the footprint corner relative to the brick and
+// the kernel values (computed once per point).  The brick's kernel streams its records into shared
+// memory with bulk copies (double-buffered), builds the operands there (K-major core matrices of 8
+// rows x 4 values; A holds only the current footprints, cleared again before reuse) and multiplies
+// them with tcgen05.mma kind::tf32 into two FP32 accumulators in tensor memory.  Each operand is split
+// into TF32 hi + lo parts and D accumulates hi*hi + hi*lo + lo*hi (3xTF32: FP32 accuracy, ~1e-7
+// relative).  Operand buffers are double-buffered: the tensor cores multiply batch b while the threads
+// build batch b + 1; mbarriers signalled by tcgen05.commit guard their reuse.  The brick's cells are
+// then read from tensor memory and written once (no atomics).  Every wait is bounded: on a timeout the
+// kernel records it in *status, stops issuing, and releases its tensor memory.
+constexpr int kTcThreads = 256;
+constexpr int kTcKB = 16;    // points per batch: two K-steps of 8
+constexpr int kTcChunk = 128;  // records per bulk copy
+constexpr int kTcRecMax = 28;  // floats per record for w <= 8
+constexpr uint32_t kTcWaitLimit = 1u << 26;
+
+// floats per record: charges (3), packed corner (1), 3 kernel rows of w values, padded to 16 bytes
+__host__ __device__ constexpr int tc_record_floats(int w) { return (4 + 3 * w + 3) & ~3; }
+
+__device__ __forceinline__ void tc_point_bricks(const LRSizes& S, const int f[3], int w, int b0[3], int two[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        b0[d] = f[d] >> 4;
+        two[d] = (f[d] & 15) + w > 16;
+    }
+}
+
+// Records per brick (counting pass): every brick a point's footprint meets.
+__global__ void tc_rec_count_kernel(LRSizes S, int nb0, int nb1, int nb2, int64_t Nq, const double* __restrict__ src,
+                                    double sx0, double sx1, double sx2, int32_t* __restrict__ counts) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= Nq) return;
+    const int w = 2 * S.m;
+    const int f[3] = {footprint_start(src[j], sx0, S.n[0], S.m), footprint_start(src[Nq + j], sx1, S.n[1], S.m),
+                      footprint_start(src[2 * Nq + j], sx2, S.n[2], S.m)};
+    int b0[3], two[3];
+    tc_point_bricks(S, f, w, b0, two);
+    const int nbv[3] = {nb0, nb1, nb2};
+    for (int e = 0; e < 8; ++e) {
+        const int ex = e & 1, ey = (e >> 1) & 1, ez = e >> 2;
+        if ((ex && !two[0]) || (ey && !two[1]) || (ez && !two[2])) continue;
+        const int bx = (b0[0] + ex) % nbv[0], by = (b0[1] + ey) % nbv[1], bz = (b0[2] + ez) % nbv[2];
+        warp_aggregated_rank(counts, (bz * nb1 + by) * nb0 + bx);
+    }
+}
+
+// The records: position start[brick] + rank (ranks from a second aggregated count into `fill`).
+__global__ void tc_rec_scatter_kernel(LRSizes S, int nb0, int nb1, int nb2, int64_t Nq, const double* __restrict__ src,
+                                      double sx0, double sx1, double sx2, const int32_t* __restrict__ start,
+                                      int32_t* __restrict__ fill, float* __restrict__ rec) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= Nq) return;
+    const int w = 2 * S.m;
+    const int R = tc_record_floats(w);
+    const double scale[3] = {sx0, sx1, sx2};
+    int f[3];
+    float phi[3][8];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double xh = (src[d * Nq + j] * scale[d]) / (2.0 * kPi / S.n[d]);
+        const int i0 = (int)floor(xh) - S.m + 1;
+        f[d] = wrapi(i0, S.n[d]);
+#pragma unroll
+        for (int s = 0; s < 8; ++s) phi[d][s] = s < w ? (float)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge) : 0.0f;
+    }
+    const float q[3] = {(float)src[3 * Nq + j], (float)src[4 * Nq + j], (float)src[5 * Nq + j]};
+    int b0[3], two[3];
+    tc_point_bricks(S, f, w, b0, two);
+    const int nbv[3] = {nb0, nb1, nb2};
+    for (int e = 0; e < 8; ++e) {
+        const int ex = e & 1, ey = (e >> 1) & 1, ez = e >> 2;
+        if ((ex && !two[0]) || (ey && !two[1]) || (ez && !two[2])) continue;
+        const int bx = (b0[0] + ex) % nbv[0], by = (b0[1] + ey) % nbv[1], bz = (b0[2] + ez) % nbv[2];
+        const int32_t b = (bz * nb1 + by) * nb0 + bx;
+        const int64_t pos = (int64_t)start[b] + warp_aggregated_rank(fill, b);
+        float* r = rec + pos * R;
+        // corner relative to the brick, biased by 64 into one byte per dimension
+        const int ox = (f[0] & 15) - 16 * ex, oy = (f[1] & 15) - 16 * ey, oz = (f[2] & 15) - 16 * ez;
+        r[0] = q[0];
+        r[1] = q[1];
+        r[2] = q[2];
+        r[3] = __int_as_float((ox + 64) | ((oy + 64) << 8) | ((oz + 64) << 16));
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int s = 0; s < 8; ++s)
+                if (s < w) r[4 + d * w + s] = phi[d][s];
+        for (int k = 4 + 3 * w; k < R; ++k) r[k] = 0.0f;
+    }
+}
+
+struct TcSpreadSmem {
+    // operands [stage][hi, lo]([half]), K-major core matrices [row / 8][k / 4][8][4]; A is zero outside
+    // the footprints of the batch it holds (entries are cleared again before the stage is reused)
+    float A[2][2][2][128 * kTcKB];
+    float B[2][2][48 * kTcKB];
+    float pts[2][kTcChunk * kTcRecMax];  // records of the current and the next chunk
+    int16_t held[2][kTcKB][2];           // (x, y) corner of the footprint each stage's A holds per slot (64: none)
+    int fail;
+    uint64_t mbar[2];    // multiplications of each operand stage done
+    uint64_t cpbar[2];   // bulk copy of each record buffer done
+    uint32_t tslot;
+};
+
+__global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int nb0, int nb1,
+                                                                  const int32_t* __restrict__ rec_start,
+                                                                  const float* __restrict__ rec, float* __restrict__ grid,
+                                                                  int* __restrict__ status) {
+    extern __shared__ __align__(128) unsigned char tc_raw[];
+    TcSpreadSmem& T = *reinterpret_cast<TcSpreadSmem*>(tc_raw);
+    constexpr int B16 = 16;
+    const int w = 2 * S.m;
+    const int R = tc_record_floats(w);
+    const int bx = blockIdx.x % nb0;
+    const int by = (blockIdx.x / nb0) % nb1;
+    const int bz = blockIdx.x / (nb0 * nb1);
+    const int bs[3] = {bx * B16, by * B16, bz * B16};
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int rs = rec_start[blockIdx.x], nrec = rec_start[blockIdx.x + 1] - rs;
+    const int nch = (nrec + kTcChunk - 1) / kTcChunk;
+    int cp_issued = 0;  // bulk copies issued (thread 0)
+    if (tid == 0) {
+        tc::mbar_init(&T.mbar[0], 1);
+        tc::mbar_init(&T.mbar[1], 1);
+        tc::mbar_init(&T.cpbar[0], 1);
+        tc::mbar_init(&T.cpbar[1], 1);
+        tc::fence_mbar_init();
+        T.fail = 0;
+        if (nch > 0) {
+            const int n0 = nrec < kTcChunk ? nrec : kTcChunk;
+            tc::bulk_g2s(T.pts[0], rec + (int64_t)rs * R, (uint32_t)(n0 * R * 4), &T.cpbar[0]);
+            cp_issued = 1;
+        }
+    }
+    {  // zero operands A (float4 stores)
+        float4* a4 = reinterpret_cast<float4*>(&T.A[0][0][0][0]);
+        for (int i = tid; i < (int)(sizeof(T.A) / sizeof(float4)); i += kTcThreads) a4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (tid < 2 * kTcKB) T.held[tid / kTcKB][tid % kTcKB][0] = T.held[tid / kTcKB][tid % kTcKB][1] = 64;
+    }
+    if (warp == 0) tc::tmem_alloc(&T.tslot, 128);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = T.tslot;
+    const uint32_t idesc = tc::idesc_tf32(128, 48);
+    const int r8 = lane >> 2, kk = lane & 3;  // this lane's row and K entry within a core matrix
+    // footprint entries of A: slot k = tid / 16 (one half-warp per slot), x entry ix = tid % 8,
+    // y entries iy = (tid / 8) % 2 + 2 i
+    const int aslot = tid >> 4, ix = tid & 7, iy0 = (tid >> 3) & 1;
+    int nbatch = 0;  // batches issued (uniform)
+    for (int ch = 0; ch < nch; ++ch) {
+        const int buf = ch & 1;
+        if (tid == 0) {
+            if (!tc::mbar_wait(&T.cpbar[buf], (ch >> 1) & 1, kTcWaitLimit)) {
+                T.fail = 1;
+                atomicExch(status, 1);
+            }
+        }
+        __syncthreads();
+        if (T.fail) break;  // uniform
+        if (tid == 0 && ch + 1 < nch) {  // the other buffer was last read before the barrier above
+            const int n1 = nrec - (ch + 1) * kTcChunk < kTcChunk ? nrec - (ch + 1) * kTcChunk : kTcChunk;
+            tc::fence_async_shared();
+            tc::bulk_g2s(T.pts[buf ^ 1], rec + (int64_t)(rs + (ch + 1) * kTcChunk) * R, (uint32_t)(n1 * R * 4),
+                         &T.cpbar[buf ^ 1]);
+            cp_issued = ch + 2;
+        }
+        const float* pts = T.pts[buf];
+        const int np = nrec - ch * kTcChunk < kTcChunk ? nrec - ch * kTcChunk : kTcChunk;
+        for (int p0 = 0; p0 < np; p0 += kTcKB) {
+            const int st = nbatch & 1;
+            if (nbatch >= 2) {  // the multiplications of batch nbatch - 2 have released this stage
+                if (tid == 0 && !tc::mbar_wait(&T.mbar[st], ((nbatch >> 1) - 1) & 1, kTcWaitLimit)) {
+                    T.fail = 1;
+                    atomicExch(status, 1);
+                }
+                __syncthreads();
+                if (T.fail) break;  // uniform
+            }
+            const int nbt = np - p0 < kTcKB ? np - p0 : kTcKB;
+            // ---- A: clear the footprint this stage holds in slot aslot, then write the new one ----
+            {
+                float* Ah0 = T.A[st][0][0];
+                float* Ah1 = T.A[st][0][1];
+                float* Al0 = T.A[st][1][0];
+                float* Al1 = T.A[st][1][1];
+                const int k = aslot, kg = k >> 2, kq = k & 3;
+                auto offset = [&](int y, int x, int& h) {  // element of A at (y, x), slot k, in half h
+                    h = y >> 3;
+                    const int m = ((y & 7) << 4) | x;
+                    return (((m >> 3) * (kTcKB / 4) + kg) * 8 + (m & 7)) * 4 + kq;
+                };
+                const int ox = T.held[st][k][0], oy = T.held[st][k][1];
+                if (ox < 64 && ix < w) {
+                    const int x = ox + ix;
+                    for (int iy = iy0; iy < w; iy += 2) {
+                        const int y = oy + iy;
+                        if ((unsigned)y < 16u && (unsigned)x < 16u) {
+                            int h;
+                            const int o = offset(y, x, h);
+                            (h ? Ah1 : Ah0)[o] = 0.0f;
+                            (h ? Al1 : Al0)[o] = 0.0f;
+                        }
+                    }
+                }
+                __syncwarp();
+                const bool live = k < nbt;
+                int nx = 64, ny = 64;
+                if (live) {
+                    const float* pt = pts + (p0 + k) * R;
+                    const int cpk = __float_as_int(pt[3]);
+                    nx = (cpk & 255) - 64;
+                    ny = ((cpk >> 8) & 255) - 64;
+                    if (ix < w) {
+                        const int x = nx + ix;
+                        const float fx = pt[4 + ix];
+                        for (int iy = iy0; iy < w; iy += 2) {
+                            const int y = ny + iy;
+                            if ((unsigned)y < 16u && (unsigned)x < 16u) {
+                                int h;
+                                const int o = offset(y, x, h);
+                                const float v = pt[4 + w + iy] * fx;
+                                const float hi = tc::to_tf32(v);
+                                (h ? Ah1 : Ah0)[o] = hi;
+                                (h ? Al1 : Al0)[o] = tc::to_tf32(v - hi);
+                            }
+                        }
+                    }
+                }
+                if ((tid & 15) == 0) {
+                    T.held[st][k][0] = (int16_t)nx;
+                    T.held[st][k][1] = (int16_t)ny;
+                }
+            }
+            // ---- B (dense): q_c phi_z(z) for rows n = (c, z) ----
+            {
+                float* Bh = T.B[st][0];
+                float* Bl = T.B[st][1];
+                for (int cm = warp; cm < 6 * (kTcKB / 4); cm += kTcThreads / 32) {
+                    const int g = cm / (kTcKB / 4), kg = cm % (kTcKB / 4);
+                    const int n = 8 * g + r8, k = 4 * kg + kk;
+                    const int c = n >> 4, z = n & 15;
+                    float v = 0.0f;
+                    if (k < nbt) {
+                        const float* pt = pts + (p0 + k) * R;
+                        const int iz = z - (((__float_as_int(pt[3]) >> 16) & 255) - 64);
+                        if ((unsigned)iz < (unsigned)w) v = pt[c] * pt[4 + 2 * w + iz];
+                    }
+                    const float hi = tc::to_tf32(v);
+                    Bh[cm * 32 + lane] = hi;
+                    Bl[cm * 32 + lane] = tc::to_tf32(v - hi);
+                }
+            }
+            tc::fence_async_shared();
+            __syncthreads();
+            if (tid == 0) {
+                tc::fence_after_sync();
+                constexpr uint32_t lbo = 128, sbo = 128 * (kTcKB / 4);
+#pragma unroll
+                for (int s = 0; s < kTcKB / 8; ++s) {
+                    const uint64_t bh = tc::smem_desc(tc::smem_u32(T.B[st][0]) + 256 * s, lbo, sbo);
+                    const uint64_t bl = tc::smem_desc(tc::smem_u32(T.B[st][1]) + 256 * s, lbo, sbo);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint64_t ah = tc::smem_desc(tc::smem_u32(T.A[st][0][h]) + 256 * s, lbo, sbo);
+                        const uint64_t al = tc::smem_desc(tc::smem_u32(T.A[st][1][h]) + 256 * s, lbo, sbo);
+                        const uint32_t d = tmem + 64 * h;
+                        tc::mma_tf32(d, ah, bh, idesc, (nbatch == 0 && s == 0) ? 0u : 1u);
+                        tc::mma_tf32(d, ah, bl, idesc, 1u);
+                        tc::mma_tf32(d, al, bh, idesc, 1u);
+                    }
+                }
+                tc::commit(&T.mbar[st]);
+            }
+            ++nbatch;
+        }
+        if (T.fail) break;  // uniform (read after the barriers above)
+    }
+    // ---- all multiplications done (the last commit covers every earlier one); on a failure, also the
+    // bulk copies still in flight (copy c completes phase c / 2 of buffer c % 2) ----
+    if (tid == 0) {
+        if (T.fail)
+            for (int c = cp_issued - 2 < 0 ? 0 : cp_issued - 2; c < cp_issued; ++c)
+                tc::mbar_wait(&T.cpbar[c & 1], (c >> 1) & 1, kTcWaitLimit);
+        if (nbatch > 0) {
+            const int last = nbatch - 1;
+            if (!tc::mbar_wait(&T.mbar[last & 1], (last >> 1) & 1, kTcWaitLimit)) {
+                T.fail = 1;
+                atomicExch(status, 1);
+                tc::mbar_wait(&T.mbar[last & 1], (last >> 1) & 1, kTcWaitLimit);  // once more before the release
+            }
+        }
+    }
+    __syncthreads();
+    tc::fence_after_sync();
+    // ---- write the brick: warp w reads rows 32 (w % 4) .. + 31 of half w / 4; columns (c, z) ----
+    {
+        const int h = warp >> 2, qd = warp & 3;
+        const int m = 32 * qd + lane;
+        const int y = 8 * h + (m >> 4), x = m & 15;
+        const bool have = nbatch > 0 && !T.fail;
+        const int64_t ng = S.ngrid;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float v[16];
+            if (have) {
+                tc::tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + 64 * h + 16 * c, v);
+            } else {
+#pragma unroll
+                for (int z = 0; z < 16; ++z) v[z] = 0.0f;
+            }
+#pragma unroll
+            for (int z = 0; z < 16; ++z)
+                grid[c * ng + ((int64_t)(bs[2] + z) * S.n[1] + (bs[1] + y)) * S.n[0] + bs[0] + x] = v[z];
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 128);
 }
 
 // Register-column brick spreading for 16^3 bricks (no atomics at all): the 256 threads of a CTA
@@ -814,6 +1141,9 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
         StageScope st(h, ST_SPREAD);
         const int B = h->gatherB, nb0 = h->nbrick[0], nb1 = h->nbrick[1], nb2 = h->nbrick[2];
         const int64_t nbins = (int64_t)nb0 * nb1 * nb2, Nq = h->Nq;
+        // FP32 grids with narrow kernels (m <= 4) on 16^3 bricks: tensor cores, with their own per-brick
+        // records instead of the bins below
+        const bool use_tc = std::is_same<T, float>::value && B == kColB && S.m <= 4 && h->spread_mode == 0;
         if ((rc = ensure(h, h->spread_bin, sizeof(int32_t) * 2 * Nq, "spread bins"))) return rc;
         if ((rc = ensure(h, h->spread_counts, sizeof(int32_t) * nbins, "spread bin counts"))) return rc;
         if ((rc = ensure(h, h->spread_start, sizeof(int32_t) * (nbins + 1), "spread bin starts"))) return rc;
@@ -825,14 +1155,17 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
         int32_t* counts = (int32_t*)h->spread_counts.p;
         int32_t* start = (int32_t*)h->spread_start.p;
         int32_t* foot = (int32_t*)h->spread_foot.p;
-        if ((rc = check_cuda(h, cudaMemsetAsync(counts, 0, sizeof(int32_t) * nbins, h->stream), "memset"))) return rc;
-        spread_bin_count_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(S, B, nb0, nb1, nb2, Nq, src, sx[0], sx[1],
-                                                                           sx[2], bin, rank, counts);
-        h->launches++;
-        if ((rc = exclusive_scan(h, counts, start, nbins, h->scan_tmp_lr))) return rc;
-        spread_bin_scatter_kernel<T><<<grid_for(Nq, 128), 128, 0, h->stream>>>(S, Nq, src, sx[0], sx[1], sx[2], bin,
-                                                                                rank, start, (T*)h->binned.p, foot);
-        h->launches++;
+        if (!use_tc) {
+            if ((rc = check_cuda(h, cudaMemsetAsync(counts, 0, sizeof(int32_t) * nbins, h->stream), "memset"))) return rc;
+            spread_bin_count_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(S, B, nb0, nb1, nb2, Nq, src, sx[0],
+                                                                               sx[1], sx[2], bin, rank, counts);
+            h->launches++;
+            if ((rc = exclusive_scan(h, counts, start, nbins, h->scan_tmp_lr))) return rc;
+            spread_bin_scatter_kernel<T><<<grid_for(Nq, 128), 128, 0, h->stream>>>(S, Nq, src, sx[0], sx[1], sx[2],
+                                                                                    bin, rank, start, (T*)h->binned.p,
+                                                                                    foot);
+            h->launches++;
+        }
         const unsigned nblk = (unsigned)nbins;
         const T* bsrc = (const T*)h->binned.p;
         const size_t smem = sizeof(T) * 3 * B * (B * (B + 1) + 8);
@@ -853,7 +1186,30 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
                 // FP32 grids with narrow kernels (m <= 4): the plane-owner kernel (the 16-deep
                 // register columns mostly multiply zeros there); wider kernels and FP64 grids use
                 // the columns
-                if (std::is_same<T, float>::value && S.m <= 4)
+                if (use_tc) {
+                    // tensor cores: per-brick records, then the brick product in 3xTF32
+                    if ((rc = ensure_status(h))) return rc;
+                    const int R = tc_record_floats(2 * S.m);
+                    if ((rc = ensure(h, h->tc_counts, sizeof(int32_t) * 2 * nbins, "record counts"))) return rc;
+                    if ((rc = ensure(h, h->tc_start, sizeof(int32_t) * (nbins + 1), "record starts"))) return rc;
+                    if ((rc = ensure(h, h->tc_rec, sizeof(float) * R * 8 * (size_t)Nq, "brick records"))) return rc;
+                    int32_t* tcount = (int32_t*)h->tc_counts.p;
+                    int32_t* tfill = tcount + nbins;
+                    if ((rc = check_cuda(h, cudaMemsetAsync(tcount, 0, sizeof(int32_t) * 2 * nbins, h->stream), "memset")))
+                        return rc;
+                    tc_rec_count_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(S, nb0, nb1, nb2, Nq, src, sx[0], sx[1],
+                                                                                   sx[2], tcount);
+                    if ((rc = exclusive_scan(h, tcount, (int32_t*)h->tc_start.p, nbins, h->scan_tmp_lr))) return rc;
+                    tc_rec_scatter_kernel<<<grid_for(Nq, 128), 128, 0, h->stream>>>(
+                        S, nb0, nb1, nb2, Nq, src, sx[0], sx[1], sx[2], (const int32_t*)h->tc_start.p, tfill,
+                        (float*)h->tc_rec.p);
+                    const size_t tsmem = sizeof(TcSpreadSmem);
+                    cudaFuncSetAttribute(spread_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
+                    spread_tc_kernel<<<nblk, kTcThreads, tsmem, h->stream>>>(S, nb0, nb1, (const int32_t*)h->tc_start.p,
+                                                                            (const float*)h->tc_rec.p, (float*)grid,
+                                                                            h->status_dev);
+                    h->launches += 2;
+                } else if (std::is_same<T, float>::value && S.m <= 4)
                     launch_plane(S.m <= 2 ? spread_plane_kernel<4> : spread_plane_kernel<8>, S.m <= 2 ? 4 : 8);
                 else
                     spread_column_kernel<T><<<nblk, kColThreads, 0, h->stream>>>(S, nb0, nb1, nb2, start, bsrc, foot,

@@ -57,7 +57,7 @@ __global__ void cell_count_kernel(KParams K, CellGrid cg, int64_t n, const doubl
     if (j >= n) return;
     int64_t c = cell_of(cg, K, xyz[j], xyz[n + j], xyz[2 * n + j]);
     cell[j] = (int32_t)c;
-    rank[j] = atomicAdd(&counts[c], 1);
+    rank[j] = warp_aggregated_rank(counts, (int32_t)c);
 }
 
 // Exclusive scan of counts[0..n) into start[0..n] with one CTA of 1024 threads.

@@ -86,6 +86,20 @@ __device__ __forceinline__ void ewald_weights(const KParams& K, double x, double
     }
 }
 
+// Rank of this thread's element within its bin, from one atomicAdd per distinct bin in the warp:
+// the points arrive in cell order, so the lanes of a warp mostly share a bin, and 32 same-address
+// atomics would serialise.  Lanes of the warp that have exited must not be named in the mask.
+__device__ __forceinline__ int32_t warp_aggregated_rank(int32_t* counts, int32_t b) {
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, b);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int32_t base = 0;
+    if (lane == leader) base = atomicAdd(&counts[b], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
+}
+
 // Cell-list geometry.  Cells are r_cut / M wide in y and z (M = nsubdiv); in x each such
 // cell is further split into G slabs (nc[0] counts the slabs), so the candidate range of a
 // node in a row of cells can be trimmed to the slabs within r_cut.
@@ -159,7 +173,11 @@ struct vpbs_handle {
     vpbs::LRSizes lr{};
     vpbs::DevBuf grid_r, grid_c, grid_c2, uhat, decx, decy, decz, nodes_lr;
     vpbs::DevBuf spread_bin, spread_counts, spread_start, binned, spread_foot;  // brick spreading
+    vpbs::DevBuf tc_counts, tc_start, tc_rec;  // tensor-core spreading: per-brick (point, brick) records
     int gatherB = 0;   // brick edge of the atomic-free spreading (0: atomic fallback)
+    int spread_mode = 0;  // 0: tensor-core spreading where it applies; 1: CUDA-core kernels only
+    int* status_host = nullptr;  // mapped pinned word: device-side faults of bounded waits (0: none)
+    int* status_dev = nullptr;
     int nbrick[3] = {0, 0, 0};
     cufftHandle plan_r2c = 0, plan_c2r = 0, plan_c2r_6 = 0;
     bool have_plans = false;
@@ -205,6 +223,8 @@ int set_error(vpbs_handle* h, int code, const std::string& msg);
 int check_cuda(vpbs_handle* h, cudaError_t e, const char* what);
 int ensure(vpbs_handle* h, DevBuf& b, size_t bytes, const char* what);
 int ensure_pinned(vpbs_handle* h, void** buf, size_t* cap, size_t bytes);
+int ensure_status(vpbs_handle* h);   // the mapped status word of bounded device-side waits
+int check_status(vpbs_handle* h);    // after a synchronisation: VPBS_ERR_TIMEOUT if a wait gave up
 
 inline unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
 
