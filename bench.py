@@ -672,7 +672,38 @@ def main():
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.kernel_case:
         return run_kernel_case(args)
+    rc = check_world(args.gpus)
+    if rc is not None:
+        return rc
     return run_reference(args) if args.impl == "reference" else run_ours(args)
+
+
+def launch_command(gpus: int, argv, port: int) -> list:
+    """The torchrun command that runs this script with one rank per GPU (loopback rendezvous)."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+            "--master-addr=127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *argv]
+
+
+def check_world(gpus: int):
+    """--gpus N: under torchrun the world size must be N (else an error); without torchrun and N > 1
+    the script relaunches itself with one rank per GPU and returns that run's exit code.  None: run
+    here."""
+    if gpus < 1:
+        print("bench.py: --gpus must be >= 1", file=sys.stderr)
+        return 2
+    world_env = os.environ.get("WORLD_SIZE")
+    if world_env is not None:
+        if int(world_env) != gpus:
+            print(f"bench.py: --gpus {gpus} but the launcher started {world_env} ranks", file=sys.stderr)
+            return 2
+        return None
+    if gpus == 1:
+        return None
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    return subprocess.call(launch_command(gpus, sys.argv[1:], port))
 
 
 if __name__ == "__main__":

@@ -50,6 +50,13 @@ typedef enum {
 #define VPBS_PRECISION_MIXED 1 /* FP32 bulk (pairs, spreading, FFT, interpolation); FP64
                                   positions, separations, local term, final accumulation */
 
+/* NUFFT spreading kernels.  The reference passes no kernel to NonuniformFFTs.jl (compat "0.8.2, 0.9",
+ * not in its tree), whose default is a Kaiser-Bessel-type kernel; its exact shape parameter, evaluation
+ * and FFT-size rounding cannot be pinned here, so results agree with the reference's to the NUFFT
+ * tolerance (~1e-6 at m = 4), not bit for bit. */
+#define VPBS_NUFFT_ES 0              /* exponential of semicircle, beta = 0.97 pi m (2 - 1/sigma) */
+#define VPBS_NUFFT_KAISER_BESSEL 1   /* backward Kaiser-Bessel, beta = 0.995 pi m (2 - 1/sigma) */
+
 /* Ewald splitting kernels (src/BiotSavart/splitting/splitting.jl:1-47). */
 #define VPBS_SPLITTING_GAUSSIAN 0      /* GaussianSplitting, or NoSplitting when alpha == 0 */
 #define VPBS_SPLITTING_KAISER_BESSEL 1 /* KaiserBesselSplitting (splitting/kaiser_bessel.jl) */
@@ -89,6 +96,7 @@ typedef struct {
     int32_t splitting;            /* VPBS_SPLITTING_* (0, the zero-initialised value: Gaussian) */
     double kb_beta;               /* Kaiser-Bessel shape parameter beta */
     double kb_rtol;               /* Kaiser-Bessel relative accuracy rtol */
+    int32_t nufft_kernel;         /* VPBS_NUFFT_* (0, the zero-initialised value: ES) */
 } vpbs_params;
 
 /* Structure-of-arrays view of a vector of Vec3 (the layout of a StructVector{Vec3}). */
@@ -147,6 +155,15 @@ int vpbs_set_points(vpbs_handle* h, int64_t Np, vpbs_cvec3 nodes, const int32_t*
  * (local_integrals.jl:115-126).  Asynchronous on the handle's stream. */
 int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t shortrange, int32_t longrange,
                  double integration_cutoff);
+
+/* The reference's default device split (src/BiotSavart/BiotSavart.jl:535-605; the short range on
+ * device 2, shortrange/backends/cell_lists.jl:7,50,81; the long range on device 1,
+ * longrange/backends/nonuniformffts.jl:108-118): two handles evaluate the two parts of the same
+ * filaments concurrently (vpbs_compute with shortrange = 1, longrange = 0 on one and the reverse on the
+ * other), and this call adds the computed `fields` of `src` into those of `dst`, on dst's stream after
+ * src's work.  When src lives on another GPU its field crosses once, by a peer copy into dst's memory.
+ * Both handles must hold the same nodes.  Asynchronous. */
+int vpbs_add_field(vpbs_handle* dst, vpbs_handle* src, int32_t fields);
 
 /* copy_output_values_on_nodes! (src/BiotSavart/BiotSavart.jl:628-715): device -> host copy of a
  * computed field (VPBS_VELOCITY or VPBS_STREAMFUNCTION) in node order, AoS [Np][3].

@@ -26,7 +26,7 @@ class OParams(ct.Structure):
         ("m", ct.c_int), ("nquad", ct.c_int), ("nquad_near", ct.c_int), ("lia_segment_fraction", ct.c_double),
         ("avoid_explicit_erf", ct.c_int), ("truncate_spherical", ct.c_int), ("nsubdiv", ct.c_int),
         ("longrange_exact", ct.c_int), ("nthreads", ct.c_int), ("splitting", ct.c_int), ("kb_beta", ct.c_double),
-        ("kb_rtol", ct.c_double), ("fil_offsets", ct.c_void_p),
+        ("kb_rtol", ct.c_double), ("fil_offsets", ct.c_void_p), ("nufft_kernel", ct.c_int),
     ]
 
 
@@ -96,6 +96,7 @@ def make_params(p, *, exact=False, nthreads=0) -> OParams:
             o.Ns[d] = sp.Ns[d]
     o.sigma = p.backend_long.sigma
     o.m = p.backend_long.m
+    o.nufft_kernel = {"es": 0, "kaiser_bessel": 1}[getattr(p.backend_long, "kernel", "es")]
     o.nquad = len(p.quadrature)
     o.nquad_near = len(p.quadrature_near_singularity)
     o.lia_segment_fraction = p.lia_segment_fraction if p.lia_segment_fraction is not None else 0.0

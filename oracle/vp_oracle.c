@@ -895,15 +895,28 @@ static void fft3(cplx* a, const int n[3], int sign) {
 /*   backends/exact_sum.jl:72-121; cache_common.jl:64-108)                  */
 /* ------------------------------------------------------------------------- */
 
-static double es_beta(const vpo_params* p) { return 0.97 * VPO_PI * (1.0 - 1.0 / (2.0 * p->sigma)) * (2.0 * p->m); }
+/* Spreading kernels: ES (exponential of semicircle, Barnett, Magland & af Klinteberg 2019) with
+ * beta = 0.97 pi m (2 - 1/sigma), or the backward Kaiser-Bessel kernel of the NFFT literature
+ * (Potts & Steidl 2003) with beta = 0.995 pi m (2 - 1/sigma); p->nufft_kernel selects (0 / 1). */
+static double es_beta(const vpo_params* p) {
+    if (p->nufft_kernel == 1) return 0.995 * VPO_PI * p->m * (2.0 - 1.0 / p->sigma);
+    return 0.97 * VPO_PI * (1.0 - 1.0 / (2.0 * p->sigma)) * (2.0 * p->m);
+}
+static int g_kernel_kind = 0; /* kernel of the current evaluation (set with the parameters) */
 
-/* ES kernel shifted down by its edge value e^{-beta}, so that it vanishes continuously at
- * |u| = m: the 2m-point window of a point lying on a grid node then does not depend on the
- * last bit of its coordinate (the unshifted kernel jumps by e^{-beta} there). */
+/* Kernels shifted down by their edge value, so that they vanish continuously at |u| = m: the
+ * 2m-point window of a point lying on a grid node then does not depend on the last bit of its
+ * coordinate.  With r = sqrt(1 - (u/m)^2): ES exp(beta (r - 1)) - e^{-beta}; backward
+ * Kaiser-Bessel sinh(beta r) / (r sinh beta) - beta / sinh beta. */
 static inline double es_kernel(double u, int m, double beta) {
     double z = u / m;
     double s = 1.0 - z * z;
-    return s > 0 ? exp(beta * (sqrt(s) - 1.0)) - exp(-beta) : 0.0;
+    if (!(s > 0)) return 0.0;
+    if (g_kernel_kind == 1) {
+        double r = sqrt(s);
+        return (r > 1e-12 ? sinh(beta * r) / (r * sinh(beta)) : beta / sinh(beta)) - beta / sinh(beta);
+    }
+    return exp(beta * (sqrt(s) - 1.0)) - exp(-beta);
 }
 
 /* Fourier transform of the (shifted) ES kernel in grid units: int_{-m}^{m} psi(u) cos(xi u) du,
@@ -920,7 +933,10 @@ static double es_hat(double xi, int m, double beta) {
     double s = 0.0;
     for (int i = 0; i < 128; ++i) {
         double th = gz[i];
-        s += gw[i] * (exp(beta * (cos(th) - 1.0)) - exp(-beta)) * cos(xi * m * sin(th)) * cos(th);
+        double c = cos(th);
+        double pc = g_kernel_kind == 1 ? sinh(beta * c) / sinh(beta) - (beta / sinh(beta)) * c
+                                       : (exp(beta * (c - 1.0)) - exp(-beta)) * c;
+        s += gw[i] * pc * cos(xi * m * sin(th));
     }
     return m * s;
 }
@@ -1020,6 +1036,7 @@ static void lr_vorticity(const vpo_params* p, int64_t Nq, const double* points, 
     int n[3], m = p->m;
     for (int d = 0; d < 3; ++d) n[d] = vpo_fft_size(F->Ns[d], p->sigma);
     double beta = es_beta(p);
+    g_kernel_kind = p->nufft_kernel;
     if (st) { for (int d = 0; d < 3; ++d) st->fft_n[d] = n[d]; st->es_beta = beta; }
     size_t ng = (size_t)n[0] * n[1] * n[2];
     double* grid = (double*)calloc(3 * ng, sizeof(double));
@@ -1160,6 +1177,7 @@ static void lr_interpolate(const vpo_params* p, const lr_field* W, int field, in
     int n[3], m = p->m, w = 2 * m;
     for (int d = 0; d < 3; ++d) n[d] = vpo_fft_size(W->Ns[d], p->sigma);
     double beta = es_beta(p);
+    g_kernel_kind = p->nufft_kernel;
     double* dec[3];
     for (int d = 0; d < 3; ++d) {
         dec[d] = (double*)malloc(sizeof(double) * W->Ns[d]);

@@ -42,6 +42,7 @@ typedef struct {
     double kb_rtol;                  /* Kaiser-Bessel rtol (Chebyshev truncation) */
     const double* fil_offsets;       /* [nfil][3] end-to-end offsets of the filaments (NULL: all
                                         zero, closed filaments; closed_filament.jl:118-132) */
+    int    nufft_kernel;             /* 0: ES kernel; 1: backward Kaiser-Bessel kernel */
 } vpo_params;
 
 /* Kaiser-Bessel short-range weights 1 - F(r) and 1 - F(r) + r f(r) from the truncated

@@ -37,7 +37,8 @@ def test_params_struct_layout(vp):
     # the Kaiser-Bessel fields appended after `device`: int32 then two doubles (8-byte aligned)
     assert P.splitting.offset == P.device.offset + 4
     assert P.kb_beta.offset % 8 == 0 and P.kb_rtol.offset == P.kb_beta.offset + 8
-    assert ct.sizeof(P) == P.kb_rtol.offset + 8
+    assert P.nufft_kernel.offset == P.kb_rtol.offset + 8
+    assert ct.sizeof(P) == P.nufft_kernel.offset + 8  # int32 plus tail padding to 8-byte alignment
 
 
 def _params(vp, **kw):

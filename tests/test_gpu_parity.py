@@ -72,7 +72,7 @@ def test_flags(vp, oracle, built_lib, LIA, short, long):
 
 
 @pytest.mark.parametrize("variant", ["explicit_erf", "lia_fraction", "truncate", "m5", "m6", "m8", "sigma125_m3",
-                                     "gl2", "nsubdiv1"])
+                                     "gl2", "nsubdiv1", "kb_kernel_m4", "kb_kernel_m6"])
 def test_parameter_variants(vp, oracle, built_lib, variant):
     fs, p = vp.configs.tangle20k()
     fs = fs[:30]
@@ -86,6 +86,8 @@ def test_parameter_variants(vp, oracle, built_lib, variant):
         "sigma125_m3": dict(backend_long=vp.NonuniformFFTsBackend(1.25, 3)),
         "gl2": dict(quadrature=vp.GaussLegendre(2)),
         "nsubdiv1": dict(backend_short=vp.CellListsBackend(1)),
+        "kb_kernel_m4": dict(backend_long=vp.NonuniformFFTsBackend(1.5, 4, "kaiser_bessel")),
+        "kb_kernel_m6": dict(backend_long=vp.NonuniformFFTsBackend(1.5, 6, "kaiser_bessel")),
     }[variant]
     p = p.with_(**kw)
     v, psi, _ = gpu_fields(vp, p, fs)
@@ -282,15 +284,16 @@ def test_host_entry_points_agree(vp):
     assert np.abs(v_ptr - v_list).max() <= 1e-13 * np.abs(v_list).max()
 
 
-@pytest.mark.parametrize("sigma,m", [(1.5, 3), (1.5, 4), (2.0, 2), (1.25, 3)])
-def test_tensor_core_spreading(vp, oracle, built_lib, sigma, m):
+@pytest.mark.parametrize("sigma,m,kernel", [(1.5, 3, "es"), (1.5, 4, "es"), (2.0, 2, "es"), (1.25, 3, "es"),
+                                            (1.5, 4, "kaiser_bessel")])
+def test_tensor_core_spreading(vp, oracle, built_lib, sigma, m, kernel):
     """Mixed form: the tensor-core brick product (tcgen05, 3xTF32) against the CUDA-core plane
     kernel and the oracle -- vorticity coefficients (the spread grid after the forward FFT) and
     velocities."""
     from vortexpasta_b200 import _lib
     fs, p = vp.configs.tangle20k(precision="mixed")
     fs = fs[:40]
-    p = p.with_(backend_long=vp.NonuniformFFTsBackend(sigma, m))
+    p = p.with_(backend_long=vp.NonuniformFFTsBackend(sigma, m, kernel))
     assert _lib.load().vpbs_fft_size(p.splitting.Ns[0], sigma) % 16 == 0  # brick spreading applies
     out = {}
     for mode in (0, 1):
@@ -307,3 +310,29 @@ def test_tensor_core_spreading(vp, oracle, built_lib, sigma, m):
     vo, _, _ = oracle.compute_on_nodes(p, fs)
     assert rel(v_tc, vo) < MIXED_TOL
     assert np.linalg.norm(u_tc - u_cc) / np.linalg.norm(u_cc) < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_split_devices_match_single_handle(vp, built_lib, precision):
+    """The reference's device split (short range and long range on two handles, the short-range field
+    added into the long-range one) gives the single-handle result.  Here both handles share GPU 0 (a
+    test box has one GPU); across GPUs the same call adds a peer copy."""
+    import torch
+    fs, p = vp.configs.tangle20k(precision=precision)
+    fs = fs[:30]
+    v1, p1, _ = gpu_fields(vp, p, fs)
+    long_dev = 0
+    short_dev = 1 if torch.cuda.device_count() > 1 else 0
+    c = vp.SplitDevicesCache(p, long_device=long_dev, short_device=short_dev)
+    try:
+        vs = [np.zeros_like(f) for f in fs]
+        ps = [np.zeros_like(f) for f in fs]
+        c.compute_on_nodes_({"velocity": vs, "streamfunction": ps}, fs)
+        vl = [np.zeros_like(f) for f in fs]
+        c.compute_on_nodes_({"velocity": vl}, fs, LIA="only")
+    finally:
+        c.close()
+    tol = 1e-14 if precision == "fp64" else 1e-6
+    assert rel(np.concatenate(vs), v1) < tol and rel(np.concatenate(ps), p1) < tol
+    vo, _, _ = gpu_fields(vp, p, fs, LIA="only")
+    assert rel(np.concatenate(vl), vo) < 1e-14

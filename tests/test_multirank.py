@@ -100,3 +100,18 @@ def test_form_summary_stage_model():
     fs1, p1 = vp.configs.tangle1m()
     out = bench.form_summary(p1, m, 1_000_000, 3_000_000, 1, args, peaks)
     assert out["stages"]["interp"]["frac"] > 0 and out["stages"]["fourier"]["frac"] > 0
+
+
+def test_bench_world_size_checks(monkeypatch):
+    """bench.py --gpus N fails loudly when the launcher started another number of ranks, runs in place
+    for N = 1 or under a matching launcher, and relaunches itself through torchrun otherwise."""
+    import bench
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    assert bench.check_world(4) == 2
+    assert bench.check_world(2) is None
+    monkeypatch.delenv("WORLD_SIZE")
+    assert bench.check_world(1) is None
+    assert bench.check_world(0) == 2
+    cmd = bench.launch_command(4, ["--gpus", "4", "--steps", "3"], 29500)
+    assert cmd[1:3] == ["-m", "torch.distributed.run"] and "--nproc-per-node=4" in cmd
+    assert "--master-addr=127.0.0.1" in cmd and cmd[-4:] == ["--gpus", "4", "--steps", "3"]

@@ -35,6 +35,7 @@ class VpbsParams(ct.Structure):
         ("lia_segment_fraction", ct.c_double), ("avoid_explicit_erf", ct.c_int32),
         ("truncate_spherical", ct.c_int32), ("nsubdiv", ct.c_int32), ("precision", ct.c_int32),
         ("device", ct.c_int32), ("splitting", ct.c_int32), ("kb_beta", ct.c_double), ("kb_rtol", ct.c_double),
+        ("nufft_kernel", ct.c_int32),
     ]
 
 
@@ -53,6 +54,7 @@ SIGNATURES = {
     "vpbs_set_points": (ct.c_int, [ct.c_void_p, ct.c_int64, CVec3, c_int32_p, CVec3, CVec3, c_double_p, c_double_p,
                                    CVec3, CVec3]),
     "vpbs_compute": (ct.c_int, [ct.c_void_p, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_double]),
+    "vpbs_add_field": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_int32]),
     "vpbs_get": (ct.c_int, [ct.c_void_p, ct.c_int32, c_double_p, ct.c_int32]),
     "vpbs_get_soa": (ct.c_int, [ct.c_void_p, ct.c_int32, CVec3, ct.c_int32]),
     "vpbs_device_field": (ct.c_int, [ct.c_void_p, ct.c_int32, ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_void_p),

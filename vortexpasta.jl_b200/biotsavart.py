@@ -44,6 +44,7 @@ def _c_params(p: ParamsBiotSavart) -> _lib.VpbsParams:
             c.Ns[d] = sp.Ns[d]
     c.sigma = p.backend_long.sigma
     c.m = p.backend_long.m
+    c.nufft_kernel = {"es": 0, "kaiser_bessel": 1}[getattr(p.backend_long, "kernel", "es")]
     z, w = p.quadrature.rule()
     c.nquad = len(z)
     for q in range(len(z)):
@@ -319,6 +320,46 @@ def velocity_on_nodes(cache: BiotSavartCache, fs, **kws):
     """velocity_on_nodes (src/BiotSavart/BiotSavart.jl:94-102)."""
     vs = [np.empty_like(np.asarray(f, dtype=np.float64)) for f in fs]
     return velocity_on_nodes_(vs, cache, fs, **kws)
+
+
+class SplitDevicesCache:
+    """The reference's default placement of the two halves of compute_on_nodes! on two GPUs
+    (src/BiotSavart/BiotSavart.jl:535-605): the long range on `long_device` (its cache holds the
+    Fourier field, for the diagnostics) and the short range (local term, pairs) on `short_device`,
+    evaluated concurrently; the short-range fields then cross once, by a peer copy, and are added on
+    the long-range device (vpbs_add_field).  The two devices may be the same."""
+
+    def __init__(self, params: ParamsBiotSavart, long_device: int = 0, short_device: int = 1):
+        if not params.is_periodic:
+            raise ValueError("the device split needs a periodic domain (Ewald splitting)")
+        self.params = params
+        self.long = BiotSavartCache(params.with_(device=long_device))
+        self.short = BiotSavartCache(params.with_(device=short_device))
+        self._lib = self.long._lib
+
+    def close(self):
+        self.long.close()
+        self.short.close()
+
+    def compute_on_nodes_(self, fields: dict, fs, *, LIA=True, shortrange=True, longrange=True,
+                          integration_cutoff=None):
+        names = set(fields)
+        if not names or not names <= {"velocity", "streamfunction"}:
+            raise ValueError(f"some of these fields were not recognised: {tuple(fields)}")
+        mask = ((_lib.VELOCITY if "velocity" in names else 0) |
+                (_lib.STREAMFUNCTION if "streamfunction" in names else 0))
+        lia = _lia_mode(LIA)
+        self.short.set_filaments(fs)
+        self.long.set_filaments(fs)
+        # both halves are queued before either is waited for: they run concurrently
+        self.short.compute(mask, lia, shortrange, False, integration_cutoff)
+        self.long.compute(mask, lia, False, longrange, integration_cutoff)
+        _lib.check(self._lib.vpbs_add_field(self.long.handle, self.short.handle, mask), self.long.handle,
+                   "add_field")
+        for name, bit in (("velocity", _lib.VELOCITY), ("streamfunction", _lib.STREAMFUNCTION)):
+            if name in names:
+                self.long.get_list(bit, fields[name])
+        return fields
 
 
 def _wavenumbers(sp):

@@ -231,6 +231,8 @@ int vpbs_create(const vpbs_params* params, vpbs_handle** out) {
         if (cg.ncell > (int64_t)1 << 30) return set_error(nullptr, VPBS_ERR_PARAMS, "too many cells (rcut too small)");
         if (!(P.sigma > 1.0)) return set_error(nullptr, VPBS_ERR_PARAMS, "NUFFT oversampling factor sigma must be > 1");
         if (P.m < 1 || P.m > kMaxHalfSupport) return set_error(nullptr, VPBS_ERR_PARAMS, "NUFFT half support m must be in 1:8");
+        if (P.nufft_kernel != VPBS_NUFFT_ES && P.nufft_kernel != VPBS_NUFFT_KAISER_BESSEL)
+            return set_error(nullptr, VPBS_ERR_PARAMS, "nufft_kernel must be VPBS_NUFFT_ES or VPBS_NUFFT_KAISER_BESSEL");
         for (int d = 0; d < 3; ++d) {
             if (P.Ns[d] < 2) return set_error(nullptr, VPBS_ERR_PARAMS, "Ns must be >= 2 in each direction");
             if (vpbs_fft_size(P.Ns[d], P.sigma) < 2 * P.m)
@@ -345,10 +347,11 @@ int vpbs_destroy(vpbs_handle* h) {
                       &h->src_seg, &h->dst_cell, &h->dst_start, &h->dst_fill, &h->dst_order, &h->counters,
                       &h->grid_r, &h->grid_c, &h->grid_c2, &h->uhat, &h->decx, &h->decy, &h->decz, &h->nodes_lr,
                       &h->vel, &h->psi, &h->spread_bin, &h->spread_counts, &h->spread_start, &h->binned,
-                      &h->spread_foot, &h->tc_counts, &h->tc_start, &h->tc_rec, &h->ewald_tab, &h->scan_tmp, &h->scan_tmp_lr, &h->rk_vs, &h->rk_tmp};
+                      &h->spread_foot, &h->tc_counts, &h->tc_start, &h->tc_rec, &h->peer_in, &h->ewald_tab, &h->scan_tmp, &h->scan_tmp_lr, &h->rk_vs, &h->rk_tmp};
     for (DevBuf* b : bufs) free_buf(*b);
     if (h->pin_in) cudaFreeHost(h->pin_in);
     if (h->status_host) cudaFreeHost(h->status_host);
+    if (h->xfer_done) cudaEventDestroy(h->xfer_done);
     if (h->pin_out) cudaFreeHost(h->pin_out);
     if (h->h2d_done) cudaEventDestroy(h->h2d_done);
     if (h->aux_stream) cudaStreamSynchronize(h->aux_stream);
@@ -658,6 +661,11 @@ int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t short
 }  // extern "C"
 
 namespace vpbs {
+__global__ void add_field_kernel(int64_t n, const double* __restrict__ src, double* __restrict__ dst) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] += src[i];
+}
+
 // SoA [3][Np] -> AoS [Np][3] (the node-order layout of the host output arrays)
 __global__ void soa_to_aos_kernel(int64_t Np, const double* __restrict__ src, double* __restrict__ dst) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -666,6 +674,42 @@ __global__ void soa_to_aos_kernel(int64_t Np, const double* __restrict__ src, do
 }  // namespace vpbs
 
 extern "C" {
+
+int vpbs_add_field(vpbs_handle* dst, vpbs_handle* src, int32_t fields) {
+    if (!dst || !src || dst == src) return VPBS_ERR_ARG;
+    if (fields < 1 || fields > 3) return set_error(dst, VPBS_ERR_ARG, "fields must be VELOCITY and/or STREAMFUNCTION");
+    if (dst->Np != src->Np || dst->Np < 1) return set_error(dst, VPBS_ERR_ARG, "vpbs_add_field: node counts differ");
+    if ((dst->last_fields & fields) != fields || (src->last_fields & fields) != fields)
+        return set_error(dst, VPBS_ERR_STATE, "vpbs_add_field: field was not computed on both handles");
+    int rc;
+    // the source's work is done before the destination's stream reads it
+    if ((rc = activate(src))) return rc;
+    if (!src->xfer_done && (rc = check_cuda(src, cudaEventCreateWithFlags(&src->xfer_done, cudaEventDisableTiming),
+                                            "cudaEventCreate")))
+        return rc;
+    if ((rc = check_cuda(src, cudaEventRecord(src->xfer_done, src->stream), "event record"))) return rc;
+    if ((rc = activate(dst))) return rc;
+    if ((rc = check_cuda(dst, cudaStreamWaitEvent(dst->stream, src->xfer_done, 0), "stream wait"))) return rc;
+    const int64_t n = 3 * dst->Np;
+    const size_t bytes = sizeof(double) * n;
+    for (int32_t f = VPBS_VELOCITY; f <= VPBS_STREAMFUNCTION; f <<= 1) {
+        if (!(fields & f)) continue;
+        const double* s = (const double*)(f == VPBS_VELOCITY ? src->vel.p : src->psi.p);
+        double* d = (double*)(f == VPBS_VELOCITY ? dst->vel.p : dst->psi.p);
+        if (src->device != dst->device) {
+            // another GPU: one peer copy into this GPU's memory, then the addition reads local memory
+            if ((rc = ensure(dst, dst->peer_in, bytes, "peer field"))) return rc;
+            if ((rc = check_cuda(dst, cudaMemcpyPeerAsync(dst->peer_in.p, dst->device, s, src->device, bytes, dst->stream),
+                                 "peer copy")))
+                return rc;
+            s = (const double*)dst->peer_in.p;
+        }
+        add_field_kernel<<<grid_for(n, 256), 256, 0, dst->stream>>>(n, s, d);
+        dst->launches++;
+        if ((rc = check_cuda(dst, cudaGetLastError(), "add field kernel"))) return rc;
+    }
+    return 0;
+}
 
 static int fetch_soa(vpbs_handle* h, int32_t field, const double** out) {
     if (field != VPBS_VELOCITY && field != VPBS_STREAMFUNCTION) return set_error(h, VPBS_ERR_ARG, "bad field");

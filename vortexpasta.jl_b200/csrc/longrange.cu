@@ -53,18 +53,22 @@ void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
 namespace {
 
 
-// Fourier transform of the shifted ES kernel psi(u) = exp(beta (sqrt(1 - (u/m)^2) - 1)) - e^{-beta}, |u| <= m,
-// at frequency xi (radians per grid spacing): m * int_{-pi/2}^{pi/2} (e^{beta(cos t - 1)} - e^{-beta})
-// cos(xi m sin t) cos t dt, evaluated with a 128-point Gauss-Legendre rule (the substitution
-// u = m sin t removes the square-root endpoint behaviour, so the rule converges fast).
-double es_hat(double xi, int m, double beta) {
+// Fourier transform of the spreading kernel at frequency xi (radians per grid spacing), both kernels
+// shifted down by their edge value so that they vanish at |u| = m (r = sqrt(1 - (u/m)^2)):
+//   ES (exponential of semicircle): psi(u) = exp(beta (r - 1)) - e^{-beta};
+//   backward Kaiser-Bessel:         psi(u) = sinh(beta r) / (r sinh beta) - beta / sinh beta.
+// With u = m sin t (r = cos t) the transform is m int_{-pi/2}^{pi/2} psi(m sin t) cos(xi m sin t) cos t dt,
+// a smooth integrand, evaluated with a 128-point Gauss-Legendre rule.
+double es_hat(double xi, int m, double beta, int kind) {
     static std::vector<double> gx, gw;
     if (gx.empty()) gauss_legendre(128, gx, gw);
     double s = 0.0;
     for (size_t i = 0; i < gx.size(); ++i) {
-        double th = 0.5 * kPi * gx[i];
-        s += 0.5 * kPi * gw[i] * (std::exp(beta * (std::cos(th) - 1.0)) - std::exp(-beta)) * std::cos(xi * m * std::sin(th)) *
-             std::cos(th);
+        const double th = 0.5 * kPi * gx[i], c = std::cos(th);
+        const double pc = kind == VPBS_NUFFT_KAISER_BESSEL
+                              ? std::sinh(beta * c) / std::sinh(beta) - (beta / std::sinh(beta)) * c
+                              : (std::exp(beta * (c - 1.0)) - std::exp(-beta)) * c;
+        s += 0.5 * kPi * gw[i] * pc * std::cos(xi * m * std::sin(th));
     }
     return m * s;
 }
@@ -74,10 +78,16 @@ inline int mode_of(int i, int N) { return i < (N + 1) / 2 ? i : i - N; }
 // ES kernel shifted down by its edge value e^{-beta} (passed as `edge`) so that it vanishes
 // continuously at |u| = m: which 2m-point window a point on a grid node gets then no longer
 // depends on the last bit of its coordinate.
-__device__ __forceinline__ double es_kernel(double u, int m, double beta, double edge) {
+__device__ __forceinline__ double es_kernel(double u, int m, double beta, double edge, int kind) {
     double z = u / m;
     double s = 1.0 - z * z;
-    return s > 0.0 ? exp(beta * (sqrt(s) - 1.0)) - edge : 0.0;
+    if (!(s > 0.0)) return 0.0;
+    if (kind == VPBS_NUFFT_KAISER_BESSEL) {
+        // backward Kaiser-Bessel kernel sinh(beta r) / (r sinh beta), less its edge value beta / sinh beta
+        const double r = sqrt(s);
+        return (r > 1e-12 ? sinh(beta * r) / (r * sinh(beta)) : beta / sinh(beta)) - edge;
+    }
+    return exp(beta * (sqrt(s) - 1.0)) - edge;
 }
 
 __device__ __forceinline__ int wrapi(int i, int n) {
@@ -116,7 +126,7 @@ __global__ void __launch_bounds__(256) spread_kernel_atomic(
         const double xh = (src[d * Nq + j] * scale[d]) / h;
         const int i0 = (int)floor(xh) - S.m + 1;
         i0s[p][d] = i0;
-        for (int s = 0; s < w; ++s) phi[p][d][s] = es_kernel(xh - (i0 + s), S.m, S.beta, S.edge);
+        for (int s = 0; s < w; ++s) phi[p][d][s] = es_kernel(xh - (i0 + s), S.m, S.beta, S.edge, S.kernel);
         qs[p][d] = src[(3 + d) * Nq + j];
     }
     __syncthreads();
@@ -271,7 +281,7 @@ __global__ void spread_bin_scatter_kernel(LRSizes S, int64_t Nq, const double* _
         const double xh = (src[d * Nq + j] * scale[d]) / (2.0 * kPi / S.n[d]);
         const int i0 = (int)floor(xh) - S.m + 1;
         foot[3 * pos + d] = wrapi(i0, S.n[d]);
-        for (int s = 0; s < w; ++s) out[3 + d * w + s] = (T)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge);
+        for (int s = 0; s < w; ++s) out[3 + d * w + s] = (T)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge, S.kernel);
     }
 }
 
@@ -598,7 +608,7 @@ __global__ void tc_rec_scatter_kernel(LRSizes S, int nb0, int nb1, int nb2, int6
         const int i0 = (int)floor(xh) - S.m + 1;
         f[d] = wrapi(i0, S.n[d]);
 #pragma unroll
-        for (int s = 0; s < 8; ++s) phi[d][s] = s < w ? (float)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge) : 0.0f;
+        for (int s = 0; s < 8; ++s) phi[d][s] = s < w ? (float)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge, S.kernel) : 0.0f;
     }
     const float q[3] = {(float)src[3 * Nq + j], (float)src[4 * Nq + j], (float)src[5 * Nq + j]};
     int b0[3], two[3];
@@ -681,9 +691,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
     const uint32_t tmem = T.tslot;
     const uint32_t idesc = tc::idesc_tf32(128, 48);
     const int r8 = lane >> 2, kk = lane & 3;  // this lane's row and K entry within a core matrix
-    // footprint entries of A: slot k = tid / 16 (one half-warp per slot), x entry ix = tid % 8,
-    // y entries iy = (tid / 8) % 2 + 2 i
-    const int aslot = tid >> 4, ix = tid & 7, iy0 = (tid >> 3) & 1;
+    // warp 0 issues the multiplications; warps 1-4 write A (8 threads per slot: x entry ix = lane % 8,
+    // all y entries), warps 5-7 write B, so the issue overlaps with the building of the next batch
+    const int aslot = (tid - 32) >> 3, ix = tid & 7;
+    const bool builds_a = warp >= 1 && warp <= 4, builds_b = warp >= 5;
     int nbatch = 0;  // batches issued (uniform)
     for (int ch = 0; ch < nch; ++ch) {
         const int buf = ch & 1;
@@ -716,7 +727,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
             }
             const int nbt = np - p0 < kTcKB ? np - p0 : kTcKB;
             // ---- A: clear the footprint this stage holds in slot aslot, then write the new one ----
-            {
+            if (builds_a) {
                 float* Ah0 = T.A[st][0][0];
                 float* Ah1 = T.A[st][0][1];
                 float* Al0 = T.A[st][1][0];
@@ -730,7 +741,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
                 const int ox = T.held[st][k][0], oy = T.held[st][k][1];
                 if (ox < 64 && ix < w) {
                     const int x = ox + ix;
-                    for (int iy = iy0; iy < w; iy += 2) {
+                    for (int iy = 0; iy < w; ++iy) {
                         const int y = oy + iy;
                         if ((unsigned)y < 16u && (unsigned)x < 16u) {
                             int h;
@@ -751,7 +762,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
                     if (ix < w) {
                         const int x = nx + ix;
                         const float fx = pt[4 + ix];
-                        for (int iy = iy0; iy < w; iy += 2) {
+                        for (int iy = 0; iy < w; ++iy) {
                             const int y = ny + iy;
                             if ((unsigned)y < 16u && (unsigned)x < 16u) {
                                 int h;
@@ -764,16 +775,16 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
                         }
                     }
                 }
-                if ((tid & 15) == 0) {
+                if (ix == 0) {
                     T.held[st][k][0] = (int16_t)nx;
                     T.held[st][k][1] = (int16_t)ny;
                 }
             }
             // ---- B (dense): q_c phi_z(z) for rows n = (c, z) ----
-            {
+            if (builds_b) {
                 float* Bh = T.B[st][0];
                 float* Bl = T.B[st][1];
-                for (int cm = warp; cm < 6 * (kTcKB / 4); cm += kTcThreads / 32) {
+                for (int cm = warp - 5; cm < 6 * (kTcKB / 4); cm += 3) {
                     const int g = cm / (kTcKB / 4), kg = cm % (kTcKB / 4);
                     const int n = 8 * g + r8, k = 4 * kg + kk;
                     const int c = n >> 4, z = n & 15;
@@ -995,7 +1006,7 @@ __global__ void __launch_bounds__(256) interp_warp_kernel(
         const double scale = d == 0 ? sx0 : (d == 1 ? sx1 : sx2);
         const double xh = (nodes[d * Np + i] * scale) / (2.0 * kPi / S.n[d]);
         const int i0 = (int)floor(xh) - S.m + 1;
-        phs[warp][d][s] = (T)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge);
+        phs[warp][d][s] = (T)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge, S.kernel);
         ixs[warp][d][s] = wrapi(i0 + s, S.n[d]);
     }
     __syncwarp();
@@ -1048,8 +1059,15 @@ int longrange_init(vpbs_handle* h) {
     S.ncgrid = (int64_t)S.nxc * S.n[1] * S.n[2];
     S.nmodes = (int64_t)S.nkx * S.Ns[1] * S.Ns[2];
     S.m = P.m;
-    S.beta = 0.97 * kPi * (1.0 - 1.0 / (2.0 * P.sigma)) * (2.0 * P.m);
-    S.edge = std::exp(-S.beta);
+    S.kernel = P.nufft_kernel;
+    if (S.kernel == VPBS_NUFFT_KAISER_BESSEL) {
+        // the NFFT literature's shape parameter pi m (2 - 1/sigma) (Potts & Steidl 2003), scaled by 0.995
+        S.beta = 0.995 * kPi * P.m * (2.0 - 1.0 / P.sigma);
+        S.edge = S.beta / std::sinh(S.beta);
+    } else {
+        S.beta = 0.97 * kPi * (1.0 - 1.0 / (2.0 * P.sigma)) * (2.0 * P.m);
+        S.edge = std::exp(-S.beta);
+    }
     // brick edge for atomic-free spreading: divides every grid size, >= kernel width, >= 2 bricks
     h->gatherB = 0;
     for (int B : {16, 12, 10, 8}) {
@@ -1080,7 +1098,7 @@ int longrange_init(vpbs_handle* h) {
         const double k0 = 2.0 * kPi / P.L[d];
         for (int i = 0; i < len; ++i) {
             const int k = d == 0 ? i : mode_of(i, S.Ns[d]);
-            const double dec = 1.0 / es_hat(2.0 * kPi * k / S.n[d], S.m, S.beta);
+            const double dec = 1.0 / es_hat(2.0 * kPi * k / S.n[d], S.m, S.beta, S.kernel);
             const double kk = k0 * k;
             tab[d][i] = dec;
             tab[3 + d][i] = dec * std::exp(beta_g * kk * kk);

@@ -120,8 +120,9 @@ struct LRSizes {
     int64_t ncgrid;  // nxc*n1*n2 (complex)
     int64_t nmodes;  // nkx*Ns1*Ns2
     int m;
-    double beta;     // ES kernel shape
-    double edge;     // e^{-beta}, subtracted so the kernel vanishes at |u| = m
+    double beta;     // spreading-kernel shape
+    double edge;     // the kernel's value at |u| = m, subtracted so that it vanishes there
+    int kernel;      // VPBS_NUFFT_*
 };
 
 // Host <-> device staging of flat node and output arrays goes in chunks of at least
@@ -174,6 +175,8 @@ struct vpbs_handle {
     vpbs::DevBuf grid_r, grid_c, grid_c2, uhat, decx, decy, decz, nodes_lr;
     vpbs::DevBuf spread_bin, spread_counts, spread_start, binned, spread_foot;  // brick spreading
     vpbs::DevBuf tc_counts, tc_start, tc_rec;  // tensor-core spreading: per-brick (point, brick) records
+    vpbs::DevBuf peer_in;                       // vpbs_add_field: a field copied from another GPU
+    cudaEvent_t xfer_done = nullptr;            // vpbs_add_field: this handle's fields are complete
     int gatherB = 0;   // brick edge of the atomic-free spreading (0: atomic fallback)
     int spread_mode = 0;  // 0: tensor-core spreading where it applies; 1: CUDA-core kernels only
     int* status_host = nullptr;  // mapped pinned word: device-side faults of bounded waits (0: none)

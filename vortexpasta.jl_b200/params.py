@@ -185,10 +185,17 @@ class NaiveShortRangeBackend:
 
 @dataclass(frozen=True)
 class NonuniformFFTsBackend:
-    """Long-range backend: CUDA NUFFT with the ES kernel (replaces
-    longrange/backends/nonuniformffts.jl:97-126). Defaults sigma = 1.5, m = 4."""
+    """Long-range backend: CUDA NUFFT (replaces longrange/backends/nonuniformffts.jl:97-126).  Defaults
+    sigma = 1.5, m = 4.  `kernel`: "es" (exponential of semicircle, the default) or "kaiser_bessel"
+    (backward Kaiser-Bessel, the kind NonuniformFFTs.jl uses by default; its exact shape parameter is
+    not pinned here, so results match the reference's to the NUFFT tolerance either way)."""
     sigma: float = 1.5
     m: int = 4
+    kernel: str = "es"
+
+    def __post_init__(self):
+        if self.kernel not in ("es", "kaiser_bessel"):
+            raise ValueError("NonuniformFFTsBackend kernel must be 'es' or 'kaiser_bessel'")
 
 
 @dataclass
