@@ -613,6 +613,8 @@ KERNEL_CASES = {
     "pairs1m": "pair kernel of tangle1m (r_cut = L/16, beta = 4) with a 64^3 Fourier grid, FP64 then mixed",
     "tuned500k": "2500 rings x 200 nodes (500k nodes) at the tuned 1M parameters (alpha = 22.03, r_cut = 0.1561, "
                  "Ns = 341, sigma = 1.5, m = 3), mixed precision",
+    "tuned1m": "tangle1m at the Kaiser-Bessel split the tuned form picks (beta = 12.44 from rtol 1e-5 / 4, "
+               "r_cut = 0.13956 = L/45, Ns = 192, FFT 288^3, sigma = 1.5, m = 3), mixed precision",
 }
 
 
@@ -626,6 +628,13 @@ def run_kernel_case(args):
         fs = vp.configs.tangle(5000, 200, 42)
         cases = [("fp64", vp.configs.params_for(L / 16, 4.0, 64, 5)),
                  ("mixed", vp.configs.params_for(L / 16, 4.0, 64, 5, precision="mixed"))]
+    elif args.kernel_case == "tuned1m":
+        from vortexpasta_b200 import learned
+        from vortexpasta_b200.params import C_RTOL_KB
+        fs = vp.configs.tangle(5000, 200, 42)
+        beta = -math.log(1e-5 / learned.KB_MARGIN / C_RTOL_KB)
+        ch = tuning.kb_choice_from(L, 0.139555577934889, beta, 1.5, 3)
+        cases = [("mixed", ch.params(L, "mixed"))]
     else:
         fs = vp.configs.tangle(2500, 200, 42)
         ch = tuning.EwaldChoice(alpha=22.0286100737363, rcut=0.15608485585182466, Ns=341, sigma=1.5, m=3)
