@@ -556,15 +556,17 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) spread_plane_kernel(
 // then read from tensor memory and written once (no atomics).  Every wait is bounded: on a timeout the
 // kernel records it in *status, stops issuing, and releases its tensor memory.
 constexpr int kTcThreads = 256;
-constexpr int kTcKB = 16;    // points per batch: two K-steps of 8
-constexpr int kTcChunk = 128;  // records per bulk copy
+constexpr int kTcKB = 16;      // points per batch: two K-steps of 8
+constexpr int kTcChunk = 128;  // records per bulk copy (a multiple of kTcKB: batches never straddle chunks)
+constexpr int kTcBatchesPerChunk = kTcChunk / kTcKB;
 constexpr int kTcRecMax = 28;  // floats per record for w <= 8
+constexpr int kTcBuilderWarps = 7;  // warps 1-4 write A, warps 5-7 write B
 constexpr uint32_t kTcWaitLimit = 1u << 26;
 
 // floats per record: charges (3), packed corner (1), 3 kernel rows of w values, padded to 16 bytes
 __host__ __device__ constexpr int tc_record_floats(int w) { return (4 + 3 * w + 3) & ~3; }
 
-__device__ __forceinline__ void tc_point_bricks(const LRSizes& S, const int f[3], int w, int b0[3], int two[3]) {
+__device__ __forceinline__ void tc_point_bricks(const int f[3], int w, int b0[3], int two[3]) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         b0[d] = f[d] >> 4;
@@ -581,7 +583,7 @@ __global__ void tc_rec_count_kernel(LRSizes S, int nb0, int nb1, int nb2, int64_
     const int f[3] = {footprint_start(src[j], sx0, S.n[0], S.m), footprint_start(src[Nq + j], sx1, S.n[1], S.m),
                       footprint_start(src[2 * Nq + j], sx2, S.n[2], S.m)};
     int b0[3], two[3];
-    tc_point_bricks(S, f, w, b0, two);
+    tc_point_bricks(f, w, b0, two);
     const int nbv[3] = {nb0, nb1, nb2};
     for (int e = 0; e < 8; ++e) {
         const int ex = e & 1, ey = (e >> 1) & 1, ez = e >> 2;
@@ -591,28 +593,33 @@ __global__ void tc_rec_count_kernel(LRSizes S, int nb0, int nb1, int nb2, int64_
     }
 }
 
-// The records: position start[brick] + rank (ranks from a second aggregated count into `fill`).
-__global__ void tc_rec_scatter_kernel(LRSizes S, int nb0, int nb1, int nb2, int64_t Nq, const double* __restrict__ src,
-                                      double sx0, double sx1, double sx2, const int32_t* __restrict__ start,
-                                      int32_t* __restrict__ fill, float* __restrict__ rec) {
+// The records: position start[brick] + rank (ranks from a second aggregated count into `fill`).  A
+// record is assembled in registers and written with 16-byte stores.
+template <int W>
+__global__ void __launch_bounds__(128) tc_rec_scatter_kernel(LRSizes S, int nb0, int nb1, int nb2, int64_t Nq,
+                                                             const double* __restrict__ src, double sx0, double sx1,
+                                                             double sx2, const int32_t* __restrict__ start,
+                                                             int32_t* __restrict__ fill, float* __restrict__ rec) {
+    constexpr int R = tc_record_floats(W);
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= Nq) return;
-    const int w = 2 * S.m;
-    const int R = tc_record_floats(w);
     const double scale[3] = {sx0, sx1, sx2};
     int f[3];
-    float phi[3][8];
+    float r[R];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const double xh = (src[d * Nq + j] * scale[d]) / (2.0 * kPi / S.n[d]);
         const int i0 = (int)floor(xh) - S.m + 1;
         f[d] = wrapi(i0, S.n[d]);
 #pragma unroll
-        for (int s = 0; s < 8; ++s) phi[d][s] = s < w ? (float)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge, S.kernel) : 0.0f;
+        for (int s = 0; s < W; ++s) r[4 + d * W + s] = (float)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge, S.kernel);
     }
-    const float q[3] = {(float)src[3 * Nq + j], (float)src[4 * Nq + j], (float)src[5 * Nq + j]};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) r[c] = (float)src[(3 + c) * Nq + j];
+#pragma unroll
+    for (int k = 4 + 3 * W; k < R; ++k) r[k] = 0.0f;
     int b0[3], two[3];
-    tc_point_bricks(S, f, w, b0, two);
+    tc_point_bricks(f, W, b0, two);
     const int nbv[3] = {nb0, nb1, nb2};
     for (int e = 0; e < 8; ++e) {
         const int ex = e & 1, ey = (e >> 1) & 1, ez = e >> 2;
@@ -620,44 +627,47 @@ __global__ void tc_rec_scatter_kernel(LRSizes S, int nb0, int nb1, int nb2, int6
         const int bx = (b0[0] + ex) % nbv[0], by = (b0[1] + ey) % nbv[1], bz = (b0[2] + ez) % nbv[2];
         const int32_t b = (bz * nb1 + by) * nb0 + bx;
         const int64_t pos = (int64_t)start[b] + warp_aggregated_rank(fill, b);
-        float* r = rec + pos * R;
         // corner relative to the brick, biased by 64 into one byte per dimension
         const int ox = (f[0] & 15) - 16 * ex, oy = (f[1] & 15) - 16 * ey, oz = (f[2] & 15) - 16 * ez;
-        r[0] = q[0];
-        r[1] = q[1];
-        r[2] = q[2];
         r[3] = __int_as_float((ox + 64) | ((oy + 64) << 8) | ((oz + 64) << 16));
+        float4* dst = reinterpret_cast<float4*>(rec + pos * R);
 #pragma unroll
-        for (int d = 0; d < 3; ++d)
-#pragma unroll
-            for (int s = 0; s < 8; ++s)
-                if (s < w) r[4 + d * w + s] = phi[d][s];
-        for (int k = 4 + 3 * w; k < R; ++k) r[k] = 0.0f;
+        for (int k = 0; k < R / 4; ++k) dst[k] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
     }
 }
 
 struct TcSpreadSmem {
-    // operands [stage][hi, lo]([half]), K-major core matrices [row / 8][k / 4][8][4]; A is zero outside
-    // the footprints of the batch it holds (entries are cleared again before the stage is reused)
-    float A[2][2][2][128 * kTcKB];
+    // operands [stage][hi, lo], K-major core matrices of 8 rows x 4 values.  A: rows m = 16 y + x, the
+    // halves y < 8 and y >= 8 one after the other, so the element (y, x, k) sits at
+    // 256 y + 128 (x / 8) + 4 (x % 8) + 32 (k / 4) + k % 4; zero outside the footprints of the batch
+    // the stage holds (entries are cleared again before the stage is reused).  B: rows n = 16 c + z.
+    float A[2][2][256 * kTcKB];
     float B[2][2][48 * kTcKB];
     float pts[2][kTcChunk * kTcRecMax];  // records of the current and the next chunk
     int16_t held[2][kTcKB][2];           // (x, y) corner of the footprint each stage's A holds per slot (64: none)
     int fail;
-    uint64_t mbar[2];    // multiplications of each operand stage done
+    uint64_t full[2];    // operands of each stage written (one arrival per builder warp)
+    uint64_t empty[2];   // multiplications of each stage done (tcgen05.commit)
     uint64_t cpbar[2];   // bulk copy of each record buffer done
     uint32_t tslot;
 };
 
+// Warp roles: warp 0 (one elected thread) issues the bulk copies of the records and the multiplications;
+// warps 1-4 write A (8 threads per point slot: x entry ix = lane % 8, all y entries), warps 5-7 write B.
+// No CTA-wide barrier inside the loop: builders arrive on full[stage] when their part of a batch is
+// written, the issuing thread waits on it, multiplies and commits to empty[stage], which the builders
+// wait on before they overwrite that stage two batches later.  A record buffer is refilled (chunk c + 2)
+// once the issuing thread has seen every batch of chunk c written, i.e. read by all builders.
+template <int W>
 __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int nb0, int nb1,
                                                                   const int32_t* __restrict__ rec_start,
                                                                   const float* __restrict__ rec, float* __restrict__ grid,
                                                                   int* __restrict__ status) {
     extern __shared__ __align__(128) unsigned char tc_raw[];
     TcSpreadSmem& T = *reinterpret_cast<TcSpreadSmem*>(tc_raw);
+    volatile int* fail = &T.fail;
     constexpr int B16 = 16;
-    const int w = 2 * S.m;
-    const int R = tc_record_floats(w);
+    constexpr int R = tc_record_floats(W);
     const int bx = blockIdx.x % nb0;
     const int by = (blockIdx.x / nb0) % nb1;
     const int bz = blockIdx.x / (nb0 * nb1);
@@ -665,22 +675,24 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int rs = rec_start[blockIdx.x], nrec = rec_start[blockIdx.x + 1] - rs;
     const int nch = (nrec + kTcChunk - 1) / kTcChunk;
+    const int nbt = (nrec + kTcKB - 1) / kTcKB;  // batches
+    auto chunk_copy = [&](int c) {               // thread 0 only
+        const int n = nrec - c * kTcChunk < kTcChunk ? nrec - c * kTcChunk : kTcChunk;
+        tc::bulk_g2s(T.pts[c & 1], rec + (int64_t)(rs + c * kTcChunk) * R, (uint32_t)(n * R * 4), &T.cpbar[c & 1]);
+    };
     int cp_issued = 0;  // bulk copies issued (thread 0)
     if (tid == 0) {
-        tc::mbar_init(&T.mbar[0], 1);
-        tc::mbar_init(&T.mbar[1], 1);
-        tc::mbar_init(&T.cpbar[0], 1);
-        tc::mbar_init(&T.cpbar[1], 1);
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&T.full[i], kTcBuilderWarps);
+            tc::mbar_init(&T.empty[i], 1);
+            tc::mbar_init(&T.cpbar[i], 1);
+        }
         tc::fence_mbar_init();
         T.fail = 0;
-        if (nch > 0) {
-            const int n0 = nrec < kTcChunk ? nrec : kTcChunk;
-            tc::bulk_g2s(T.pts[0], rec + (int64_t)rs * R, (uint32_t)(n0 * R * 4), &T.cpbar[0]);
-            cp_issued = 1;
-        }
+        for (; cp_issued < 2 && cp_issued < nch; ++cp_issued) chunk_copy(cp_issued);
     }
     {  // zero operands A (float4 stores)
-        float4* a4 = reinterpret_cast<float4*>(&T.A[0][0][0][0]);
+        float4* a4 = reinterpret_cast<float4*>(&T.A[0][0][0]);
         for (int i = tid; i < (int)(sizeof(T.A) / sizeof(float4)); i += kTcThreads) a4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (tid < 2 * kTcKB) T.held[tid / kTcKB][tid % kTcKB][0] = T.held[tid / kTcKB][tid % kTcKB][1] = 64;
     }
@@ -689,119 +701,31 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = T.tslot;
-    const uint32_t idesc = tc::idesc_tf32(128, 48);
-    const int r8 = lane >> 2, kk = lane & 3;  // this lane's row and K entry within a core matrix
-    // warp 0 issues the multiplications; warps 1-4 write A (8 threads per slot: x entry ix = lane % 8,
-    // all y entries), warps 5-7 write B, so the issue overlaps with the building of the next batch
-    const int aslot = (tid - 32) >> 3, ix = tid & 7;
-    const bool builds_a = warp >= 1 && warp <= 4, builds_b = warp >= 5;
-    int nbatch = 0;  // batches issued (uniform)
-    for (int ch = 0; ch < nch; ++ch) {
-        const int buf = ch & 1;
-        if (tid == 0) {
-            if (!tc::mbar_wait(&T.cpbar[buf], (ch >> 1) & 1, kTcWaitLimit)) {
-                T.fail = 1;
-                atomicExch(status, 1);
-            }
-        }
-        __syncthreads();
-        if (T.fail) break;  // uniform
-        if (tid == 0 && ch + 1 < nch) {  // the other buffer was last read before the barrier above
-            const int n1 = nrec - (ch + 1) * kTcChunk < kTcChunk ? nrec - (ch + 1) * kTcChunk : kTcChunk;
-            tc::fence_async_shared();
-            tc::bulk_g2s(T.pts[buf ^ 1], rec + (int64_t)(rs + (ch + 1) * kTcChunk) * R, (uint32_t)(n1 * R * 4),
-                         &T.cpbar[buf ^ 1]);
-            cp_issued = ch + 2;
-        }
-        const float* pts = T.pts[buf];
-        const int np = nrec - ch * kTcChunk < kTcChunk ? nrec - ch * kTcChunk : kTcChunk;
-        for (int p0 = 0; p0 < np; p0 += kTcKB) {
-            const int st = nbatch & 1;
-            if (nbatch >= 2) {  // the multiplications of batch nbatch - 2 have released this stage
-                if (tid == 0 && !tc::mbar_wait(&T.mbar[st], ((nbatch >> 1) - 1) & 1, kTcWaitLimit)) {
-                    T.fail = 1;
-                    atomicExch(status, 1);
-                }
-                __syncthreads();
-                if (T.fail) break;  // uniform
-            }
-            const int nbt = np - p0 < kTcKB ? np - p0 : kTcKB;
-            // ---- A: clear the footprint this stage holds in slot aslot, then write the new one ----
-            if (builds_a) {
-                float* Ah0 = T.A[st][0][0];
-                float* Ah1 = T.A[st][0][1];
-                float* Al0 = T.A[st][1][0];
-                float* Al1 = T.A[st][1][1];
-                const int k = aslot, kg = k >> 2, kq = k & 3;
-                auto offset = [&](int y, int x, int& h) {  // element of A at (y, x), slot k, in half h
-                    h = y >> 3;
-                    const int m = ((y & 7) << 4) | x;
-                    return (((m >> 3) * (kTcKB / 4) + kg) * 8 + (m & 7)) * 4 + kq;
-                };
-                const int ox = T.held[st][k][0], oy = T.held[st][k][1];
-                if (ox < 64 && ix < w) {
-                    const int x = ox + ix;
-                    for (int iy = 0; iy < w; ++iy) {
-                        const int y = oy + iy;
-                        if ((unsigned)y < 16u && (unsigned)x < 16u) {
-                            int h;
-                            const int o = offset(y, x, h);
-                            (h ? Ah1 : Ah0)[o] = 0.0f;
-                            (h ? Al1 : Al0)[o] = 0.0f;
-                        }
+    auto give_up = [&]() {
+        *fail = 1;
+        atomicExch(status, 1);
+    };
+    if (warp == 0) {
+        // ---- issuing thread ----
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_tf32(128, 48);
+            int issued = 0;
+            for (int b = 0; b < nbt; ++b) {
+                const int st = b & 1;
+                if (b > 0 && b % kTcBatchesPerChunk == 0) {
+                    // batch b starts chunk c - 1; every batch of chunk c - 2 (the previous content of
+                    // chunk c's buffer) has been written, so its records have been read
+                    const int c = b / kTcBatchesPerChunk + 1;
+                    if (c < nch) {
+                        tc::fence_async_shared();
+                        chunk_copy(c);
+                        cp_issued = c + 1;
                     }
                 }
-                __syncwarp();
-                const bool live = k < nbt;
-                int nx = 64, ny = 64;
-                if (live) {
-                    const float* pt = pts + (p0 + k) * R;
-                    const int cpk = __float_as_int(pt[3]);
-                    nx = (cpk & 255) - 64;
-                    ny = ((cpk >> 8) & 255) - 64;
-                    if (ix < w) {
-                        const int x = nx + ix;
-                        const float fx = pt[4 + ix];
-                        for (int iy = 0; iy < w; ++iy) {
-                            const int y = ny + iy;
-                            if ((unsigned)y < 16u && (unsigned)x < 16u) {
-                                int h;
-                                const int o = offset(y, x, h);
-                                const float v = pt[4 + w + iy] * fx;
-                                const float hi = tc::to_tf32(v);
-                                (h ? Ah1 : Ah0)[o] = hi;
-                                (h ? Al1 : Al0)[o] = tc::to_tf32(v - hi);
-                            }
-                        }
-                    }
+                if (*fail || !tc::mbar_wait(&T.full[st], (b >> 1) & 1, kTcWaitLimit)) {
+                    give_up();
+                    break;
                 }
-                if (ix == 0) {
-                    T.held[st][k][0] = (int16_t)nx;
-                    T.held[st][k][1] = (int16_t)ny;
-                }
-            }
-            // ---- B (dense): q_c phi_z(z) for rows n = (c, z) ----
-            if (builds_b) {
-                float* Bh = T.B[st][0];
-                float* Bl = T.B[st][1];
-                for (int cm = warp - 5; cm < 6 * (kTcKB / 4); cm += 3) {
-                    const int g = cm / (kTcKB / 4), kg = cm % (kTcKB / 4);
-                    const int n = 8 * g + r8, k = 4 * kg + kk;
-                    const int c = n >> 4, z = n & 15;
-                    float v = 0.0f;
-                    if (k < nbt) {
-                        const float* pt = pts + (p0 + k) * R;
-                        const int iz = z - (((__float_as_int(pt[3]) >> 16) & 255) - 64);
-                        if ((unsigned)iz < (unsigned)w) v = pt[c] * pt[4 + 2 * w + iz];
-                    }
-                    const float hi = tc::to_tf32(v);
-                    Bh[cm * 32 + lane] = hi;
-                    Bl[cm * 32 + lane] = tc::to_tf32(v - hi);
-                }
-            }
-            tc::fence_async_shared();
-            __syncthreads();
-            if (tid == 0) {
                 tc::fence_after_sync();
                 constexpr uint32_t lbo = 128, sbo = 128 * (kTcKB / 4);
 #pragma unroll
@@ -810,33 +734,122 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
                     const uint64_t bl = tc::smem_desc(tc::smem_u32(T.B[st][1]) + 256 * s, lbo, sbo);
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
-                        const uint64_t ah = tc::smem_desc(tc::smem_u32(T.A[st][0][h]) + 256 * s, lbo, sbo);
-                        const uint64_t al = tc::smem_desc(tc::smem_u32(T.A[st][1][h]) + 256 * s, lbo, sbo);
+                        const uint32_t a0 = tc::smem_u32(T.A[st][0]) + 8192 * h + 256 * s;
+                        const uint32_t a1 = tc::smem_u32(T.A[st][1]) + 8192 * h + 256 * s;
+                        const uint64_t ah = tc::smem_desc(a0, lbo, sbo);
+                        const uint64_t al = tc::smem_desc(a1, lbo, sbo);
                         const uint32_t d = tmem + 64 * h;
-                        tc::mma_tf32(d, ah, bh, idesc, (nbatch == 0 && s == 0) ? 0u : 1u);
+                        tc::mma_tf32(d, ah, bh, idesc, (b == 0 && s == 0) ? 0u : 1u);
                         tc::mma_tf32(d, ah, bl, idesc, 1u);
                         tc::mma_tf32(d, al, bh, idesc, 1u);
                     }
                 }
-                tc::commit(&T.mbar[st]);
+                tc::commit(&T.empty[st]);
+                issued = b + 1;
             }
-            ++nbatch;
+            // all multiplications done (the last commit covers every earlier one); after a failure,
+            // also the bulk copies still in flight (copy c completes phase c / 2 of buffer c % 2)
+            if (issued > 0 && !tc::mbar_wait(&T.empty[(issued - 1) & 1], ((issued - 1) >> 1) & 1, kTcWaitLimit)) {
+                give_up();
+                tc::mbar_wait(&T.empty[(issued - 1) & 1], ((issued - 1) >> 1) & 1, kTcWaitLimit);
+            }
+            if (*fail)
+                for (int c = cp_issued - 2 < 0 ? 0 : cp_issued - 2; c < cp_issued; ++c)
+                    tc::mbar_wait(&T.cpbar[c & 1], (c >> 1) & 1, kTcWaitLimit);
         }
-        if (T.fail) break;  // uniform (read after the barriers above)
-    }
-    // ---- all multiplications done (the last commit covers every earlier one); on a failure, also the
-    // bulk copies still in flight (copy c completes phase c / 2 of buffer c % 2) ----
-    if (tid == 0) {
-        if (T.fail)
-            for (int c = cp_issued - 2 < 0 ? 0 : cp_issued - 2; c < cp_issued; ++c)
-                tc::mbar_wait(&T.cpbar[c & 1], (c >> 1) & 1, kTcWaitLimit);
-        if (nbatch > 0) {
-            const int last = nbatch - 1;
-            if (!tc::mbar_wait(&T.mbar[last & 1], (last >> 1) & 1, kTcWaitLimit)) {
-                T.fail = 1;
-                atomicExch(status, 1);
-                tc::mbar_wait(&T.mbar[last & 1], (last >> 1) & 1, kTcWaitLimit);  // once more before the release
+        __syncwarp();
+    } else {
+        // ---- builders ----
+        const bool builds_a = warp <= 4;
+        const int aslot = (tid - 32) >> 3, ix = tid & 7;          // A: slot and x entry
+        const int r8 = lane >> 2, kk = lane & 3;                  // B: row and K entry within a core matrix
+        const int kof = (aslot >> 2) * 32 + (aslot & 3);          // A: K offset of the slot
+        int b = 0;
+        for (int ch = 0; ch < nch; ++ch) {
+            if (*fail || !tc::mbar_wait(&T.cpbar[ch & 1], (ch >> 1) & 1, kTcWaitLimit)) {
+                give_up();
+                break;
             }
+            const float* pts = T.pts[ch & 1];
+            const int np = nrec - ch * kTcChunk < kTcChunk ? nrec - ch * kTcChunk : kTcChunk;
+            for (int p0 = 0; p0 < np; p0 += kTcKB, ++b) {
+                const int st = b & 1;
+                if (b >= 2 && (*fail || !tc::mbar_wait(&T.empty[st], ((b >> 1) - 1) & 1, kTcWaitLimit))) {
+                    give_up();
+                    break;
+                }
+                const int nb = np - p0 < kTcKB ? np - p0 : kTcKB;
+                if (builds_a) {
+                    // clear the footprint this stage holds in slot aslot, then write the new one
+                    float* Ah = T.A[st][0];
+                    float* Al = T.A[st][1];
+                    const int ox = T.held[st][aslot][0], oy = T.held[st][aslot][1];
+                    if (ox < 64 && ix < W) {
+                        const int x = ox + ix;
+                        if ((unsigned)x < 16u) {
+                            const int base = (x >> 3) * 128 + (x & 7) * 4 + kof;
+#pragma unroll
+                            for (int iy = 0; iy < W; ++iy) {
+                                const int y = oy + iy;
+                                if ((unsigned)y < 16u) {
+                                    Ah[256 * y + base] = 0.0f;
+                                    Al[256 * y + base] = 0.0f;
+                                }
+                            }
+                        }
+                    }
+                    __syncwarp();
+                    int nx = 64, ny = 64;
+                    if (aslot < nb) {
+                        const float* pt = pts + (p0 + aslot) * R;
+                        const int cpk = __float_as_int(pt[3]);
+                        nx = (cpk & 255) - 64;
+                        ny = ((cpk >> 8) & 255) - 64;
+                        const int x = nx + ix;
+                        if (ix < W && (unsigned)x < 16u) {
+                            const float fx = pt[4 + ix];
+                            const int base = (x >> 3) * 128 + (x & 7) * 4 + kof;
+#pragma unroll
+                            for (int iy = 0; iy < W; ++iy) {
+                                const int y = ny + iy;
+                                if ((unsigned)y < 16u) {
+                                    const float v = pt[4 + W + iy] * fx;
+                                    const float hi = tc::to_tf32(v);
+                                    Ah[256 * y + base] = hi;
+                                    Al[256 * y + base] = tc::to_tf32(v - hi);
+                                }
+                            }
+                        }
+                    }
+                    if (ix == 0) {
+                        T.held[st][aslot][0] = (int16_t)nx;
+                        T.held[st][aslot][1] = (int16_t)ny;
+                    }
+                } else {
+                    // B (dense): q_c phi_z(z) for rows n = (c, z)
+                    float* Bh = T.B[st][0];
+                    float* Bl = T.B[st][1];
+#pragma unroll 2
+                    for (int cm = warp - 5; cm < 6 * (kTcKB / 4); cm += 3) {
+                        const int g = cm >> 2, kg = cm & 3;
+                        const int n = 8 * g + r8, k = 4 * kg + kk;
+                        const int c = n >> 4, z = n & 15;
+                        float v = 0.0f;
+                        if (k < nb) {
+                            const float* pt = pts + (p0 + k) * R;
+                            const int iz = z - (((__float_as_int(pt[3]) >> 16) & 255) - 64);
+                            if ((unsigned)iz < (unsigned)W) v = pt[c] * pt[4 + 2 * W + iz];
+                        }
+                        const float hi = tc::to_tf32(v);
+                        Bh[cm * 32 + lane] = hi;
+                        Bl[cm * 32 + lane] = tc::to_tf32(v - hi);
+                    }
+                }
+                tc::fence_async_shared();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&T.full[st]);
+            }
+            if (*fail) break;
         }
     }
     __syncthreads();
@@ -846,7 +859,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
         const int h = warp >> 2, qd = warp & 3;
         const int m = 32 * qd + lane;
         const int y = 8 * h + (m >> 4), x = m & 15;
-        const bool have = nbatch > 0 && !T.fail;
+        const bool have = nbt > 0 && !*fail;
         const int64_t ng = S.ngrid;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -1218,14 +1231,23 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
                     tc_rec_count_kernel<<<grid_for(Nq, 256), 256, 0, h->stream>>>(S, nb0, nb1, nb2, Nq, src, sx[0], sx[1],
                                                                                    sx[2], tcount);
                     if ((rc = exclusive_scan(h, tcount, (int32_t*)h->tc_start.p, nbins, h->scan_tmp_lr))) return rc;
-                    tc_rec_scatter_kernel<<<grid_for(Nq, 128), 128, 0, h->stream>>>(
-                        S, nb0, nb1, nb2, Nq, src, sx[0], sx[1], sx[2], (const int32_t*)h->tc_start.p, tfill,
-                        (float*)h->tc_rec.p);
-                    const size_t tsmem = sizeof(TcSpreadSmem);
-                    cudaFuncSetAttribute(spread_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
-                    spread_tc_kernel<<<nblk, kTcThreads, tsmem, h->stream>>>(S, nb0, nb1, (const int32_t*)h->tc_start.p,
-                                                                            (const float*)h->tc_rec.p, (float*)grid,
-                                                                            h->status_dev);
+                    auto launch_tc = [&](auto wtag) {
+                        constexpr int W = decltype(wtag)::value;
+                        tc_rec_scatter_kernel<W><<<grid_for(Nq, 128), 128, 0, h->stream>>>(
+                            S, nb0, nb1, nb2, Nq, src, sx[0], sx[1], sx[2], (const int32_t*)h->tc_start.p, tfill,
+                            (float*)h->tc_rec.p);
+                        const size_t tsmem = sizeof(TcSpreadSmem);
+                        cudaFuncSetAttribute(spread_tc_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
+                        spread_tc_kernel<W><<<nblk, kTcThreads, tsmem, h->stream>>>(
+                            S, nb0, nb1, (const int32_t*)h->tc_start.p, (const float*)h->tc_rec.p, (float*)grid,
+                            h->status_dev);
+                    };
+                    switch (S.m) {
+                        case 1: launch_tc(std::integral_constant<int, 2>()); break;
+                        case 2: launch_tc(std::integral_constant<int, 4>()); break;
+                        case 3: launch_tc(std::integral_constant<int, 6>()); break;
+                        default: launch_tc(std::integral_constant<int, 8>()); break;
+                    }
                     h->launches += 2;
                 } else if (std::is_same<T, float>::value && S.m <= 4)
                     launch_plane(S.m <= 2 ? spread_plane_kernel<4> : spread_plane_kernel<8>, S.m <= 2 ? 4 : 8);
