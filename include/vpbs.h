@@ -290,6 +290,13 @@ int vpbs_f32_weights_eval(int32_t splitting, double alpha, double rcut, double k
  * reference. */
 int vpbs_periodic_eval(double L, int32_t nc, const double* x, int64_t n, double* folded, int64_t* cell);
 
+/* Host copies dst[k] <- src[k] of bytes[k] each (k < n) on the library's copy threads, the routine the
+ * host-buffer entry points stage their inputs and outputs with: blocks split into pieces of about
+ * 1 MB, small blocks grouped, a pool of up to 7 threads plus the caller (created on first use, and
+ * again in a forked child).  Host memory only; no GPU needed.  Exists to test the staging; no
+ * counterpart in the reference. */
+int vpbs_host_copies(int64_t n, void* const* dst, const void* const* src, const size_t* bytes);
+
 /* Measured CUDA-core FMA throughput of `device` in TFLOP/s (fp64 = 1: double, 0: float); the
  * denominator of the pair kernel's roofline.  Measurement support; no counterpart in the
  * reference. */

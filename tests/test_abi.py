@@ -204,3 +204,62 @@ def test_f32_pair_weights(vp, built_lib, case):
         ea, eg, _ = O.kb_weights(beta, rcut, rtol, r)
     assert np.abs(a - ea).max() < 2e-7
     assert np.abs(g - eg).max() < 2e-7
+
+
+def _host_copies(lib, dsts, srcs):
+    from vortexpasta_b200 import _lib  # noqa: F401
+    n = len(dsts)
+    dp = (ct.c_void_p * max(n, 1))(*[d.ctypes.data for d in dsts])
+    sp = (ct.c_void_p * max(n, 1))(*[s.ctypes.data for s in srcs])
+    nb = (ct.c_size_t * max(n, 1))(*[s.nbytes for s in srcs])
+    return lib.vpbs_host_copies(n, dp, sp, nb)
+
+
+def test_host_copy_threads(built_lib):
+    """The staging copies of the host-buffer entry points: every byte of every block arrives, for one
+    large block (split into pieces), many small blocks (grouped), mixed sizes and empty blocks, over
+    repeated jobs on the same thread pool."""
+    from vortexpasta_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(5)
+    cases = [[24 << 20], [4800] * 3000, [0, 17, 3 << 20, 1 << 20, 5, 0, (1 << 20) + 3, 999_999],
+             [1 << 10], [(2 << 20) + 8]]
+    for rep in range(3):
+        for sizes in cases:
+            srcs = [rng.integers(0, 256, size=b, dtype=np.uint8) for b in sizes]
+            dsts = [np.zeros(b, dtype=np.uint8) for b in sizes]
+            assert _host_copies(lib, dsts, srcs) == 0
+            for s, d in zip(srcs, dsts):
+                assert np.array_equal(s, d)
+    assert lib.vpbs_host_copies(-1, None, None, None) != 0
+
+
+def _copy_in_child(q):
+    from vortexpasta_b200 import _lib
+    lib = _lib.load()
+    src = [np.arange(3 << 20, dtype=np.uint8)]
+    dst = [np.zeros(3 << 20, dtype=np.uint8)]
+    rc = _host_copies(lib, dst, src)
+    q.put(rc == 0 and np.array_equal(src[0], dst[0]))
+
+
+@pytest.mark.filterwarnings("ignore:This process .* is multi-threaded:DeprecationWarning")
+def test_host_copy_threads_after_fork(built_lib):
+    """A child forked after the parent's copy threads started has none of them: its first large copy
+    starts its own pool instead of waiting for threads that do not exist."""
+    import multiprocessing as mp
+    from vortexpasta_b200 import _lib
+    lib = _lib.load()
+    src = [np.ones(4 << 20, dtype=np.uint8)]
+    dst = [np.zeros(4 << 20, dtype=np.uint8)]
+    assert _host_copies(lib, dst, src) == 0  # the parent's pool exists now
+    ctx = mp.get_context("fork")
+    q = ctx.Queue()
+    p = ctx.Process(target=_copy_in_child, args=(q,))
+    p.start()
+    p.join(60)
+    alive = p.is_alive()
+    if alive:
+        p.kill()
+    assert not alive and p.exitcode == 0
+    assert q.get(timeout=5)

@@ -74,6 +74,8 @@ SIGNATURES = {
     "vpbs_f32_weights_eval": (ct.c_int, [ct.c_int32, ct.c_double, ct.c_double, ct.c_double, ct.c_double, c_double_p,
                                          ct.c_int64, c_float_p, c_float_p]),
     "vpbs_periodic_eval": (ct.c_int, [ct.c_double, ct.c_int32, c_double_p, ct.c_int64, c_double_p, c_int64_p]),
+    "vpbs_host_copies": (ct.c_int, [ct.c_int64, ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_void_p),
+                                    ct.POINTER(ct.c_size_t)]),
     "vpbs_point_data_noalloc": (ct.c_int, [ct.POINTER(VpbsParams), ct.c_int64, c_int64_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                            ct.c_void_p, ct.c_void_p, ct.c_void_p]),

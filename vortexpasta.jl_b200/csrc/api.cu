@@ -5,8 +5,15 @@
 #include <algorithm>
 #include <new>
 #include <string>
+#include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
+
+#include <unistd.h>
 
 #include "vpbs_internal.cuh"
 #include "periodic.cuh"
@@ -381,31 +388,115 @@ namespace vpbs {
 
 // Copies `n` blocks (dst[k] <- src[k], bytes[k]) with up to 8 host threads (large inputs only):
 // the staging of filament lists into and out of pinned memory is bound by host memory copies.
+// Host copy threads: a pool created on first use (and again in a forked child, whose parent's threads
+// do not exist there; the old pool is left alone), running the pieces of one job at a time with the
+// calling thread taking part.  Each job has its own counters, so a thread still leaving an old job never
+// takes a piece of the next one.
+namespace copy_threads {
+struct CopyJob {
+    std::function<void(int64_t)> fn;
+    int64_t n = 0;
+    std::atomic<int64_t> next{0}, done{0};
+    std::mutex m;
+    std::condition_variable cv;
+};
+
+struct CopyPool {
+    std::mutex submit, m;
+    std::condition_variable cv;
+    std::shared_ptr<CopyJob> job;
+    uint64_t gen = 0;
+    pid_t pid;
+    explicit CopyPool(int nthreads) : pid(getpid()) {
+        for (int i = 0; i < nthreads; ++i) std::thread([this] { loop(); }).detach();
+    }
+    static void work(CopyJob& j) {
+        int64_t i;
+        while ((i = j.next.fetch_add(1)) < j.n) {
+            j.fn(i);
+            if (j.done.fetch_add(1) + 1 == j.n) {
+                std::lock_guard<std::mutex> lk(j.m);
+                j.cv.notify_all();
+            }
+        }
+    }
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            std::shared_ptr<CopyJob> j;
+            {
+                std::unique_lock<std::mutex> lk(m);
+                cv.wait(lk, [&] { return gen != seen; });
+                seen = gen;
+                j = job;
+            }
+            if (j) work(*j);
+        }
+    }
+    void run(int64_t n, std::function<void(int64_t)> fn) {
+        std::lock_guard<std::mutex> one(submit);
+        auto j = std::make_shared<CopyJob>();
+        j->fn = std::move(fn);
+        j->n = n;
+        {
+            std::lock_guard<std::mutex> lk(m);
+            job = j;
+            ++gen;
+        }
+        cv.notify_all();
+        work(*j);
+        std::unique_lock<std::mutex> lk(j->m);
+        j->cv.wait(lk, [&] { return j->done.load() == j->n; });
+    }
+};
+
+CopyPool& copy_pool() {
+    static std::mutex mu;
+    static CopyPool* pool = nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pool || pool->pid != getpid()) {
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        pool = new CopyPool((int)std::min(7u, hw > 1 ? hw - 1 : 1u));  // lives until the process ends
+    }
+    return *pool;
+}
+}  // namespace copy_threads
+
+// Host copies of n blocks, split into pieces of about 1 MB run on the copy pool (blocks below 2 MB
+// in total are copied by the calling thread).
 static void parallel_copies(int64_t n, void* const* dst, const void* const* src, const size_t* bytes) {
+    constexpr size_t kPiece = (size_t)1 << 20;
     size_t total = 0;
     for (int64_t k = 0; k < n; ++k) total += bytes[k];
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const int T = (int)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, total >> 21));  // >= 2 MB per thread
-    auto work = [&](int64_t a, int64_t b) {
-        for (int64_t k = a; k < b; ++k) std::memcpy(dst[k], src[k], bytes[k]);
-    };
-    if (T <= 1) {
-        work(0, n);
+    if (total < 2 * kPiece) {
+        for (int64_t k = 0; k < n; ++k) std::memcpy(dst[k], src[k], bytes[k]);
         return;
     }
-    // split the blocks into T ranges of about equal bytes
-    std::vector<int64_t> cut(T + 1, n);
-    cut[0] = 0;
-    size_t acc = 0;
-    int t = 1;
-    for (int64_t k = 0; k < n && t < T; ++k) {
-        acc += bytes[k];
-        if (acc >= total * t / T) cut[t++] = k + 1;
+    struct Piece {
+        char* d;
+        const char* s;
+        size_t b;
+    };
+    std::vector<Piece> pieces;
+    for (int64_t k = 0; k < n; ++k) {  // large blocks split into pieces
+        if (bytes[k] >= kPiece) {
+            for (size_t o = 0; o < bytes[k]; o += kPiece)
+                pieces.push_back({(char*)dst[k] + o, (const char*)src[k] + o, std::min(kPiece, bytes[k] - o)});
+        } else {
+            pieces.push_back({(char*)dst[k], (const char*)src[k], bytes[k]});
+        }
     }
-    std::vector<std::thread> pool;
-    for (int i = 0; i < T; ++i)
-        if (cut[i] < cut[i + 1]) pool.emplace_back(work, cut[i], cut[i + 1]);
-    for (auto& th : pool) th.join();
+    // merge runs of small pieces so that each job item copies about kPiece bytes
+    std::vector<std::pair<size_t, size_t>> items;  // [first piece, end piece)
+    for (size_t i = 0; i < pieces.size();) {
+        size_t j = i, acc = 0;
+        while (j < pieces.size() && (j == i || acc + pieces[j].b <= kPiece)) acc += pieces[j++].b;
+        items.push_back({i, j});
+        i = j;
+    }
+    copy_threads::copy_pool().run((int64_t)items.size(), [&](int64_t it) {
+        for (size_t p = items[it].first; p < items[it].second; ++p) std::memcpy(pieces[p].d, pieces[p].s, pieces[p].b);
+    });
 }
 
 // Shared tail of the filament entry points: offsets (host) are staged in pin_in[0..), the nodes
@@ -1059,7 +1150,15 @@ extern "C" int vpbs_f32_weights_eval(int32_t splitting, double alpha, double rcu
     return 0;
 }
 
-extern "C" int vpbs_periodic_eval(double L, int32_t nc, const double* x, int64_t n, double* folded, int64_t* cell) {
+extern "C" int vpbs_host_copies(int64_t n, void* const* dst, const void* const* src, const size_t* bytes) {
+    if (n < 0 || (n > 0 && (!dst || !src || !bytes))) return VPBS_ERR_ARG;
+    for (int64_t k = 0; k < n; ++k)
+        if (bytes[k] && (!dst[k] || !src[k])) return VPBS_ERR_ARG;
+    parallel_copies(n, dst, src, bytes);
+    return 0;
+}
+
+int vpbs_periodic_eval(double L, int32_t nc, const double* x, int64_t n, double* folded, int64_t* cell) {
     using namespace vpbs;
     if (!(L > 0) || nc < 1 || n < 0 || (n > 0 && !x)) return set_error(nullptr, VPBS_ERR_ARG, "vpbs_periodic_eval: bad arguments");
     const int ncs[3] = {nc, 1, 1};

@@ -32,13 +32,23 @@ __device__ __forceinline__ FilView fil_view(const double* knots, const double* p
     return f;
 }
 
+// j mod n in [0, n).  The spline code only asks for j in [-n, 2n) (n >= 5 nodes, indices at most 6
+// away from a node), which takes no division; other j take the general form.
 __device__ __forceinline__ long pmodl(long j, long n) {
+    if (j >= 0 && j < n) return j;
+    if (j < 0 && j >= -n) return j + n;
+    if (j >= n && j < 2 * n) return j - n;
     long r = j % n;
     return r < 0 ? r + n : r;
 }
 
+// Knot t_j of the periodically extended sequence, t_{j + q n} = t_j + q T (the same rounding as
+// t[j - q n] + q T for every q: q = +-1 adds or subtracts T exactly as the general form does).
 __device__ __forceinline__ double knot_at(const FilView& f, long j) {
-    long n = f.n;
+    const long n = f.n;
+    if (j >= 0 && j < n) return f.t[j];
+    if (j < 0 && j >= -n) return f.t[j + n] - f.T;
+    if (j >= n && j < 2 * n) return f.t[j - n] + f.T;
     long q = (j >= 0) ? j / n : -((-j + n - 1) / n);
     return f.t[j - q * n] + (double)q * f.T;
 }

@@ -127,7 +127,7 @@ struct LRSizes {
 
 // Host <-> device staging of flat node and output arrays goes in chunks of at least
 // kStageChunk bytes (at most kStageEvents of them), host copies overlapping the transfers.
-constexpr size_t kStageChunk = (size_t)8 << 20;
+constexpr size_t kStageChunk = (size_t)4 << 20;
 constexpr int kStageEvents = 16;
 
 struct DevBuf {
