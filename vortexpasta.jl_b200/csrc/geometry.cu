@@ -101,6 +101,70 @@ __device__ __forceinline__ void eval_seg(const FilView& f, const double* coef, l
     }
 }
 
+// Knots t_{i-4} .. t_{i+5} around segment i and the reciprocals of the knot spans the B-spline
+// recurrence divides by, 1 / (t_{i+s+1} - t_{i+s+1-r}) for r = 1..5 and s < r (spline.jl:116-160 uses
+// the same recurrence): the spans do not depend on the evaluation point, so every evaluation on the
+// segment shares one division per span.
+struct SegBasis {
+    double t[10];    // t[4 + j] = t_{i+j}
+    double inv[15];  // inv[r (r - 1) / 2 + s]
+};
+
+__device__ __forceinline__ void seg_basis_init(const FilView& f, long i, SegBasis& B) {
+#pragma unroll
+    for (int j = -4; j <= 5; ++j) B.t[4 + j] = knot_at(f, i + j);
+#pragma unroll
+    for (int r = 1; r <= 5; ++r)
+#pragma unroll
+        for (int s = 0; s < r; ++s) B.inv[r * (r - 1) / 2 + s] = 1.0 / (B.t[5 + s] - B.t[5 + s - r]);
+}
+
+// bsplvb<K> on the segment of B: N[s] = B_{i-K+1+s, K}(x) for x in [t_i, t_{i+1}).
+template <int K>
+__device__ __forceinline__ void bsplvb_seg(const SegBasis& B, double x, double (&N)[K]) {
+    double left[K], right[K];
+    N[0] = 1.0;
+#pragma unroll
+    for (int r = 1; r < K; ++r) {
+        left[r] = x - B.t[5 - r];
+        right[r] = B.t[4 + r] - x;
+        double saved = 0.0;
+#pragma unroll
+        for (int s = 0; s < r; ++s) {
+            const double tmp = N[s] * B.inv[r * (r - 1) / 2 + s];
+            N[s] = saved + right[s + 1] * tmp;
+            saved = left[r - s] * tmp;
+        }
+        N[r] = saved;
+    }
+}
+
+// eval_seg<D> with the segment's shared knots and spans.
+template <int D>
+__device__ __forceinline__ void eval_seg_b(const FilView& f, const SegBasis& B, const double* coef, long i,
+                                           double zeta, double out[3]) {
+    constexpr int K = 6 - D;
+    const double x = (1.0 - zeta) * B.t[4] + zeta * B.t[5];
+    double N[K];
+    bsplvb_seg<K>(B, x, N);
+    out[0] = out[1] = out[2] = 0.0;
+#pragma unroll
+    for (int s = 0; s < K; ++s) {
+        const long j = pmodl(i - K + 1 + s, f.n);
+        out[0] += coef[3 * j + 0] * N[s];
+        out[1] += coef[3 * j + 1] * N[s];
+        out[2] += coef[3 * j + 2] * N[s];
+    }
+    if (D == 0) {
+        const double r = x / f.T;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) out[d] += r * f.o[d];
+    } else if (D == 1) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) out[d] += f.o[d] / f.T;
+    }
+}
+
 // Solve the 4x4 Woodbury capacitance system with partial pivoting (3 right-hand sides).
 __device__ void solve4(double H[4][4], double r[4][3]) {
     for (int c = 0; c < 4; ++c) {
@@ -324,7 +388,10 @@ __device__ double seg_len(const FilView& f, const double* c1, long i, int nq, co
 
 // One thread per node: point data of pointdata_impl.jl:65-108 and, when
 // lia_segment_fraction is set, the local integrals of local_integrals.jl:253-293.
-__global__ void __launch_bounds__(128) point_data_kernel(
+// FUSE: full segments without lia_segment_fraction (quadrature points written here); compiled
+// separately so that the common path carries none of the other path's code.
+template <bool FUSE>
+__global__ void __launch_bounds__(128, FUSE ? 4 : 1) point_data_kernel(
     KParams K, int64_t Np, const int64_t* __restrict__ offsets, const int32_t* __restrict__ fil_of_node,
     const double* __restrict__ X, const double* __restrict__ knots, const double* __restrict__ periods,
     const double* __restrict__ coef, const double* __restrict__ dcoef1, const double* __restrict__ dcoef2,
@@ -351,9 +418,11 @@ __global__ void __launch_bounds__(128) point_data_kernel(
         nodes[d * Np + k] = xf[d];
     }
     idx_prev[k] = (int32_t)(i == 0 ? off + n - 1 : k - 1);
+    SegBasis B;
+    seg_basis_init(f, i, B);
     double s1[3], s2[3];
-    eval_seg<1>(f, c1, i, 0.0, s1);
-    eval_seg<2>(f, c2, i, 0.0, s2);
+    eval_seg_b<1>(f, B, c1, i, 0.0, s1);
+    eval_seg_b<2>(f, B, c2, i, 0.0, s2);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         d1[d * Np + k] = s1[d];
@@ -361,16 +430,16 @@ __global__ void __launch_bounds__(128) point_data_kernel(
     }
     const double g = K.lia_fraction;
     const bool has_g = g > 0;
-    if (fuse_quad) {
+    if (FUSE) {
         // full segments (no lia_segment_fraction): the quadrature points and charges of segment i
         // (as quad_points_kernel computes them) and its length from the same s' values, in the
         // operation order of seg_len; delta^- is the previous node's delta^+ (dm_from_prev_kernel)
-        const double dt = knot_at(f, i + 1) - knot_at(f, i);
+        const double dt = B.t[5] - B.t[4];
         double acc = 0.0;
         for (int q = 0; q < K.nquad; ++q) {
             double s[3], sp[3];
-            eval_seg<0>(f, c, i, K.qz[q], s);
-            eval_seg<1>(f, c1, i, K.qz[q], sp);
+            eval_seg_b<0>(f, B, c, i, K.qz[q], s);
+            eval_seg_b<1>(f, B, c1, i, K.qz[q], sp);
             const int64_t mq = k * K.nquad + q;
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
@@ -384,7 +453,7 @@ __global__ void __launch_bounds__(128) point_data_kernel(
         dm[k] = seg_len(f, c1, i - 1, K.nquad, K.qz, K.qw, has_g ? 1.0 - g : 0.0, 1.0);
         dp[k] = seg_len(f, c1, i, K.nquad, K.qz, K.qw, 0.0, has_g ? g : 1.0);
     }
-    if (want_li) {
+    if (!FUSE && want_li) {
         // nonlia_integration_limits: ((0, 1-g), (g, 1))  (local_integrals.jl:103-104)
         double v[3] = {0, 0, 0}, ps[3] = {0, 0, 0};
         for (int side = 0; side < 2; ++side) {
@@ -501,7 +570,7 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
     // without lia_segment_fraction the point-data kernel also writes the quadrature points
     // and charges (one pass of spline evaluations per segment instead of two)
     const bool fuse = !want_li;
-    point_data_kernel<<<grid_for(Np, 128), 128, 0, h->stream>>>(
+    (fuse ? point_data_kernel<true> : point_data_kernel<false>)<<<grid_for(Np, 128), 128, 0, h->stream>>>(
         h->K, Np, d_offsets, (const int32_t*)h->fil_of_node.p, d_nodes, knots, periods, (const double*)h->coefs.p,
         (const double*)h->dcoef1.p, (const double*)h->dcoef2.p, (double*)h->nodes.p, (int32_t*)h->idx_prev.p,
         (double*)h->d1.p, (double*)h->d2.p, (double*)h->dm.p, (double*)h->dp.p, (double*)h->points.p,
@@ -642,7 +711,7 @@ extern "C" int vpbs_point_data_noalloc(const vpbs_params* params, int64_t nfil, 
         return set_error(nullptr, VPBS_ERR_CUDA, std::string("vpbs_point_data_noalloc: ") + cudaGetErrorString(e));
     spline_solve_kernel<<<grid_for(nfil, 4), 128, 0, s>>>(nfil, d_offsets, nodes_xyz, knots, periods, fil_of_node, coefs,
                                                           dcoef1, dcoef2, scratch, status, 0, 0, nullptr);
-    point_data_kernel<<<grid_for(Np, 128), 128, 0, s>>>(K, Np, d_offsets, fil_of_node, nodes_xyz, knots, periods, coefs,
+    point_data_kernel<false><<<grid_for(Np, 128), 128, 0, s>>>(K, Np, d_offsets, fil_of_node, nodes_xyz, knots, periods, coefs,
                                                         dcoef1, dcoef2, nodes, node_idx_prev, deriv1, deriv2,
                                                         delta_minus, delta_plus, points, charges, nullptr, nullptr, 0,
                                                         0, nullptr);
