@@ -28,6 +28,11 @@ from pathlib import Path
 
 import numpy as np
 
+# Hardware work queues of this process's CUDA context (read when the context is created, so set before
+# any CUDA call): the batching form runs one stream per system, and with the default 8 queues streams
+# share queues and their kernels run one after another.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -388,14 +393,33 @@ def ensemble_systems(vp, nsys=64, seed=64):
     return out
 
 
-def measure_ensemble(vp, args, local_rank, rank=0, world=1):
-    """RK4 steps of the ensemble replayed as one CUDA graph per step, against the same steps
-    issued system by system without a graph.  With several ranks the systems are sharded by
-    estimated cost (timestepping.shard_systems; no data exchange), each rank steps its shard,
-    and the job's time is the max over ranks."""
+def small_ensemble_systems(vp, nsys=256, seed=65):
+    """A launch-bound ensemble: `nsys` small random tangles (5-10 rings x 200 nodes), Ns = 32 (FFT 48^3),
+    beta = 3.5, NUFFT m = 4, mixed precision, dt as in ``ensemble_systems``.  Each system's kernels are
+    a few microseconds long, so issuing them one by one from the host costs more than running them."""
+    from vortexpasta_b200.params import (GaussianSplitting, GaussLegendre, NonuniformFFTsBackend, ParamsBiotSavart,
+                                         kelvin_wave_period)
+    L = 2 * math.pi
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(nsys):
+        fs = vp.curves.random_tangle(int(rng.integers(5, 11)), 200, L=L, seed=int(rng.integers(1 << 31)))
+        p = ParamsBiotSavart(Gamma=1.0, a=1e-8, Delta=0.25, splitting=GaussianSplitting(Ls=L, beta=3.5, Ns=32),
+                             quadrature=GaussLegendre(3), backend_long=NonuniformFFTsBackend(1.5, 4), precision="mixed")
+        dmin = min(float(np.linalg.norm(np.roll(f, -1, axis=0) - f, axis=1).min()) for f in fs)
+        dt = min(1e-3 * L ** 2 / 1.0, kelvin_wave_period(dmin, a=1e-8, Delta=0.25, Gamma=1.0))
+        out.append((fs, p, dt))
+    return out
+
+
+def time_ensemble(vp, all_systems, args, local_rank, rank, world, autotune):
+    """RK4 steps of an ensemble replayed as one CUDA graph per step, against the same steps issued
+    system by system without a graph (each system on its own streams, so those calls overlap on the
+    device too).  With several ranks the systems are sharded by estimated cost
+    (timestepping.shard_systems; no data exchange) and the job's time is the max over ranks."""
     import torch
     from vortexpasta_b200 import timestepping, tuning
-    all_systems = ensemble_systems(vp)
+    L = 2 * math.pi
     costs = [timestepping.system_cost(sum(len(f) for f in fs), tuning.fft_size(p.splitting.Ns[0], p.backend_long.sigma))
              for fs, p, _ in all_systems]
     mine = timestepping.shard_systems(costs, world)[rank]
@@ -404,7 +428,7 @@ def measure_ensemble(vp, args, local_rank, rank=0, world=1):
     nodes = sum(sum(len(f) for f in fs) for fs, _, _ in systems)
     t0 = time.perf_counter()
     ens = timestepping.Ensemble([(fs, p.with_(device=local_rank), dt) for fs, p, dt in systems], device=local_rank,
-                                autotune_pairs=True)
+                                autotune_pairs=autotune)
     t_setup = time.perf_counter() - t0
     try:
         stream = torch.cuda.ExternalStream(ens.stream(), device=local_rank)
@@ -416,28 +440,54 @@ def measure_ensemble(vp, args, local_rank, rank=0, world=1):
         e1.record(stream)
         ens.synchronize()
         ms_graph = e0.elapsed_time(e1)
-        # the same steps, system by system, no graph (host wall clock around a synchronised loop)
+        # the same steps, system by system, no graph (host wall clock around a synchronised loop);
+        # `host_ms` is the time the host spends issuing them (the calls return before the device is done)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         for _ in range(args.ensemble_steps):
             for c, x, (_, _, dt) in zip(ens.caches, ens.nodes, systems):
                 timestepping.rk4_step(c, x.data_ptr(), dt)
+        host_ms = (time.perf_counter() - t1) * 1e3
         torch.cuda.synchronize()
         ms_seq = (time.perf_counter() - t1) * 1e3
         finite = all(bool(torch.isfinite(x).all()) for x in ens.nodes)
     finally:
         ens.close()
-    ms_graph, ms_seq, nonfinite = max_over_ranks([ms_graph, ms_seq, 0.0 if finite else 1.0], local_rank, world)
+    ms_graph, ms_seq, host_ms, nonfinite = max_over_ranks([ms_graph, ms_seq, host_ms, 0.0 if finite else 1.0],
+                                                          local_rank, world)
     evals = 4 * nodes_all * args.ensemble_steps
-    return {"systems": len(all_systems), "nodes_total": nodes_all, "rk4_steps": args.ensemble_steps,
-            "ranks": world, "systems_on_rank0": len(systems), "nodes_on_rank0": nodes,
-            "node_velocities_per_s": evals / (ms_graph * 1e-3), "ms_per_step": ms_graph / args.ensemble_steps,
-            "sequential_node_velocities_per_s": evals / (ms_seq * 1e-3), "graph_speedup": ms_seq / ms_graph,
-            "pair_blocks_autotuned": {"systems_off_rule": sum(1 for t in ens.tuned if t), "edges": sorted(set(ens.tuned))}, "setup_s": t_setup, "finite": nonfinite == 0.0,
-            "description": "64 random tangles, N log-uniform in [2k, 200k] (200-node rings), Ns = nearest power of "
-                           "two to N^(1/3)*4 in [64, 256], beta = 3.5, mixed precision, RK4 with dt = min(1e-3 L^2/Gamma, "
-                           "Kelvin-wave period of the shortest segment); one CUDA graph launch per RK4 step (all "
-                           "systems, one stream each), vs the same steps issued system by system"}
+    kw_limited = sum(1 for _, _, dt in all_systems if dt < 1e-3 * L ** 2)
+    out = {"systems": len(all_systems), "nodes_total": nodes_all, "rk4_steps": args.ensemble_steps,
+           "ranks": world, "systems_on_rank0": len(systems), "nodes_on_rank0": nodes,
+           "node_velocities_per_s": evals / (ms_graph * 1e-3), "ms_per_step": ms_graph / args.ensemble_steps,
+           "sequential_node_velocities_per_s": evals / (ms_seq * 1e-3), "graph_speedup": ms_seq / ms_graph,
+           "sequential_host_issue_ms_per_step": host_ms / args.ensemble_steps,
+           "sequential_ms_per_step": ms_seq / args.ensemble_steps,
+           "dt_rule": "min(1e-3 L^2/Gamma, Kelvin-wave period of the shortest segment)",
+           "dt_kelvin_wave_limited_systems": kw_limited,
+           "setup_s": t_setup, "finite": nonfinite == 0.0}
+    if autotune:
+        out["autotuned"] = {"pair_block_systems_off_rule": sum(1 for t in ens.tuned if t),
+                            "pair_block_edges": sorted(set(ens.tuned)),
+                            "spread_mode_systems_cuda_cores": sum(1 for m in ens.spread_modes if m)}
+    return out
+
+
+def measure_ensemble(vp, args, local_rank, rank=0, world=1):
+    """The batching form on two ensembles: the 64 random tangles of ``ensemble_systems`` (device-bound:
+    the host issues a step's kernels faster than the device runs them, so the graph has nothing to
+    save) and the 256 small tangles of ``small_ensemble_systems`` (launch-bound)."""
+    big = time_ensemble(vp, ensemble_systems(vp), args, local_rank, rank, world, autotune=True)
+    big["description"] = ("64 random tangles, N log-uniform in [2k, 200k] (200-node rings), Ns = nearest power of "
+                          "two to N^(1/3)*4 in [64, 256], beta = 3.5, mixed precision, RK4 with dt = min(1e-3 L^2/Gamma, "
+                          "Kelvin-wave period of the shortest segment); one CUDA graph launch per RK4 step (all "
+                          "systems, one stream each), vs the same steps issued system by system")
+    small = time_ensemble(vp, small_ensemble_systems(vp), args, local_rank, rank, world, autotune=True)
+    small["description"] = ("256 random tangles of 5-10 rings x 200 nodes, Ns = 32 (FFT 48^3), beta = 3.5, m = 4, "
+                            "mixed precision, dt as above; one CUDA graph launch per RK4 step vs the same steps "
+                            "issued system by system")
+    big["small_systems"] = small
+    return big
 
 
 def run_ours(args):

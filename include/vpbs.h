@@ -364,6 +364,12 @@ const char* vpbs_ensemble_last_error(void);
  * Synchronous. */
 int vpbs_autotune(vpbs_handle* h, int32_t* chosen);
 
+/* Autotuner of the long range: times one long-range evaluation (spreading, FFTs, Fourier operators,
+ * interpolation) on the handle's current point data with each spreading mode of vpbs_spread_mode and
+ * keeps the fastest (`chosen`: the mode; mode 0 unless mode 1 is more than 3 % faster).  Overwrites
+ * the handle's output fields.  Synchronous. */
+int vpbs_autotune_spread(vpbs_handle* h, int32_t* chosen);
+
 /* Spreading kernels of the FP32 (mixed) form for NUFFT half-supports m <= 4 on grids of 16^3 bricks:
  * mode 0 (default) multiplies each brick on the tensor cores (tcgen05, 3xTF32); mode 1 uses the CUDA
  * cores only (plane-owner kernel).  Tuning and testing support; no counterpart in the reference. */

@@ -106,3 +106,23 @@ def test_autotune_keeps_results():
     finally:
         c.close()
     assert np.linalg.norm(v1 - v0) <= 1e-12 * np.linalg.norm(v0)
+
+
+@pytest.mark.gpu
+def test_spread_autotune_keeps_results():
+    """The spreading autotuner picks a mode (tensor cores or CUDA cores) and the velocities stay those
+    of the default mode to the run-to-run order of the FP32 spreading sums."""
+    fs = configs.tangle(40, 100, seed=7)
+    p = configs.params_for(L / 8, 3.5, 64, 3, precision="mixed")
+    c = vp.init_cache(p)
+    try:
+        c.set_filaments(fs)
+        c.compute(_lib.VELOCITY)
+        v0 = c.get(_lib.VELOCITY)
+        m = timestepping.autotune_spread(c)
+        assert m in (0, 1)
+        c.compute(_lib.VELOCITY)
+        v1 = c.get(_lib.VELOCITY)
+    finally:
+        c.close()
+    assert np.linalg.norm(v1 - v0) <= 1e-6 * np.linalg.norm(v0)

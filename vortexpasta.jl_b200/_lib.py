@@ -99,6 +99,7 @@ SIGNATURES = {
     "vpbs_ensemble_destroy": (ct.c_int, [ct.c_void_p]),
     "vpbs_ensemble_last_error": (ct.c_char_p, []),
     "vpbs_autotune": (ct.c_int, [ct.c_void_p, c_int32_p]),
+    "vpbs_autotune_spread": (ct.c_int, [ct.c_void_p, c_int32_p]),
     "vpbs_pair_block": (ct.c_int, [ct.c_void_p, ct.c_int32]),
     "vpbs_spread_mode": (ct.c_int, [ct.c_void_p, ct.c_int32]),
     "vpbs_mlp_create": (ct.c_int, [ct.c_int32, ct.c_int32, ct.POINTER(ct.c_void_p)]),

@@ -5,7 +5,8 @@
   (vpbs_rk4_step; knots frozen inside the step as the reference's RK4 does).
 * ``Ensemble``: independent systems (any sizes and grids) advanced together; one RK4 step of all
   of them is captured in one CUDA graph and replayed with one launch per step
-  (vpbs_ensemble_*).  ``autotune=True`` first runs the pair-kernel autotuner on every system.
+  (vpbs_ensemble_*).  ``autotune_pairs=True`` first runs the pair-kernel and spreading autotuners
+  on every system.
 
 Device memory for the node arrays comes from torch (plumbing only); every kernel is the
 library's.
@@ -58,6 +59,14 @@ def autotune(cache: BiotSavartCache) -> int:
     return int(b.value)
 
 
+def autotune_spread(cache: BiotSavartCache) -> int:
+    """Pick the spreading mode for the loaded point data (vpbs_spread_mode: 0 tensor cores where they
+    apply, 1 CUDA cores only)."""
+    m = ct.c_int32()
+    _lib.check(cache._lib.vpbs_autotune_spread(cache.handle, ct.byref(m)), cache.handle, "autotune_spread")
+    return int(m.value)
+
+
 class Ensemble:
     """Independent filament systems advanced by RK4 with one CUDA-graph launch per step.
 
@@ -67,12 +76,13 @@ class Ensemble:
         import torch
         self._lib = _lib.load()
         self.device = int(device)
-        self.caches, self.nodes, self.layouts, self.tuned = [], [], [], []
+        self.caches, self.nodes, self.layouts, self.tuned, self.spread_modes = [], [], [], [], []
         for fs, p, dt in systems:
             c = init_cache(p.with_(device=self.device))
             c.set_filaments(fs)
             if autotune_pairs:
                 self.tuned.append(autotune(c))
+                self.spread_modes.append(autotune_spread(c))
             nodes, offsets = curves.concat(fs)
             self.nodes.append(torch.from_numpy(nodes).to(torch.device("cuda", self.device)))
             self.layouts.append(offsets)
