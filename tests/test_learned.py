@@ -180,3 +180,35 @@ def test_kaiser_bessel_variants_parameters():
         assert k.as_dict()["splitting"] == "kaiser_bessel"
     again = learned.kaiser_bessel_variants(tuning.EwaldChoice(alpha=20.0, rcut=L / 40, Ns=300, sigma=1.5, m=3), L, 1e-5)
     assert len(again) == 2  # (1.5, 3) predicted and in KB_NUFFT: one candidate
+
+
+def test_choice_cache_classes_and_roundtrip(tmp_path):
+    """The checked-choice cache: configurations whose features round to the same class share an entry,
+    distinct node counts, rtol or a shifted nearest-distance histogram do not, and both kinds of
+    choice survive the JSON file."""
+    L = 2 * math.pi
+    hist = np.array([0, 1, 3, 8, 20, 30, 20, 8, 3, 1, 0, 0], dtype=np.float64)
+    f = np.concatenate([[6.0, 2.1, -2.5, -3.0], hist])
+    g = f.copy()
+    g[0] += 0.02  # 5 % more nodes: same class
+    key = learned.ChoiceCache.key
+    assert key(f, L, 1e-5) == key(g, L, 1e-5)
+    assert key(f, L, 1e-5) != key(f, L, 1e-6)
+    h = f.copy()
+    h[0] += 0.3  # 2x the nodes
+    assert key(f, L, 1e-5) != key(h, L, 1e-5)
+    s = f.copy()
+    s[4:] = np.roll(hist, 2)
+    assert key(f, L, 1e-5) != key(s, L, 1e-5)
+    path = tmp_path / "choices.json"
+    c = learned.ChoiceCache(path)
+    assert c.get(f, L, 1e-5) is None
+    kb = tuning.kb_choice_from(L, L / 45, 12.44, 1.5, 3)
+    ga = tuning.default_rule(L, 1e-5, L / 16)
+    c.put(f, L, 1e-5, kb, 7e-6, False)
+    c.put(h, L, 1e-5, ga, None, True)
+    c2 = learned.ChoiceCache(path)
+    ch, e = c2.get(g, L, 1e-5)
+    assert ch == kb and e["rel_l2"] == 7e-6 and not e["fallback"]
+    ch, e = c2.get(h, L, 1e-5)
+    assert ch == ga and e["fallback"]

@@ -1,6 +1,7 @@
 """Build the learned parameter predictor (predictor.npz beside this script).
 
-    python make_predictor.py generate N SEED OUT.npz      # sweep N random tangles (GPU)
+    python make_predictor.py generate N SEED OUT.npz [reduced MAX_SECONDS MIN_NODES MAX_NODES]
+                                                          # sweep N random tangles (GPU)
     python make_predictor.py train OUT.npz DS.npz [...]   # train on the GPU with the library's MLP kernels
     python make_predictor.py evaluate MODEL.npz N SEED OUT.json   # held-out tangles: predictor vs default rule
 
@@ -36,12 +37,15 @@ def load_package():
     return mod
 
 
-def generate(n, seed, out):
+def generate(n, seed, out, reduced=False, max_seconds=None, min_nodes=5_000, max_nodes=1_200_000):
     load_package()
     from vortexpasta_b200 import learned
     t0 = time.time()
-    d = learned.generate_dataset(n, seed, log=lambda s: print(f"[{time.time() - t0:7.1f}s] {s}", flush=True))
+    d = learned.generate_dataset(n, seed, log=lambda s: print(f"[{time.time() - t0:7.1f}s] {s}", flush=True),
+                                 reduced=reduced, deadline=t0 + max_seconds if max_seconds else None,
+                                 checkpoint=lambda ds: np.savez(out, **ds), min_nodes=min_nodes, max_nodes=max_nodes)
     np.savez(out, **d)
+    print(f"{len(d['X'])} configurations in {time.time() - t0:.0f} s", flush=True)
 
 
 def train(out, paths, steps=6000, lr=3e-3, seed=0):
@@ -92,7 +96,12 @@ def evaluate(model, n, seed, out):
 if __name__ == "__main__":
     cmd = sys.argv[1]
     if cmd == "generate":
-        generate(int(sys.argv[2]), int(sys.argv[3]), sys.argv[4])
+        # optional: reduced  MAX_SECONDS  MIN_NODES  MAX_NODES
+        extra = sys.argv[5:]
+        generate(int(sys.argv[2]), int(sys.argv[3]), sys.argv[4], reduced=bool(extra and extra[0] == "reduced"),
+                 max_seconds=float(extra[1]) if len(extra) > 1 else None,
+                 min_nodes=int(extra[2]) if len(extra) > 2 else 5_000,
+                 max_nodes=int(extra[3]) if len(extra) > 3 else 1_200_000)
     elif cmd == "train":
         train(sys.argv[2], sys.argv[3:])
     elif cmd == "evaluate":

@@ -228,19 +228,41 @@ def sweep_configuration(fs, L: float, choices, rtol: float = 1e-5):
     return feats, recs, best, d
 
 
-def training_choices(L: float):
-    return tuning.candidate_grid(L, rcut_fracs=(1 / 12, 1 / 16, 1 / 20, 1 / 24, 1 / 32, 1 / 40, 1 / 48, 1 / 56),
-                                 betas=(2.95, 3.15, 3.35), sigma_m=((1.25, 4), (1.5, 3), (2.0, 3)))
+RCUT_FRACS = (1 / 12, 1 / 16, 1 / 20, 1 / 24, 1 / 32, 1 / 40, 1 / 48, 1 / 56)
+
+
+def training_choices(L: float, reduced: bool = False):
+    """The sweep grid: 8 cut-offs x 3 betas x 3 NUFFT (sigma, m) (72 sets), or with `reduced` the
+    32 sets of the betas and NUFFTs that won most often on the full grid (betas 3.15 and 3.35;
+    (sigma, m) = (1.5, 3) and (1.25, 4): 90 % of the 150 labels of the first data set)."""
+    if reduced:
+        return tuning.candidate_grid(L, rcut_fracs=RCUT_FRACS, betas=(3.15, 3.35), sigma_m=((1.25, 4), (1.5, 3)))
+    return tuning.candidate_grid(L, rcut_fracs=RCUT_FRACS, betas=(2.95, 3.15, 3.35),
+                                 sigma_m=((1.25, 4), (1.5, 3), (2.0, 3)))
 
 
 def generate_dataset(n: int, seed: int, L: float = 2 * math.pi, rtol: float = 1e-5, min_nodes: int = 5_000,
-                     max_nodes: int = 1_200_000, log=None) -> dict:
+                     max_nodes: int = 1_200_000, log=None, reduced: bool = False, deadline: float | None = None,
+                     checkpoint=None, checkpoint_every: int = 25) -> dict:
     """(features, label) pairs of `n` random configurations from parameter sweeps against the
-    FP64 reference, with the default rule's cost and error for comparison."""
+    FP64 reference, with the default rule's cost and error for comparison.  Stops early at the
+    wall-clock `deadline` (time.time() value); `checkpoint(dataset)` is called every
+    `checkpoint_every` configurations."""
+    import time as _time
     rng = np.random.default_rng(seed)
-    choices = training_choices(L)
+    choices = training_choices(L, reduced)
     X, Y, nodes, best_ms, default_ms, default_err = [], [], [], [], [], []
+
+    def pack():
+        return {"X": np.array(X, dtype=np.float32), "Y": np.array(Y), "nodes": np.array(nodes),
+                "best_ms": np.array(best_ms), "default_ms": np.array(default_ms),
+                "default_err": np.array(default_err), "rtol": rtol, "L": L}
+
     for k in range(n):
+        if deadline is not None and _time.time() > deadline:
+            break
+        if checkpoint is not None and k > 0 and k % checkpoint_every == 0:
+            checkpoint(pack())
         fs = random_configuration(rng, L, min_nodes, max_nodes)
         feats, recs, best, d = sweep_configuration(fs, L, choices, rtol)
         if best is None:
@@ -255,9 +277,7 @@ def generate_dataset(n: int, seed: int, L: float = 2 * math.pi, rtol: float = 1e
         if log:
             log(f"{k}: N={nodes[-1]} best {best['ms']:.2f} ms (rcut L/{L / best['rcut']:.0f}, fft {best['fft']}, "
                 f"m {best['m']}) default {d['ms']:.2f} ms err {d['rel_l2']:.1e}")
-    return {"X": np.array(X, dtype=np.float32), "Y": np.array(Y), "nodes": np.array(nodes),
-            "best_ms": np.array(best_ms), "default_ms": np.array(default_ms), "default_err": np.array(default_err),
-            "rtol": rtol, "L": L}
+    return pack()
 
 
 def train(X, Y, rtol: float, steps: int = 1000, lr: float = 1e-3, weight_decay: float = 1e-2, seed: int = 0,
@@ -305,18 +325,70 @@ def kaiser_bessel_variants(ch: tuning.EwaldChoice, L: float, rtol: float) -> lis
     return out
 
 
+class ChoiceCache:
+    """Checked parameter choices per configuration class, so that a solver meeting similar
+    configurations again (the steps of one simulation, an ensemble of similar tangles) pays the FP64
+    check once per class instead of once per call.
+
+    The class of a configuration: L, rtol and its features rounded -- log10 N and log10(line length /
+    L^2) to 1/8 (steps of 33 %), log10 of the mean and minimum chord / L to 1/4, and the bin holding
+    the median of the nearest-distance histogram.  With `path`, entries are read from and written to
+    that JSON file."""
+
+    def __init__(self, path: str | Path | None = None):
+        import json
+        self.path = Path(path) if path else None
+        self.entries: dict[str, dict] = {}
+        if self.path and self.path.exists():
+            self.entries = json.loads(self.path.read_text())
+
+    @staticmethod
+    def key(feats, L: float, rtol: float) -> str:
+        f = np.asarray(feats, dtype=np.float64).ravel()
+        hist = f[4:]
+        cum = np.cumsum(hist)
+        median_bin = int(np.searchsorted(cum, 0.5 * cum[-1])) if cum[-1] > 0 else -1
+        parts = [round(L, 9), float(f"{rtol:.3e}"), int(round(8 * f[0])), int(round(8 * f[1])),
+                 int(round(4 * f[2])), int(round(4 * f[3])), median_bin]
+        return "/".join(str(x) for x in parts)
+
+    def get(self, feats, L: float, rtol: float):
+        e = self.entries.get(self.key(feats, L, rtol))
+        if e is None:
+            return None
+        d = dict(e["choice"])
+        if d.pop("splitting", "gaussian") == "kaiser_bessel":
+            return tuning.KBChoice(**d), e
+        return tuning.EwaldChoice(**d), e
+
+    def put(self, feats, L: float, rtol: float, choice, rel_l2, fallback: bool) -> None:
+        import json
+        self.entries[self.key(feats, L, rtol)] = {"choice": choice.as_dict(), "rel_l2": rel_l2,
+                                                  "fallback": bool(fallback)}
+        if self.path:
+            self.path.write_text(json.dumps(self.entries, indent=1))
+
+
 def choose_parameters(fs, L: float, rtol: float = 1e-5, predictor: Predictor | None = None, check: bool = True,
-                      device: int = 0, kaiser_bessel: bool = True):
+                      device: int = 0, kaiser_bessel: bool = True, cache: ChoiceCache | None = None):
     """Predicted parameters for `fs` at tolerance `rtol`.  With `check`, a plain FP64 evaluation
     judges the prediction (mixed form); a rejected prediction is retried once with larger betas,
     and the default rule replaces it when that also misses rtol.  With `kaiser_bessel`, the
     Kaiser-Bessel splits at the accepted cut-off (``kaiser_bessel_variants``) are judged the same
-    way and the fastest choice meeting rtol is kept.  Returns (choice, info)."""
+    way and the fastest choice meeting rtol is kept.  With `cache`, a checked choice of the same
+    configuration class is returned without a new check (info["cached"]), and a new checked
+    choice is stored.  Returns (choice, info)."""
     pred = predictor or Predictor.load()
     feats = features_of(fs, L, device)
+    if cache is not None and check:
+        hit = cache.get(feats, L, rtol)
+        if hit is not None:
+            ch, e = hit
+            return ch, {"features": feats, "predicted": None, "attempts": [], "fallback": e["fallback"],
+                        "rel_l2": e["rel_l2"], "cached": True}
     y = pred.outputs(feats)[0]
     ch = choice_of(y, L, BETA_SHIFT)
-    info = {"features": feats, "outputs": y, "predicted": ch, "attempts": [], "fallback": False}
+    info = {"features": feats, "outputs": y, "predicted": ch, "attempts": [], "fallback": False, "cached": False}
     if not check:
         return ch, info
     vref = reference_velocity(fs, L, device)
@@ -332,6 +404,8 @@ def choose_parameters(fs, L: float, rtol: float = 1e-5, predictor: Predictor | N
     if accepted is None:
         info["fallback"] = True
         ch = tuning.default_rule(L, rtol, FEATURE_RCUT * L)
+        if cache is not None:
+            cache.put(feats, L, rtol, ch, None, True)
         return ch, info
     if kaiser_bessel:
         for kb in kaiser_bessel_variants(accepted[0], L, rtol):
@@ -341,4 +415,6 @@ def choose_parameters(fs, L: float, rtol: float = 1e-5, predictor: Predictor | N
             if err <= rtol and ms < accepted[2]:
                 accepted = (kb, err, ms)
     info["rel_l2"] = accepted[1]
+    if cache is not None:
+        cache.put(feats, L, rtol, accepted[0], accepted[1], False)
     return accepted[0], info
