@@ -263,3 +263,19 @@ def test_host_copy_threads_after_fork(built_lib):
         p.kill()
     assert not alive and p.exitcode == 0
     assert q.get(timeout=5)
+
+
+def test_destroy_frees_every_device_buffer():
+    """Every device buffer of the handle (a DevBuf member in vpbs_internal.cuh) is in vpbs_destroy's
+    list of buffers to free: a buffer left out leaks device memory on every create / destroy cycle."""
+    csrc = Path(__file__).resolve().parents[1] / "vortexpasta.jl_b200" / "csrc"
+    header = (csrc / "vpbs_internal.cuh").read_text()
+    names = []
+    for m in re.finditer(r"vpbs::DevBuf ([^;]+);", header):
+        names += [x.strip() for x in m.group(1).split(",")]
+    assert len(names) > 40
+    api = (csrc / "api.cu").read_text()
+    i = api.index("DevBuf* bufs[] = {")
+    listed = api[i:api.index("};", i)]
+    missing = [n for n in names if f"&h->{n}" not in listed]
+    assert not missing, f"not freed by vpbs_destroy: {missing}"

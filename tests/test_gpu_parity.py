@@ -336,3 +336,30 @@ def test_split_devices_match_single_handle(vp, built_lib, precision):
     assert rel(np.concatenate(vs), v1) < tol and rel(np.concatenate(ps), p1) < tol
     vo, _, _ = gpu_fields(vp, p, fs, LIA="only")
     assert rel(np.concatenate(vl), vo) < 1e-14
+
+
+def test_handles_release_device_memory(vp, built_lib):
+    """Create / evaluate / read back / destroy cycles leave the device's free memory where it was
+    (no buffer of the handle outlives it)."""
+    import torch
+    from vortexpasta_b200 import _lib
+    fs, p = vp.configs.tangle20k(precision="mixed")
+
+    def cycle():
+        c = vp.init_cache(p)
+        try:
+            c.set_filaments(fs)
+            c.compute(_lib.VELOCITY | _lib.STREAMFUNCTION)
+            c.get(_lib.VELOCITY)
+            c.get(_lib.STREAMFUNCTION)
+        finally:
+            c.close()
+
+    cycle()  # first use: module loading, library workspaces
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(10):
+        cycle()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free0 - free1 < 16 << 20, f"{(free0 - free1) / 2**20:.1f} MiB not released after 10 cycles"

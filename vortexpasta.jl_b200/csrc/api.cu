@@ -354,7 +354,8 @@ int vpbs_destroy(vpbs_handle* h) {
                       &h->src_seg, &h->dst_cell, &h->dst_start, &h->dst_fill, &h->dst_order, &h->counters,
                       &h->grid_r, &h->grid_c, &h->grid_c2, &h->uhat, &h->decx, &h->decy, &h->decz, &h->nodes_lr,
                       &h->vel, &h->psi, &h->spread_bin, &h->spread_counts, &h->spread_start, &h->binned,
-                      &h->spread_foot, &h->tc_counts, &h->tc_start, &h->tc_rec, &h->peer_in, &h->ewald_tab, &h->scan_tmp, &h->scan_tmp_lr, &h->rk_vs, &h->rk_tmp};
+                      &h->spread_foot, &h->tc_counts, &h->tc_start, &h->tc_rec, &h->peer_in, &h->ewald_tab, &h->scan_tmp, &h->scan_tmp_lr, &h->rk_vs, &h->rk_tmp,
+                      &h->aos_out, &h->fil_off};
     for (DevBuf* b : bufs) free_buf(*b);
     if (h->pin_in) cudaFreeHost(h->pin_in);
     if (h->status_host) cudaFreeHost(h->status_host);
@@ -718,6 +719,14 @@ int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t short
     // timing on, everything runs in order on the main stream so that each stage is timed alone.
     cudaStream_t main = h->stream;
     const bool fork = with_long && !h->timing;
+#ifdef VPBS_SPREAD_FIRST
+    if (fork) {
+        h->lr_part = 1;
+        rc = longrange_compute(h, fields);
+        h->lr_part = 0;
+        if (rc) return rc;
+    }
+#endif
     if (fork) {
         if ((rc = check_cuda(h, cudaEventRecord(h->ev_fork, main), "fork"))) return rc;
         if ((rc = check_cuda(h, cudaStreamWaitEvent(h->aux_stream, h->ev_fork, 0), "fork"))) return rc;
@@ -738,7 +747,11 @@ int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t short
         if ((rc = check_cuda(h, cudaEventRecord(h->ev_short, main), "short done"))) return rc;
         h->stream = h->aux_stream;
         h->interp_wait = h->ev_short;
+#ifdef VPBS_SPREAD_FIRST
+        h->lr_part = 2;
+#endif
         rc = longrange_compute(h, fields);
+        h->lr_part = 0;
         h->interp_wait = nullptr;
         h->stream = main;
         if (rc) return rc;

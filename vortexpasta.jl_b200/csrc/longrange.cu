@@ -95,6 +95,23 @@ __device__ __forceinline__ int wrapi(int i, int n) {
     return i < 0 ? i + n : i;
 }
 
+// i mod n for i in [-n, 2n) (a footprint index: n >= 2m grid points), without a division.
+__device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// es_kernel for a compile-time width W = 2m: u / m as a product with the constant 2 / W.
+template <int W>
+__device__ __forceinline__ double es_kernel_w(double u, double beta, double edge, int kind) {
+    constexpr double inv_m = 2.0 / W;
+    const double z = u * inv_m;
+    const double s = 1.0 - z * z;
+    if (!(s > 0.0)) return 0.0;
+    if (kind == VPBS_NUFFT_KAISER_BESSEL) {
+        const double r = sqrt(s);
+        return (r > 1e-12 ? sinh(beta * r) / (r * sinh(beta)) : beta / sinh(beta)) - edge;
+    }
+    return exp(beta * (sqrt(s) - 1.0)) - edge;
+}
+
 constexpr int kSpreadBatch = 32;
 
 // Complex value of the grid precision T from double parts.
@@ -612,7 +629,7 @@ __global__ void __launch_bounds__(128) tc_rec_scatter_kernel(LRSizes S, int nb0,
         const int i0 = (int)floor(xh) - S.m + 1;
         f[d] = wrapi(i0, S.n[d]);
 #pragma unroll
-        for (int s = 0; s < W; ++s) r[4 + d * W + s] = (float)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge, S.kernel);
+        for (int s = 0; s < W; ++s) r[4 + d * W + s] = (float)es_kernel_w<W>(xh - (i0 + s), S.beta, S.edge, S.kernel);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) r[c] = (float)src[(3 + c) * Nq + j];
@@ -1019,8 +1036,8 @@ __global__ void __launch_bounds__(256) interp_warp_kernel(
         const double scale = d == 0 ? sx0 : (d == 1 ? sx1 : sx2);
         const double xh = (nodes[d * Np + i] * scale) / (2.0 * kPi / S.n[d]);
         const int i0 = (int)floor(xh) - S.m + 1;
-        phs[warp][d][s] = (T)es_kernel(xh - (i0 + s), S.m, S.beta, S.edge, S.kernel);
-        ixs[warp][d][s] = wrapi(i0 + s, S.n[d]);
+        phs[warp][d][s] = (T)es_kernel_w<W>(xh - (i0 + s), S.beta, S.edge, S.kernel);
+        ixs[warp][d][s] = wrap1(i0 + s, S.n[d]);
     }
     __syncwarp();
     const int64_t ng = S.ngrid, n0 = S.n[0], n1 = S.n[1];
@@ -1168,7 +1185,9 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
     C* gc2 = (C*)h->grid_c2.p;
     // sources: cell-sorted copy (SoA x,y,z,qx,qy,qz), built by build_cell_lists
     const double* src = (const double*)h->src_sorted.p;
-    if (h->gatherB) {
+    if (h->lr_part == 2) {
+        // the spreading ran already (lr_part 1)
+    } else if (h->gatherB) {
         StageScope st(h, ST_SPREAD);
         const int B = h->gatherB, nb0 = h->nbrick[0], nb1 = h->nbrick[1], nb2 = h->nbrick[2];
         const int64_t nbins = (int64_t)nb0 * nb1 * nb2, Nq = h->Nq;
@@ -1270,6 +1289,7 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
         h->launches++;
         if ((rc = check_cuda(h, cudaGetLastError(), "spread kernel"))) return rc;
     }
+    if (h->lr_part == 1) return 0;
     {
         StageScope st(h, ST_FFT_FORWARD);
         if ((rc = check_fft(h, cufftSetStream(h->plan_r2c, h->stream), "set stream"))) return rc;
