@@ -719,14 +719,6 @@ int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t short
     // timing on, everything runs in order on the main stream so that each stage is timed alone.
     cudaStream_t main = h->stream;
     const bool fork = with_long && !h->timing;
-#ifdef VPBS_SPREAD_FIRST
-    if (fork) {
-        h->lr_part = 1;
-        rc = longrange_compute(h, fields);
-        h->lr_part = 0;
-        if (rc) return rc;
-    }
-#endif
     if (fork) {
         if ((rc = check_cuda(h, cudaEventRecord(h->ev_fork, main), "fork"))) return rc;
         if ((rc = check_cuda(h, cudaStreamWaitEvent(h->aux_stream, h->ev_fork, 0), "fork"))) return rc;
@@ -747,11 +739,7 @@ int vpbs_compute(vpbs_handle* h, int32_t fields, int32_t lia_mode, int32_t short
         if ((rc = check_cuda(h, cudaEventRecord(h->ev_short, main), "short done"))) return rc;
         h->stream = h->aux_stream;
         h->interp_wait = h->ev_short;
-#ifdef VPBS_SPREAD_FIRST
-        h->lr_part = 2;
-#endif
         rc = longrange_compute(h, fields);
-        h->lr_part = 0;
         h->interp_wait = nullptr;
         h->stream = main;
         if (rc) return rc;

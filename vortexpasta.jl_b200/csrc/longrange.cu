@@ -1185,9 +1185,7 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
     C* gc2 = (C*)h->grid_c2.p;
     // sources: cell-sorted copy (SoA x,y,z,qx,qy,qz), built by build_cell_lists
     const double* src = (const double*)h->src_sorted.p;
-    if (h->lr_part == 2) {
-        // the spreading ran already (lr_part 1)
-    } else if (h->gatherB) {
+    if (h->gatherB) {
         StageScope st(h, ST_SPREAD);
         const int B = h->gatherB, nb0 = h->nbrick[0], nb1 = h->nbrick[1], nb2 = h->nbrick[2];
         const int64_t nbins = (int64_t)nb0 * nb1 * nb2, Nq = h->Nq;
@@ -1289,7 +1287,6 @@ int longrange_compute_t(vpbs_handle* h, int fields) {
         h->launches++;
         if ((rc = check_cuda(h, cudaGetLastError(), "spread kernel"))) return rc;
     }
-    if (h->lr_part == 1) return 0;
     {
         StageScope st(h, ST_FFT_FORWARD);
         if ((rc = check_fft(h, cufftSetStream(h->plan_r2c, h->stream), "set stream"))) return rc;

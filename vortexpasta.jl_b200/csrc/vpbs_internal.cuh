@@ -179,7 +179,6 @@ struct vpbs_handle {
     cudaEvent_t xfer_done = nullptr;            // vpbs_add_field: this handle's fields are complete
     int gatherB = 0;   // brick edge of the atomic-free spreading (0: atomic fallback)
     int spread_mode = 0;  // 0: tensor-core spreading where it applies; 1: CUDA-core kernels only
-    int lr_part = 0;      // longrange_compute: 0 everything, 1 the spreading only, 2 everything after it
     int* status_host = nullptr;  // mapped pinned word: device-side faults of bounded waits (0: none)
     int* status_dev = nullptr;
     int nbrick[3] = {0, 0, 0};
