@@ -527,8 +527,13 @@ __global__ void __launch_bounds__(128) quad_points_kernel(
 
 // Shared-memory work space of the spline solve for filaments of at most nmax nodes (4 warps per
 // block, 12 doubles per node each); 0 when it does not fit and the global scratch is used.
+// Filaments (warps) per spline-solve block: with 2, a 200-node filament's 19 KB of work space per warp
+// lets 5 blocks (10 warps) share an SM; with 4, 2 blocks (8 warps) fit (1M nodes: 0.61 vs 0.66 ms for
+// the geometry).
+constexpr int kSolveWarps = 2;
+
 static int solve_smem_n(int64_t nmax, size_t* bytes) {
-    const size_t b = (size_t)4 * 12 * nmax * sizeof(double);
+    const size_t b = (size_t)kSolveWarps * 12 * nmax * sizeof(double);
     if (nmax > 0 && b <= 200 * 1024) {
         *bytes = b;
         return (int)nmax;
@@ -561,7 +566,7 @@ int geometry_from_filaments(vpbs_handle* h, int64_t nfil, const int64_t* d_offse
     const double* foff = h->have_fil_offsets ? (const double*)h->fil_off.p : nullptr;
     StageScope st(h, ST_GEOMETRY);
     if ((rc = check_cuda(h, cudaMemsetAsync(status, 0, sizeof(int32_t), h->stream), "memset"))) return rc;
-    spline_solve_kernel<<<grid_for(nfil, 4), 128, smem_bytes, h->stream>>>(
+    spline_solve_kernel<<<grid_for(nfil, kSolveWarps), 32 * kSolveWarps, smem_bytes, h->stream>>>(
         nfil, d_offsets, d_nodes, knots, periods, (int32_t*)h->fil_of_node.p, (double*)h->coefs.p,
         (double*)h->dcoef1.p, (double*)h->dcoef2.p, (double*)h->spline_scratch.p, status, smem_n, keep_knots ? 1 : 0,
         foff);
