@@ -285,7 +285,7 @@ def test_host_entry_points_agree(vp):
 
 
 @pytest.mark.parametrize("sigma,m,kernel", [(1.5, 3, "es"), (1.5, 4, "es"), (2.0, 2, "es"), (1.25, 3, "es"),
-                                            (1.5, 4, "kaiser_bessel")])
+                                            (1.5, 4, "kaiser_bessel"), (2.0, 1, "es")])
 def test_tensor_core_spreading(vp, oracle, built_lib, sigma, m, kernel):
     """Mixed form: the tensor-core brick product (tcgen05, 3xTF32) against the CUDA-core plane
     kernel and the oracle -- vorticity coefficients (the spread grid after the forward FFT) and
