@@ -292,7 +292,7 @@ int vpbs_periodic_eval(double L, int32_t nc, const double* x, int64_t n, double*
 
 /* Host copies dst[k] <- src[k] of bytes[k] each (k < n) on the library's copy threads, the routine the
  * host-buffer entry points stage their inputs and outputs with: blocks split into pieces of about
- * 1 MB, small blocks grouped, a pool of up to 15 threads plus the caller (created on first use, and
+ * 1 MB, small blocks grouped, a pool of up to 7 threads plus the caller (created on first use, and
  * again in a forked child).  Host memory only; no GPU needed.  Exists to test the staging; no
  * counterpart in the reference. */
 int vpbs_host_copies(int64_t n, void* const* dst, const void* const* src, const size_t* bytes);

@@ -457,7 +457,7 @@ CopyPool& copy_pool() {
     std::lock_guard<std::mutex> lk(mu);
     if (!pool || pool->pid != getpid()) {
         const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-        pool = new CopyPool((int)std::min(15u, hw > 1 ? hw - 1 : 1u));  // lives until the process ends
+        pool = new CopyPool((int)std::min(7u, hw > 1 ? hw - 1 : 1u));  // lives until the process ends
     }
     return *pool;
 }
