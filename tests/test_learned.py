@@ -183,32 +183,36 @@ def test_kaiser_bessel_variants_parameters():
 
 
 def test_choice_cache_classes_and_roundtrip(tmp_path):
-    """The checked-choice cache: configurations whose features round to the same class share an entry,
-    distinct node counts, rtol or a shifted nearest-distance histogram do not, and both kinds of
-    choice survive the JSON file."""
+    """The checked-choice cache: configurations whose host class features round to the same class
+    share an entry, twice the nodes or another rtol do not, and both kinds of choice survive the JSON
+    file.  The class features are those of the tangle (node count, line length, chords), computed on
+    the host."""
     L = 2 * math.pi
-    hist = np.array([0, 1, 3, 8, 20, 30, 20, 8, 3, 1, 0, 0], dtype=np.float64)
-    f = np.concatenate([[6.0, 2.1, -2.5, -3.0], hist])
-    g = f.copy()
-    g[0] += 0.02  # 5 % more nodes: same class
+    fs = configs.tangle(50, 100, seed=3)
+    cf = learned.class_features(fs, L)
+    n = sum(len(f) for f in fs)
+    assert cf[0] == pytest.approx(math.log10(n))
+    chords = np.concatenate([np.linalg.norm(np.roll(f, -1, axis=0) - f, axis=1) for f in fs])
+    assert cf[1] == pytest.approx(math.log10(chords.sum() / L ** 2))
+    assert cf[3] == pytest.approx(math.log10(chords.min() / L))
+    moved = [f + 0.01 for f in fs]  # a translated tangle: same class
     key = learned.ChoiceCache.key
-    assert key(f, L, 1e-5) == key(g, L, 1e-5)
-    assert key(f, L, 1e-5) != key(f, L, 1e-6)
-    h = f.copy()
-    h[0] += 0.3  # 2x the nodes
-    assert key(f, L, 1e-5) != key(h, L, 1e-5)
-    s = f.copy()
-    s[4:] = np.roll(hist, 2)
-    assert key(f, L, 1e-5) != key(s, L, 1e-5)
+    assert key(learned.class_features(moved, L), L, 1e-5) == key(cf, L, 1e-5)
+    assert key(cf, L, 1e-5) != key(cf, L, 1e-6)
+    double = configs.tangle(100, 100, seed=3)
+    cf2 = learned.class_features(double, L)
+    assert key(cf, L, 1e-5) != key(cf2, L, 1e-5)
+    line = vp.curves.periodic_line(64, L, x=1.0, y=2.0)  # closing chord across the end-to-end offset
+    assert learned.class_features([line], L)[3] == pytest.approx(math.log10(1 / 64), abs=1e-9)
     path = tmp_path / "choices.json"
     c = learned.ChoiceCache(path)
-    assert c.get(f, L, 1e-5) is None
+    assert c.get(cf, L, 1e-5) is None
     kb = tuning.kb_choice_from(L, L / 45, 12.44, 1.5, 3)
     ga = tuning.default_rule(L, 1e-5, L / 16)
-    c.put(f, L, 1e-5, kb, 7e-6, False)
-    c.put(h, L, 1e-5, ga, None, True)
+    c.put(cf, L, 1e-5, kb, 7e-6, False)
+    c.put(cf2, L, 1e-5, ga, None, True)
     c2 = learned.ChoiceCache(path)
-    ch, e = c2.get(g, L, 1e-5)
+    ch, e = c2.get(learned.class_features(moved, L), L, 1e-5)
     assert ch == kb and e["rel_l2"] == 7e-6 and not e["fallback"]
-    ch, e = c2.get(h, L, 1e-5)
+    ch, e = c2.get(cf2, L, 1e-5)
     assert ch == ga and e["fallback"]

@@ -325,15 +325,30 @@ def kaiser_bessel_variants(ch: tuning.EwaldChoice, L: float, rtol: float) -> lis
     return out
 
 
+def class_features(fs, L: float) -> np.ndarray:
+    """Host-side summary of a configuration for ChoiceCache (numpy, no GPU): log10 N,
+    log10(line length / L^2), log10 of the mean and the minimum chord / L (closing chords included;
+    an unclosed filament's closing chord runs to its first node plus the end-to-end offset)."""
+    n, total, cmin = 0, 0.0, math.inf
+    for f in fs:
+        x = np.asarray(f, dtype=np.float64)
+        nxt = np.roll(x, -1, axis=0)
+        nxt[-1] = nxt[-1] + curves.end_to_end_offset(f)
+        d = np.linalg.norm(nxt - x, axis=1)
+        n += len(x)
+        total += float(d.sum())
+        cmin = min(cmin, float(d.min()))
+    return np.array([math.log10(n), math.log10(total / L ** 2), math.log10(total / n / L), math.log10(cmin / L)])
+
+
 class ChoiceCache:
     """Checked parameter choices per configuration class, so that a solver meeting similar
     configurations again (the steps of one simulation, an ensemble of similar tangles) pays the FP64
-    check once per class instead of once per call.
+    check once per class instead of once per call; a lookup costs a numpy pass over the nodes.
 
-    The class of a configuration: L, rtol and its features rounded -- log10 N and log10(line length /
-    L^2) to 1/8 (steps of 33 %), log10 of the mean and minimum chord / L to 1/4, and the bin holding
-    the median of the nearest-distance histogram.  With `path`, entries are read from and written to
-    that JSON file."""
+    The class of a configuration: L, rtol and its ``class_features`` rounded -- log10 N and
+    log10(line length / L^2) to 1/8 (steps of 33 %), log10 of the mean and minimum chord / L to 1/4.
+    With `path`, entries are read from and written to that JSON file."""
 
     def __init__(self, path: str | Path | None = None):
         import json
@@ -343,13 +358,10 @@ class ChoiceCache:
             self.entries = json.loads(self.path.read_text())
 
     @staticmethod
-    def key(feats, L: float, rtol: float) -> str:
-        f = np.asarray(feats, dtype=np.float64).ravel()
-        hist = f[4:]
-        cum = np.cumsum(hist)
-        median_bin = int(np.searchsorted(cum, 0.5 * cum[-1])) if cum[-1] > 0 else -1
+    def key(cf, L: float, rtol: float) -> str:
+        f = np.asarray(cf, dtype=np.float64).ravel()
         parts = [round(L, 9), float(f"{rtol:.3e}"), int(round(8 * f[0])), int(round(8 * f[1])),
-                 int(round(4 * f[2])), int(round(4 * f[3])), median_bin]
+                 int(round(4 * f[2])), int(round(4 * f[3]))]
         return "/".join(str(x) for x in parts)
 
     def get(self, feats, L: float, rtol: float):
@@ -378,14 +390,15 @@ def choose_parameters(fs, L: float, rtol: float = 1e-5, predictor: Predictor | N
     way and the fastest choice meeting rtol is kept.  With `cache`, a checked choice of the same
     configuration class is returned without a new check (info["cached"]), and a new checked
     choice is stored.  Returns (choice, info)."""
-    pred = predictor or Predictor.load()
-    feats = features_of(fs, L, device)
+    cf = class_features(fs, L) if cache is not None else None
     if cache is not None and check:
-        hit = cache.get(feats, L, rtol)
+        hit = cache.get(cf, L, rtol)
         if hit is not None:
             ch, e = hit
-            return ch, {"features": feats, "predicted": None, "attempts": [], "fallback": e["fallback"],
+            return ch, {"features": None, "predicted": None, "attempts": [], "fallback": e["fallback"],
                         "rel_l2": e["rel_l2"], "cached": True}
+    pred = predictor or Predictor.load()
+    feats = features_of(fs, L, device)
     y = pred.outputs(feats)[0]
     ch = choice_of(y, L, BETA_SHIFT)
     info = {"features": feats, "outputs": y, "predicted": ch, "attempts": [], "fallback": False, "cached": False}
@@ -405,7 +418,7 @@ def choose_parameters(fs, L: float, rtol: float = 1e-5, predictor: Predictor | N
         info["fallback"] = True
         ch = tuning.default_rule(L, rtol, FEATURE_RCUT * L)
         if cache is not None:
-            cache.put(feats, L, rtol, ch, None, True)
+            cache.put(cf, L, rtol, ch, None, True)
         return ch, info
     if kaiser_bessel:
         for kb in kaiser_bessel_variants(accepted[0], L, rtol):
@@ -416,5 +429,5 @@ def choose_parameters(fs, L: float, rtol: float = 1e-5, predictor: Predictor | N
                 accepted = (kb, err, ms)
     info["rel_l2"] = accepted[1]
     if cache is not None:
-        cache.put(feats, L, rtol, accepted[0], accepted[1], False)
+        cache.put(cf, L, rtol, accepted[0], accepted[1], False)
     return accepted[0], info
