@@ -577,7 +577,7 @@ constexpr int kTcKB = 16;      // points per batch: two K-steps of 8
 constexpr int kTcChunk = 128;  // records per bulk copy (a multiple of kTcKB: batches never straddle chunks)
 constexpr int kTcBatchesPerChunk = kTcChunk / kTcKB;
 constexpr int kTcRecMax = 28;  // floats per record for w <= 8
-constexpr int kTcBuilderWarps = 7;  // warps 1-4 write A, warps 5-7 write B
+constexpr int kTcBuilderWarps = 7;  // warps 1..W/2 write A, the others B
 constexpr uint32_t kTcWaitLimit = 1u << 26;
 
 // floats per record: charges (3), packed corner (1), 3 kernel rows of w values, padded to 16 bytes
@@ -661,7 +661,6 @@ struct TcSpreadSmem {
     float A[2][2][256 * kTcKB];
     float B[2][2][48 * kTcKB];
     float pts[2][kTcChunk * kTcRecMax];  // records of the current and the next chunk
-    int16_t held[2][kTcKB][2];           // (x, y) corner of the footprint each stage's A holds per slot (64: none)
     int fail;
     uint64_t full[2];    // operands of each stage written (one arrival per builder warp)
     uint64_t empty[2];   // multiplications of each stage done (tcgen05.commit)
@@ -670,7 +669,8 @@ struct TcSpreadSmem {
 };
 
 // Warp roles: warp 0 (one elected thread) issues the bulk copies of the records and the multiplications;
-// warps 1-4 write A (8 threads per point slot: x entry ix = lane % 8, all y entries), warps 5-7 write B.
+// warps 1..W/2 write A (W threads per point slot: one x entry each, all y entries), the other builder
+// warps write B.
 // No CTA-wide barrier inside the loop: builders arrive on full[stage] when their part of a batch is
 // written, the issuing thread waits on it, multiplies and commits to empty[stage], which the builders
 // wait on before they overwrite that stage two batches later.  A record buffer is refilled (chunk c + 2)
@@ -711,7 +711,6 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
     {  // zero operands A (float4 stores)
         float4* a4 = reinterpret_cast<float4*>(&T.A[0][0][0]);
         for (int i = tid; i < (int)(sizeof(T.A) / sizeof(float4)); i += kTcThreads) a4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (tid < 2 * kTcKB) T.held[tid / kTcKB][tid % kTcKB][0] = T.held[tid / kTcKB][tid % kTcKB][1] = 64;
     }
     if (warp == 0) tc::tmem_alloc(&T.tslot, 128);
     tc::fence_before_sync();
@@ -777,10 +776,18 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
         __syncwarp();
     } else {
         // ---- builders ----
-        const bool builds_a = warp <= 4;
-        const int aslot = (tid - 32) >> 3, ix = tid & 7;          // A: slot and x entry
+        // A: W / 2 warps, W threads per point slot (slot = at / W, x entry ix = at % W; a slot may span
+        // two warps).  Each thread keeps, per operand stage, the corner of the footprint its slot held
+        // there, clears the entries of that footprint in its column that the new footprint does not
+        // cover, and writes its column of the new footprint: no entry is both cleared and written, and
+        // no thread reads another's, so the slot needs no synchronisation.  B: the other 7 - W / 2 warps.
+        constexpr int kAW = W / 2;
+        const bool builds_a = warp <= kAW;
+        const int at = tid - 32;
+        const int aslot = at / W, ix = at % W;
         const int r8 = lane >> 2, kk = lane & 3;                  // B: row and K entry within a core matrix
         const int kof = (aslot >> 2) * 32 + (aslot & 3);          // A: K offset of the slot
+        int hx0 = 64, hy0 = 64, hx1 = 64, hy1 = 64;              // footprint corner held per stage (64: none)
         int b = 0;
         for (int ch = 0; ch < nch; ++ch) {
             if (*fail || !tc::mbar_wait(&T.cpbar[ch & 1], (ch >> 1) & 1, kTcWaitLimit)) {
@@ -797,33 +804,34 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
                 }
                 const int nb = np - p0 < kTcKB ? np - p0 : kTcKB;
                 if (builds_a) {
-                    // clear the footprint this stage holds in slot aslot, then write the new one
                     float* Ah = T.A[st][0];
                     float* Al = T.A[st][1];
-                    const int ox = T.held[st][aslot][0], oy = T.held[st][aslot][1];
-                    if (ox < 64 && ix < W) {
+                    const int ox = st ? hx1 : hx0, oy = st ? hy1 : hy0;
+                    int nx = 64, ny = 64;
+                    const float* pt = pts + (p0 + aslot) * R;
+                    if (aslot < nb) {
+                        const int cpk = __float_as_int(pt[3]);
+                        nx = (cpk & 255) - 64;
+                        ny = ((cpk >> 8) & 255) - 64;
+                    }
+                    if (ox < 64) {  // clear the old footprint's entries outside the new one
                         const int x = ox + ix;
                         if ((unsigned)x < 16u) {
                             const int base = (x >> 3) * 128 + (x & 7) * 4 + kof;
+                            const bool xin = (unsigned)(x - nx) < (unsigned)W;
 #pragma unroll
                             for (int iy = 0; iy < W; ++iy) {
                                 const int y = oy + iy;
-                                if ((unsigned)y < 16u) {
+                                if ((unsigned)y < 16u && !(xin && (unsigned)(y - ny) < (unsigned)W)) {
                                     Ah[256 * y + base] = 0.0f;
                                     Al[256 * y + base] = 0.0f;
                                 }
                             }
                         }
                     }
-                    __syncwarp();
-                    int nx = 64, ny = 64;
-                    if (aslot < nb) {
-                        const float* pt = pts + (p0 + aslot) * R;
-                        const int cpk = __float_as_int(pt[3]);
-                        nx = (cpk & 255) - 64;
-                        ny = ((cpk >> 8) & 255) - 64;
+                    if (aslot < nb) {  // write the new footprint's column
                         const int x = nx + ix;
-                        if (ix < W && (unsigned)x < 16u) {
+                        if ((unsigned)x < 16u) {
                             const float fx = pt[4 + ix];
                             const int base = (x >> 3) * 128 + (x & 7) * 4 + kof;
 #pragma unroll
@@ -838,16 +846,19 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
                             }
                         }
                     }
-                    if (ix == 0) {
-                        T.held[st][aslot][0] = (int16_t)nx;
-                        T.held[st][aslot][1] = (int16_t)ny;
+                    if (st) {
+                        hx1 = nx;
+                        hy1 = ny;
+                    } else {
+                        hx0 = nx;
+                        hy0 = ny;
                     }
                 } else {
                     // B (dense): q_c phi_z(z) for rows n = (c, z)
                     float* Bh = T.B[st][0];
                     float* Bl = T.B[st][1];
 #pragma unroll 2
-                    for (int cm = warp - 5; cm < 6 * (kTcKB / 4); cm += 3) {
+                    for (int cm = warp - 1 - kAW; cm < 6 * (kTcKB / 4); cm += 7 - kAW) {
                         const int g = cm >> 2, kg = cm & 3;
                         const int n = 8 * g + r8, k = 4 * kg + kk;
                         const int c = n >> 4, z = n & 15;
