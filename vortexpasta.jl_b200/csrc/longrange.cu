@@ -572,12 +572,12 @@ __global__ void __launch_bounds__(kPlaneThreads, 2) spread_plane_kernel(
 // build batch b + 1; mbarriers signalled by tcgen05.commit guard their reuse.  The brick's cells are
 // then read from tensor memory and written once (no atomics).  Every wait is bounded: on a timeout the
 // kernel records it in *status, stops issuing, and releases its tensor memory.
-constexpr int kTcThreads = 256;
+constexpr int kTcThreads = 384;  // warp 0 issues; 11 builder warps
 constexpr int kTcKB = 16;      // points per batch: two K-steps of 8
 constexpr int kTcChunk = 128;  // records per bulk copy (a multiple of kTcKB: batches never straddle chunks)
 constexpr int kTcBatchesPerChunk = kTcChunk / kTcKB;
 constexpr int kTcRecMax = 28;  // floats per record for w <= 8
-constexpr int kTcBuilderWarps = 7;  // warps 1..W/2 write A, the others B
+constexpr int kTcBuilderWarps = kTcThreads / 32 - 1;  // warps 1..W/2 write A, the others B
 constexpr uint32_t kTcWaitLimit = 1u << 26;
 
 // floats per record: charges (3), packed corner (1), 3 kernel rows of w values, padded to 16 bytes
@@ -780,7 +780,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
         // two warps).  Each thread keeps, per operand stage, the corner of the footprint its slot held
         // there, clears the entries of that footprint in its column that the new footprint does not
         // cover, and writes its column of the new footprint: no entry is both cleared and written, and
-        // no thread reads another's, so the slot needs no synchronisation.  B: the other 7 - W / 2 warps.
+        // no thread reads another's, so the slot needs no synchronisation.  B: the other builder warps.
         constexpr int kAW = W / 2;
         const bool builds_a = warp <= kAW;
         const int at = tid - 32;
@@ -858,7 +858,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
                     float* Bh = T.B[st][0];
                     float* Bl = T.B[st][1];
 #pragma unroll 2
-                    for (int cm = warp - 1 - kAW; cm < 6 * (kTcKB / 4); cm += 7 - kAW) {
+                    for (int cm = warp - 1 - kAW; cm < 6 * (kTcKB / 4); cm += kTcBuilderWarps - kAW) {
                         const int g = cm >> 2, kg = cm & 3;
                         const int n = 8 * g + r8, k = 4 * kg + kk;
                         const int c = n >> 4, z = n & 15;
@@ -882,8 +882,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) spread_tc_kernel(LRSizes S, int
     }
     __syncthreads();
     tc::fence_after_sync();
-    // ---- write the brick: warp w reads rows 32 (w % 4) .. + 31 of half w / 4; columns (c, z) ----
-    {
+    // ---- write the brick: warp w < 8 reads rows 32 (w % 4) .. + 31 of half w / 4; columns (c, z) ----
+    if (warp < 8) {
         const int h = warp >> 2, qd = warp & 3;
         const int m = 32 * qd + lane;
         const int y = 8 * h + (m >> 4), x = m & 15;
