@@ -95,7 +95,7 @@ __device__ __forceinline__ int wrapi(int i, int n) {
     return i < 0 ? i + n : i;
 }
 
-// i mod n for i in [-n, 2n) (a footprint index: n >= 2m grid points), without a division.
+// i mod n for i in [-n, 2n) without a division (a folded footprint start plus s < 2m <= n).
 __device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
 // es_kernel for a compile-time width W = 2m: u / m as a product with the constant 2 / W.
@@ -1048,7 +1048,8 @@ __global__ void __launch_bounds__(256) interp_warp_kernel(
         const double xh = (nodes[d * Np + i] * scale) / (2.0 * kPi / S.n[d]);
         const int i0 = (int)floor(xh) - S.m + 1;
         phs[warp][d][s] = (T)es_kernel_w<W>(xh - (i0 + s), S.beta, S.edge, S.kernel);
-        ixs[warp][d][s] = wrap1(i0 + s, S.n[d]);
+        // the start folded once by a modulo (any i0, also from a non-finite node), then i0w + s < 2n
+        ixs[warp][d][s] = wrap1(wrapi(i0, S.n[d]) + s, S.n[d]);
     }
     __syncwarp();
     const int64_t ng = S.ngrid, n0 = S.n[0], n1 = S.n[1];
