@@ -115,3 +115,31 @@ def test_bench_world_size_checks(monkeypatch):
     cmd = bench.launch_command(4, ["--gpus", "4", "--steps", "3"], 29500)
     assert cmd[1:3] == ["-m", "torch.distributed.run"] and "--nproc-per-node=4" in cmd
     assert "--master-addr=127.0.0.1" in cmd and cmd[-4:] == ["--gpus", "4", "--steps", "3"]
+
+
+def test_ensemble_workloads_are_kelvin_wave_limited():
+    """The two batching-form ensembles of the bench: sizes and grids as described, and every time
+    step at most the Kelvin-wave period of the system's shortest segment (the fixed 1e-3 L^2 / Gamma
+    is far above it for these tangles)."""
+    import math
+    import sys
+    from pathlib import Path
+    import numpy as np
+    root = Path(__file__).resolve().parents[1]
+    sys.path.insert(0, str(root))
+    import bench
+    from conftest import load_package
+    vp = load_package()
+    from vortexpasta_b200.params import kelvin_wave_period
+    L = 2 * math.pi
+    small = bench.small_ensemble_systems(vp, nsys=12)
+    assert len(small) == 12
+    for fs, p, dt in small:
+        n = sum(len(f) for f in fs)
+        assert 1000 <= n <= 2000 and p.splitting.Ns == (32, 32, 32) and p.precision == "mixed"
+        dmin = min(float(np.linalg.norm(np.roll(f, -1, axis=0) - f, axis=1).min()) for f in fs)
+        assert dt == min(1e-3 * L ** 2, kelvin_wave_period(dmin, a=1e-8, Delta=0.25, Gamma=1.0))
+        assert dt < 1e-3 * L ** 2
+    big = bench.ensemble_systems(vp, nsys=3)
+    for fs, p, dt in big:
+        assert 64 <= p.splitting.Ns[0] <= 256 and dt < 1e-3 * L ** 2
